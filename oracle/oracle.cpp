@@ -1,0 +1,884 @@
+// Oracle: CPU restatement of librint's Rys-ERI / RHF path (test infrastructure
+// only -- see oracle.h).  Citations are paths inside the reference project.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../librint_b200/csrc/rys_tables.h"
+
+namespace {
+
+constexpr int ATM_SLOTS = 6;   // src/scf.rs:14
+constexpr int BAS_SLOTS = 8;   // src/scf.rs:15
+constexpr int LMAX = 4;        // same shell limit as src/eri.rs:10
+constexpr int NCART_MAX = (LMAX + 1) * (LMAX + 2) / 2;
+constexpr int NROOT_MAX = 2 * LMAX + 1;
+
+inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+inline int nsph(int l) { return 2 * l + 1; }
+
+// Angular normalisation libcint folds into s and p shells
+// (src/g1e.rs:776-782): 1/sqrt(4 pi) and sqrt(3/(4 pi)).
+double common_fac_sp(int l) {
+  if (l == 0) return 0.5 / std::sqrt(M_PI);
+  if (l == 1) return std::sqrt(3.0 / (4.0 * M_PI));
+  return 1.0;
+}
+
+// Cartesian exponents in libcint order, x-major descending
+// (src/eri.rs:31-50, src/cint_bas.rs:234).
+struct CartComp {
+  int n;
+  int x[NCART_MAX], y[NCART_MAX], z[NCART_MAX];
+  explicit CartComp(int l) : n(0) {
+    for (int lx = l; lx >= 0; --lx)
+      for (int ly = l - lx; ly >= 0; --ly) {
+        x[n] = lx; y[n] = ly; z[n] = l - lx - ly; ++n;
+      }
+  }
+};
+
+// ---------------------------------------------------------------- Rys roots
+// Node/weight tables from librint_b200/csrc/gen_rys_tables.py (own fits to
+// exact 60-digit rules); same u = t^2/(1-t^2) convention as CINTrys_roots
+// (src/rys_roots.rs:3036-3158).
+void rys_roots(int n, double x, double *u, double *w) {
+  const double xbreak = 43.0 + 5.0 * n;
+  if (x >= xbreak) {
+    const int off = n * (n - 1) / 2;
+    const double t = std::sqrt(M_PI / 4.0 / x);
+    for (int i = 0; i < n; ++i) {
+      const double r = RYS_LARGEX_R[off + i];
+      u[i] = r / (x - r);
+      w[i] = RYS_LARGEX_W[off + i] * t;
+    }
+    return;
+  }
+  int seg = (int)(x * (1.0 / RYS_SEG_WIDTH));
+  if (seg >= RYS_TAB_NSEG[n]) seg = RYS_TAB_NSEG[n] - 1;
+  if (seg < 0) seg = 0;
+  const double t = (x - (seg * RYS_SEG_WIDTH + 0.5 * RYS_SEG_WIDTH)) * (2.0 / RYS_SEG_WIDTH);
+  const double *c = RYS_TAB + RYS_TAB_OFFSET[n] + (size_t)seg * 2 * n * RYS_NCOEF;
+  for (int f = 0; f < 2 * n; ++f) {
+    const double *cf = c + f * RYS_NCOEF;
+    double r = cf[RYS_DEG];
+    for (int k = RYS_DEG - 1; k >= 0; --k) r = r * t + cf[k];
+    if (f < n) u[f] = r; else w[f - n] = r;
+  }
+}
+
+// ---------------------------------------------------------------- shells
+struct Shell {
+  int l, nprim, nctr;
+  const double *r, *a, *c;   // centre, exponents, coefficients [ctr][prim]
+};
+
+Shell shell_of(int sh, const int *atm, const int *bas, const double *env) {
+  const int *b = bas + BAS_SLOTS * sh;
+  Shell s;
+  s.l = b[1]; s.nprim = b[2]; s.nctr = b[3];
+  s.r = env + atm[ATM_SLOTS * b[0] + 1];
+  s.a = env + b[5];
+  s.c = env + b[6];
+  return s;
+}
+
+// log of the largest |coefficient| per primitive over the contractions
+// (src/optimizer.rs:661-687, CINTOpt_log_max_pgto_coeff).
+void log_maxc(const Shell &s, double *out) {
+  for (int p = 0; p < s.nprim; ++p) {
+    double m = 0.0;
+    for (int c = 0; c < s.nctr; ++c) m = std::max(m, std::fabs(s.c[c * s.nprim + p]));
+    out[p] = std::log(m);
+  }
+}
+
+double sqr_dist(const double *a, const double *b) {
+  const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// ---------------------------------------------------------------- 2e kernel
+// Per root and axis the 2D table is built on the "base" centre of each pair
+// and shifted to the partner by horizontal recurrence: the base of (ij) is i
+// when li > lj, else j; of (kl) k when lk > ll, else l (libcint's choice,
+// src/g2e.rs:113-181, which keeps the HRR short on the high-l centre).
+// G[a][b][c][d]: a = power on the bra base A, b on its partner B, c on the
+// ket base C, d on its partner D.
+constexpr int NAB = 2 * LMAX + 1;
+constexpr int GSIZE = NAB * (LMAX + 1) * NAB * (LMAX + 1);
+
+struct Quartet {
+  Shell si, sj, sk, sl;
+  int li, lj, lk, ll, nroots;
+  bool ibase, kbase;
+  int lA, lB, lC, lD, nab, ncd;
+  const double *rA, *rB, *rC, *rD;
+  double common_factor, expcutoff;
+  double rirj[3], rkrl[3], rr_ij, rr_kl;
+  double AB[3], CD[3];
+  int sB, sC, sA;   // strides of G: index = ((a*(lB+1) + b)*(ncd+1) + c)*(lD+1) + d
+};
+
+Quartet make_quartet(const int *shls, const int *atm, const int *bas, const double *env) {
+  Quartet q;
+  q.si = shell_of(shls[0], atm, bas, env);
+  q.sj = shell_of(shls[1], atm, bas, env);
+  q.sk = shell_of(shls[2], atm, bas, env);
+  q.sl = shell_of(shls[3], atm, bas, env);
+  q.li = q.si.l; q.lj = q.sj.l; q.lk = q.sk.l; q.ll = q.sl.l;
+  q.nroots = (q.li + q.lj + q.lk + q.ll) / 2 + 1;   // src/g2e.rs:100-101
+  q.ibase = q.li > q.lj;
+  q.kbase = q.lk > q.ll;
+  q.lA = q.ibase ? q.li : q.lj; q.lB = q.ibase ? q.lj : q.li;
+  q.lC = q.kbase ? q.lk : q.ll; q.lD = q.kbase ? q.ll : q.lk;
+  q.rA = q.ibase ? q.si.r : q.sj.r; q.rB = q.ibase ? q.sj.r : q.si.r;
+  q.rC = q.kbase ? q.sk.r : q.sl.r; q.rD = q.kbase ? q.sl.r : q.sk.r;
+  q.nab = q.lA + q.lB;
+  q.ncd = q.lC + q.lD;
+  q.sC = q.lD + 1;
+  q.sB = (q.ncd + 1) * q.sC;
+  q.sA = (q.lB + 1) * q.sB;
+  // 2 pi^3 / sqrt(pi) times the s/p angular factors (src/g2e.rs:74-82)
+  q.common_factor = 2.0 * M_PI * M_PI * M_PI / std::sqrt(M_PI) *
+                    common_fac_sp(q.li) * common_fac_sp(q.lj) *
+                    common_fac_sp(q.lk) * common_fac_sp(q.ll);
+  // src/g2e.rs:83-92 (the no-optimizer loop reads envs.expcutoff)
+  q.expcutoff = env[0] == 0.0 ? 60.0 : std::max(40.0, env[0]) + 1.0;
+  for (int d = 0; d < 3; ++d) {
+    q.rirj[d] = q.si.r[d] - q.sj.r[d];
+    q.rkrl[d] = q.sk.r[d] - q.sl.r[d];
+    q.AB[d] = q.rA[d] - q.rB[d];
+    q.CD[d] = q.rC[d] - q.rD[d];
+  }
+  q.rr_ij = q.rirj[0] * q.rirj[0] + q.rirj[1] * q.rirj[1] + q.rirj[2] * q.rirj[2];
+  q.rr_kl = q.rkrl[0] * q.rkrl[0] + q.rkrl[1] * q.rkrl[1] + q.rkrl[2] * q.rkrl[2];
+  return q;
+}
+
+// One root: B00/B10/B01/C00/C0p (src/g2e.rs:5655-5673), 2D VRR on (A, C)
+// (src/g2e.rs:316-506), HRR A->B and C->D (src/g2e.rs:507-909).
+void g_one_root(double *g[3], const Quartet &q, double aij, double akl,
+                double a0, double fac1, double u, double w,
+                const double *rij, const double *rkl, const double *rijrkl) {
+  const int nab = q.nab, ncd = q.ncd, sA = q.sA, sB = q.sB, sC = q.sC;
+  const double a1 = aij * akl;
+  const double u2 = a0 * u;
+  const double tmp4 = 0.5 / (u2 * (aij + akl) + a1);
+  const double tmp5 = u2 * tmp4;
+  const double tmp1 = 2.0 * tmp5;
+  const double tmp2 = tmp1 * akl;
+  const double tmp3 = tmp1 * aij;
+  const double b00 = tmp5;
+  const double b10 = tmp5 + tmp4 * akl;
+  const double b01 = tmp5 + tmp4 * aij;
+  for (int ax = 0; ax < 3; ++ax) {
+    double *G = g[ax];
+    const double cn = rij[ax] - q.rA[ax] - tmp2 * rijrkl[ax];
+    const double cm = rkl[ax] - q.rC[ax] + tmp3 * rijrkl[ax];
+    // V(n, m) lives at G[n][0][m][0]
+    auto V = [&](int n, int m) -> double & { return G[n * sA + m * sC]; };
+    V(0, 0) = ax == 2 ? w * fac1 : 1.0;
+    for (int m = 1; m <= ncd; ++m) {
+      double v = cm * V(0, m - 1);
+      if (m > 1) v += (m - 1) * b01 * V(0, m - 2);
+      V(0, m) = v;
+    }
+    for (int n = 1; n <= nab; ++n)
+      for (int m = 0; m <= ncd; ++m) {
+        double v = cn * V(n - 1, m);
+        if (n > 1) v += (n - 1) * b10 * V(n - 2, m);
+        if (m > 0) v += m * b00 * V(n - 1, m - 1);
+        V(n, m) = v;
+      }
+    // bra HRR: (x-RB) = (x-RA) + (RA-RB)
+    const double ab = q.AB[ax];
+    for (int b = 1; b <= q.lB; ++b)
+      for (int a = 0; a <= nab - b; ++a)
+        for (int c = 0; c <= ncd; ++c)
+          G[a * sA + b * sB + c * sC] = G[(a + 1) * sA + (b - 1) * sB + c * sC] +
+                                        ab * G[a * sA + (b - 1) * sB + c * sC];
+    const double cd = q.CD[ax];
+    for (int a = 0; a <= q.lA; ++a)
+      for (int b = 0; b <= q.lB; ++b)
+        for (int d = 1; d <= q.lD; ++d)
+          for (int c = 0; c <= ncd - d; ++c)
+            G[a * sA + b * sB + c * sC + d] = G[a * sA + b * sB + (c + 1) * sC + d - 1] +
+                                              cd * G[a * sA + b * sB + c * sC + d - 1];
+  }
+}
+
+// Cartesian block for one quartet, any contraction pattern.  Loop nest and
+// screening follow CINT2e_loop_nopt (src/cint2e.rs:36-465) with
+// CINTset_pairdata (src/optimizer.rs:732-808); the recurrence and the gout
+// root sum follow src/eri.rs:421-516 / src/cint2e.rs:2456, with the
+// recurrence orientation of src/g2e.rs:113-181.
+// out must hold ncart(i)*nctr_i * ... doubles; it is overwritten.
+int eri_cart(double *out, const Quartet &q) {
+  const Shell &si = q.si, &sj = q.sj, &sk = q.sk, &sl = q.sl;
+  const int nfi = ncart(q.li), nfj = ncart(q.lj), nfk = ncart(q.lk), nfl = ncart(q.ll);
+  const int ni = nfi * si.nctr, nj = nfj * sj.nctr, nk = nfk * sk.nctr, nl = nfl * sl.nctr;
+  const size_t ntot = (size_t)ni * nj * nk * nl;
+  std::memset(out, 0, ntot * sizeof(double));
+
+  double lci[16], lcj[16], lck[16], lcl[16];
+  log_maxc(si, lci); log_maxc(sj, lcj); log_maxc(sk, lck); log_maxc(sl, lcl);
+
+  // pair data for (ij)
+  double log_rr_ij = 1.7 - 1.5 * std::log(si.a[si.nprim - 1] + sj.a[sj.nprim - 1]);
+  if (q.li + q.lj > 0) log_rr_ij += (q.li + q.lj) * std::log(std::sqrt(q.rr_ij) + 1.0);
+  std::vector<double> cceij(si.nprim * sj.nprim), eij(si.nprim * sj.nprim),
+      rij(3 * si.nprim * sj.nprim);
+  bool empty = true;
+  for (int jp = 0; jp < sj.nprim; ++jp)
+    for (int ip = 0; ip < si.nprim; ++ip) {
+      const int n = jp * si.nprim + ip;
+      const double inv = 1.0 / (si.a[ip] + sj.a[jp]);
+      const double e = q.rr_ij * si.a[ip] * sj.a[jp] * inv;
+      cceij[n] = e - log_rr_ij - lci[ip] - lcj[jp];
+      if (cceij[n] < q.expcutoff) {
+        empty = false;
+        const double wj = sj.a[jp] * inv;
+        for (int d = 0; d < 3; ++d) rij[3 * n + d] = si.r[d] + wj * (sj.r[d] - si.r[d]);
+        eij[n] = std::exp(-e);
+      } else {
+        for (int d = 0; d < 3; ++d) rij[3 * n + d] = 1e18;
+        eij[n] = 0.0;
+      }
+    }
+  if (empty) return 0;
+  double log_rr_kl = 1.7 - 1.5 * std::log(sk.a[sk.nprim - 1] + sl.a[sl.nprim - 1]);
+  if (q.lk + q.ll > 0) log_rr_kl += (q.lk + q.ll) * std::log(std::sqrt(q.rr_kl) + 1.0);
+
+  const CartComp ci(q.li), cj(q.lj), ck(q.lk), cl(q.ll);
+  const int nf = nfi * nfj * nfk * nfl;
+  const int nc = si.nctr * sj.nctr * sk.nctr * sl.nctr;
+  std::vector<double> gbuf(3 * GSIZE), prim(nf);
+  double *g[3] = {gbuf.data(), gbuf.data() + GSIZE, gbuf.data() + 2 * GSIZE};
+  double u[NROOT_MAX], w[NROOT_MAX];
+  int any = 0;
+
+  for (int lp = 0; lp < sl.nprim; ++lp) {
+    const double al = sl.a[lp];
+    for (int kp = 0; kp < sk.nprim; ++kp) {
+      const double ak = sk.a[kp];
+      const double akl = ak + al;
+      const double ekl_val = q.rr_kl * ak * al / akl;
+      const double ccekl = ekl_val - log_rr_kl - lck[kp] - lcl[lp];
+      if (ccekl > q.expcutoff) continue;
+      double rkl[3];
+      for (int d = 0; d < 3; ++d) rkl[d] = (ak * sk.r[d] + al * sl.r[d]) / akl;
+      const double eijcutoff = q.expcutoff - ccekl;
+      const double ekl = std::exp(-ekl_val);
+      for (int jp = 0; jp < sj.nprim; ++jp)
+        for (int ip = 0; ip < si.nprim; ++ip) {
+          const int n = jp * si.nprim + ip;
+          if (cceij[n] > eijcutoff) continue;
+          const double aij = si.a[ip] + sj.a[jp];
+          const double *pij = &rij[3 * n];
+          const double fac = q.common_factor * eij[n] * ekl;
+          // CINTg0_2e prefactors (src/g2e.rs:5563-5568)
+          const double a1 = aij * akl;
+          const double a0 = a1 / (aij + akl);
+          const double fac1 = std::sqrt(a0 / (a1 * a1 * a1)) * fac;
+          double rijrkl[3];
+          for (int d = 0; d < 3; ++d) rijrkl[d] = pij[d] - rkl[d];
+          const double x = a0 * (rijrkl[0] * rijrkl[0] + rijrkl[1] * rijrkl[1] +
+                                 rijrkl[2] * rijrkl[2]);
+          rys_roots(q.nroots, x, u, w);
+          std::fill(prim.begin(), prim.end(), 0.0);
+          for (int r = 0; r < q.nroots; ++r) {
+            g_one_root(g, q, aij, akl, a0, fac1, u[r], w[r], pij, rkl, rijrkl);
+            int idx = 0;
+            for (int lf = 0; lf < nfl; ++lf)
+              for (int kf = 0; kf < nfk; ++kf)
+                for (int jf = 0; jf < nfj; ++jf)
+                  for (int iff = 0; iff < nfi; ++iff, ++idx) {
+                    const int pi_[3] = {ci.x[iff], ci.y[iff], ci.z[iff]};
+                    const int pj_[3] = {cj.x[jf], cj.y[jf], cj.z[jf]};
+                    const int pk_[3] = {ck.x[kf], ck.y[kf], ck.z[kf]};
+                    const int pl_[3] = {cl.x[lf], cl.y[lf], cl.z[lf]};
+                    double v = 1.0;
+                    for (int ax = 0; ax < 3; ++ax) {
+                      const int a = q.ibase ? pi_[ax] : pj_[ax], b = q.ibase ? pj_[ax] : pi_[ax];
+                      const int c = q.kbase ? pk_[ax] : pl_[ax], d = q.kbase ? pl_[ax] : pk_[ax];
+                      v *= g[ax][a * q.sA + b * q.sB + c * q.sC + d];
+                    }
+                    prim[idx] += v;
+                  }
+          }
+          any = 1;
+          // contract over every (ci, cj, ck, cl) combination
+          for (int c = 0; c < nc; ++c) {
+            const int cci = c % si.nctr, ccj = (c / si.nctr) % sj.nctr;
+            const int cck = (c / (si.nctr * sj.nctr)) % sk.nctr;
+            const int ccl = c / (si.nctr * sj.nctr * sk.nctr);
+            const double cc = si.c[cci * si.nprim + ip] * sj.c[ccj * sj.nprim + jp] *
+                              sk.c[cck * sk.nprim + kp] * sl.c[ccl * sl.nprim + lp];
+            int idx2 = 0;
+            for (int lf = 0; lf < nfl; ++lf)
+              for (int kf = 0; kf < nfk; ++kf)
+                for (int jf = 0; jf < nfj; ++jf)
+                  for (int iff = 0; iff < nfi; ++iff, ++idx2) {
+                    const size_t o = (size_t)(iff + nfi * cci) +
+                                     (size_t)ni * ((jf + nfj * ccj) +
+                                     (size_t)nj * ((kf + nfk * cck) + (size_t)nk * (lf + nfl * ccl)));
+                    out[o] += cc * prim[idx2];
+                  }
+          }
+        }
+    }
+  }
+  return any;
+}
+
+// ---------------------------------------------------------------- cart2sph
+// Real solid harmonics in libcint order and normalisation (m = -l..l; p kept
+// as x, y, z).  Coefficients from the closed form of Helgaker, Jorgensen &
+// Olsen, "Molecular Electronic-Structure Theory", eqs. 6.4.47-6.4.50, scaled
+// by sqrt((2l+1)/(4 pi)); the reference tabulates the same numbers
+// (src/cart2sph.rs:26, d shells at :88463-88538).
+double binom(int n, int k) {
+  if (k < 0 || k > n) return 0.0;
+  double r = 1.0;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+double fact(int n) { double r = 1.0; for (int i = 2; i <= n; ++i) r *= i; return r; }
+
+struct SphTable {
+  // c[l][ms][cart]: coefficient of cartesian component cart in sph function ms
+  std::vector<double> c[LMAX + 1];
+  SphTable() {
+    for (int l = 0; l <= LMAX; ++l) {
+      const int nc = ncart(l), ns = nsph(l);
+      c[l].assign(ns * nc, 0.0);
+      if (l <= 1) {
+        for (int i = 0; i < nc; ++i) c[l][i * nc + i] = 1.0;
+        continue;
+      }
+      const CartComp cc(l);
+      const double scale = std::sqrt((2 * l + 1) / (4.0 * M_PI));
+      for (int m = -l; m <= l; ++m) {
+        const int am = std::abs(m);
+        const double norm = 1.0 / (std::pow(2.0, am) * fact(l)) *
+                            std::sqrt(2.0 * fact(l + am) * fact(l - am) / (m == 0 ? 2.0 : 1.0));
+        const int twovm = m < 0 ? 1 : 0;   // 2 v_m
+        for (int t = 0; t <= (l - am) / 2; ++t)
+          for (int uu = 0; uu <= t; ++uu)
+            for (int twov = twovm; twov <= am; twov += 2) {
+              // v = twov/2; v runs v_m .. floor(|m|/2 - v_m) + v_m
+              const int sgn_exp = t + (twov - twovm) / 2;
+              const double coef = (sgn_exp % 2 ? -1.0 : 1.0) * std::pow(0.25, t) * binom(l, t) *
+                                  binom(l - t, am + t) * binom(t, uu) * binom(am, twov);
+              const int px = 2 * t + am - 2 * uu - twov;
+              const int py = 2 * uu + twov;
+              const int pz = l - 2 * t - am;
+              for (int k = 0; k < nc; ++k)
+                if (cc.x[k] == px && cc.y[k] == py && cc.z[k] == pz)
+                  c[l][(m + l) * nc + k] += norm * scale * coef;
+            }
+      }
+    }
+  }
+};
+const SphTable &sph_table() { static SphTable t; return t; }
+
+// Transform a cartesian block (i fastest, nctr folded in) to spherical
+// (src/cart2sph.rs:90199-90282 transforms j, l, k, then i; the order only
+// changes rounding).
+void cart2sph_4(double *sph, const double *cart, const Quartet &q) {
+  const int l4[4] = {q.li, q.lj, q.lk, q.ll};
+  const int nct[4] = {q.si.nctr, q.sj.nctr, q.sk.nctr, q.sl.nctr};
+  int dim[4];
+  for (int a = 0; a < 4; ++a) dim[a] = ncart(l4[a]) * nct[a];
+  std::vector<double> cur(cart, cart + (size_t)dim[0] * dim[1] * dim[2] * dim[3]);
+  for (int ax = 0; ax < 4; ++ax) {
+    const int l = l4[ax], nc = ncart(l), ns = nsph(l);
+    const std::vector<double> &co = sph_table().c[l];
+    int ndim[4] = {dim[0], dim[1], dim[2], dim[3]};
+    ndim[ax] = ns * nct[ax];
+    size_t inner = 1, outer = 1;
+    for (int a = 0; a < ax; ++a) inner *= dim[a];
+    for (int a = ax + 1; a < 4; ++a) outer *= dim[a];
+    std::vector<double> nxt(inner * ndim[ax] * outer, 0.0);
+    for (size_t o = 0; o < outer; ++o)
+      for (int ct = 0; ct < nct[ax]; ++ct)
+        for (int m = 0; m < ns; ++m)
+          for (int k = 0; k < nc; ++k) {
+            const double cf = co[m * nc + k];
+            if (cf == 0.0) continue;
+            const double *src = &cur[(o * dim[ax] + ct * nc + k) * inner];
+            double *dst = &nxt[(o * ndim[ax] + ct * ns + m) * inner];
+            for (size_t i = 0; i < inner; ++i) dst[i] += cf * src[i];
+          }
+    cur.swap(nxt);
+    dim[ax] = ndim[ax];
+  }
+  std::memcpy(sph, cur.data(), cur.size() * sizeof(double));
+}
+
+int quartet_block(double *out, int coord, const int *shls, const int *atm,
+                  const int *bas, const double *env) {
+  const Quartet q = make_quartet(shls, atm, bas, env);
+  if (coord == 0) return eri_cart(out, q);
+  const size_t nct = (size_t)ncart(q.li) * q.si.nctr * ncart(q.lj) * q.sj.nctr *
+                     ncart(q.lk) * q.sk.nctr * ncart(q.ll) * q.sl.nctr;
+  std::vector<double> cart(nct);
+  const int r = eri_cart(cart.data(), q);
+  cart2sph_4(out, cart.data(), q);
+  return r;
+}
+
+int shell_dim(int coord, const int *bas, int sh) {
+  const int l = bas[BAS_SLOTS * sh + 1], nctr = bas[BAS_SLOTS * sh + 3];
+  return (coord == 0 ? ncart(l) : nsph(l)) * nctr;
+}
+
+std::vector<int> shell_offsets(int coord, const int *bas, int nbas) {
+  std::vector<int> off(nbas + 1, 0);
+  for (int s = 0; s < nbas; ++s) off[s + 1] = off[s] + shell_dim(coord, bas, s);
+  return off;
+}
+
+int threads_or_default(int nthreads) {
+#ifdef _OPENMP
+  return nthreads > 0 ? nthreads : omp_get_max_threads();
+#else
+  (void)nthreads;
+  return 1;
+#endif
+}
+
+// ---------------------------------------------------------------- 1e
+// Primitive-pair 1D overlaps by the Obara-Saika recurrence; kinetic as
+// -1/2 d^2/dx^2 on the ket; nuclear attraction by Rys quadrature with
+// (li+lj)/2+1 roots per point nucleus.  Same operators and normalisation as
+// cint1e_ovlp/kin/nuc_cart (src/cint1e.rs:925,976; src/intor1.rs:168;
+// src/g1e.rs:241-330).
+void overlap_1d(double *s, int imax, int jmax, double xpa, double xpb, double oo2p) {
+  // s[i*(jmax+1)+j], s(0,0) = 1
+  const int ld = jmax + 1;
+  s[0] = 1.0;
+  for (int i = 0; i <= imax; ++i)
+    for (int j = 0; j <= jmax; ++j) {
+      if (i == 0 && j == 0) continue;
+      double v;
+      if (i > 0) {
+        v = xpa * s[(i - 1) * ld + j];
+        if (i > 1) v += oo2p * (i - 1) * s[(i - 2) * ld + j];
+        if (j > 0) v += oo2p * j * s[(i - 1) * ld + j - 1];
+      } else {
+        v = xpb * s[j - 1];
+        if (j > 1) v += oo2p * (j - 1) * s[j - 2];
+      }
+      s[i * ld + j] = v;
+    }
+}
+
+void int1e_block(double *out, int typec, const Shell &a, const Shell &b,
+                 const int *atm, int natm, const double *env) {
+  const int la = a.l, lb = b.l, nfa = ncart(la), nfb = ncart(lb);
+  const int na = nfa * a.nctr, nb = nfb * b.nctr;
+  std::memset(out, 0, sizeof(double) * na * nb);
+  const CartComp ca(la), cb(lb);
+  const double rab2 = sqr_dist(a.r, b.r);
+  const double cfac = common_fac_sp(la) * common_fac_sp(lb);
+  const int imax = la, jmax = lb + (typec == 1 ? 2 : 0);
+  double sx[3][(LMAX + 1) * (LMAX + 3)];
+  std::vector<double> prim(nfa * nfb);
+  for (int jp = 0; jp < b.nprim; ++jp)
+    for (int ip = 0; ip < a.nprim; ++ip) {
+      const double ai = a.a[ip], bj = b.a[jp], p = ai + bj;
+      const double mu = ai * bj / p;
+      const double eab = std::exp(-mu * rab2);
+      double P[3];
+      for (int d = 0; d < 3; ++d) P[d] = (ai * a.r[d] + bj * b.r[d]) / p;
+      std::fill(prim.begin(), prim.end(), 0.0);
+      if (typec == 0 || typec == 1) {
+        for (int d = 0; d < 3; ++d)
+          overlap_1d(sx[d], imax, jmax, P[d] - a.r[d], P[d] - b.r[d], 0.5 / p);
+        const double pre = cfac * eab * std::pow(M_PI / p, 1.5);
+        const int ld = jmax + 1;
+        for (int jf = 0; jf < nfb; ++jf)
+          for (int iff = 0; iff < nfa; ++iff) {
+            const int ia[3] = {ca.x[iff], ca.y[iff], ca.z[iff]};
+            const int jb[3] = {cb.x[jf], cb.y[jf], cb.z[jf]};
+            double v;
+            if (typec == 0) {
+              v = sx[0][ia[0] * ld + jb[0]] * sx[1][ia[1] * ld + jb[1]] * sx[2][ia[2] * ld + jb[2]];
+            } else {
+              v = 0.0;
+              for (int d = 0; d < 3; ++d) {
+                const int j = jb[d];
+                const double *s = sx[d] + ia[d] * ld;
+                double t = -2.0 * bj * (2 * j + 1) * s[j] + 4.0 * bj * bj * s[j + 2];
+                if (j >= 2) t += j * (j - 1) * s[j - 2];
+                t *= -0.5;
+                double o = 1.0;
+                for (int e = 0; e < 3; ++e)
+                  if (e != d) o *= sx[e][ia[e] * ld + jb[e]];
+                v += t * o;
+              }
+            }
+            prim[iff + nfa * jf] = pre * v;
+          }
+      } else {
+        const int nroots = (la + lb) / 2 + 1;
+        double u[NROOT_MAX], w[NROOT_MAX];
+        const int lsum = la + lb;
+        double ix[3][LMAX * 2 + 1][LMAX + 1];
+        for (int c = 0; c < natm; ++c) {
+          const int *ac = atm + ATM_SLOTS * c;
+          const double *rc = env + ac[1];
+          const double z = -std::fabs((double)ac[0]);
+          const double pc2 = sqr_dist(P, rc);
+          rys_roots(nroots, p * pc2, u, w);
+          const double pre = cfac * eab * 2.0 * M_PI / p * z;
+          for (int r = 0; r < nroots; ++r) {
+            const double t2 = u[r] / (1.0 + u[r]);
+            for (int d = 0; d < 3; ++d) {
+              // 1D: I(n+1) = (PA - t2 PC) I(n) + n/(2p) (1-t2) I(n-1), then HRR to j
+              double g[2 * LMAX + 2];
+              g[0] = 1.0;
+              const double c0 = (P[d] - a.r[d]) - t2 * (P[d] - rc[d]);
+              const double b1 = 0.5 / p * (1.0 - t2);
+              if (lsum > 0) g[1] = c0;
+              for (int n = 1; n < lsum; ++n) g[n + 1] = c0 * g[n] + n * b1 * g[n - 1];
+              // HRR: I(i, j+1) = I(i+1, j) + (A-B) I(i, j)
+              double h[2 * LMAX + 2][LMAX + 1];
+              for (int i = 0; i <= lsum; ++i) h[i][0] = g[i];
+              const double ab = a.r[d] - b.r[d];
+              for (int j = 1; j <= lb; ++j)
+                for (int i = 0; i <= lsum - j; ++i) h[i][j] = h[i + 1][j - 1] + ab * h[i][j - 1];
+              for (int i = 0; i <= la; ++i)
+                for (int j = 0; j <= lb; ++j) ix[d][i][j] = h[i][j];
+            }
+            for (int jf = 0; jf < nfb; ++jf)
+              for (int iff = 0; iff < nfa; ++iff)
+                prim[iff + nfa * jf] += pre * w[r] * ix[0][ca.x[iff]][cb.x[jf]] *
+                                        ix[1][ca.y[iff]][cb.y[jf]] * ix[2][ca.z[iff]][cb.z[jf]];
+          }
+        }
+      }
+      for (int cj = 0; cj < b.nctr; ++cj)
+        for (int cI = 0; cI < a.nctr; ++cI) {
+          const double cc = a.c[cI * a.nprim + ip] * b.c[cj * b.nprim + jp];
+          for (int jf = 0; jf < nfb; ++jf)
+            for (int iff = 0; iff < nfa; ++iff)
+              out[(iff + nfa * cI) + na * (jf + nfb * cj)] += cc * prim[iff + nfa * jf];
+        }
+    }
+}
+
+// 2-index cart -> sph for a 1e block (i fastest)
+void cart2sph_2(double *sph, const double *cart, const Shell &a, const Shell &b) {
+  const int nca = ncart(a.l), ncb = ncart(b.l), nsa = nsph(a.l), nsb = nsph(b.l);
+  const int Na = nca * a.nctr, Nb = ncb * b.nctr, Sa = nsa * a.nctr, Sb = nsb * b.nctr;
+  const std::vector<double> &A = sph_table().c[a.l], &B = sph_table().c[b.l];
+  std::vector<double> tmp((size_t)Sa * Nb, 0.0);
+  for (int j = 0; j < Nb; ++j)
+    for (int ct = 0; ct < a.nctr; ++ct)
+      for (int m = 0; m < nsa; ++m) {
+        double v = 0.0;
+        for (int k = 0; k < nca; ++k) v += A[m * nca + k] * cart[(ct * nca + k) + Na * j];
+        tmp[(ct * nsa + m) + Sa * j] = v;
+      }
+  for (int i = 0; i < Sa; ++i)
+    for (int ct = 0; ct < b.nctr; ++ct)
+      for (int m = 0; m < nsb; ++m) {
+        double v = 0.0;
+        for (int k = 0; k < ncb; ++k) v += B[m * ncb + k] * tmp[i + Sa * (ct * ncb + k)];
+        sph[i + Sa * (ct * nsb + m)] = v;
+      }
+}
+
+// ---------------------------------------------------------------- linear algebra
+// Cyclic Jacobi eigensolver for a symmetric matrix (row-major, overwritten).
+// Eigenvalues ascending in w, eigenvectors in the columns of V (row-major).
+void eigh(int n, std::vector<double> A, std::vector<double> &w, std::vector<double> &V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const double a2 = A[(size_t)i * n + j] * A[(size_t)i * n + j];
+        tot += a2;
+        if (i != j) off += a2;
+      }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = A[(size_t)p * n + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+          A[(size_t)k * n + p] = c * akp - s * akq;
+          A[(size_t)k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+          A[(size_t)p * n + k] = c * apk - s * aqk;
+          A[(size_t)q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+          V[(size_t)k * n + p] = c * vkp - s * vkq;
+          V[(size_t)k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  w.resize(n);
+  for (int i = 0; i < n; ++i) w[i] = A[(size_t)i * n + i];
+  std::vector<int> idx(n);
+  for (int i = 0; i < n; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return w[x] < w[y]; });
+  std::vector<double> w2(n), V2((size_t)n * n);
+  for (int c = 0; c < n; ++c) {
+    w2[c] = w[idx[c]];
+    for (int r = 0; r < n; ++r) V2[(size_t)r * n + c] = V[(size_t)r * n + idx[c]];
+  }
+  w.swap(w2);
+  V.swap(V2);
+}
+
+std::vector<double> matmul(int n, const std::vector<double> &A, const std::vector<double> &B) {
+  std::vector<double> C((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < n; ++k) {
+      const double a = A[(size_t)i * n + k];
+      for (int j = 0; j < n; ++j) C[(size_t)i * n + j] += a * B[(size_t)k * n + j];
+    }
+  return C;
+}
+
+double nuclear_repulsion(const int *atm, int natm, const double *env) {
+  double e = 0.0;
+  for (int i = 0; i < natm; ++i)
+    for (int j = 0; j < i; ++j) {
+      const double *ri = env + atm[ATM_SLOTS * i + 1], *rj = env + atm[ATM_SLOTS * j + 1];
+      e += (double)(atm[ATM_SLOTS * i] * atm[ATM_SLOTS * j]) / std::sqrt(sqr_dist(ri, rj));
+    }
+  return e;
+}
+
+}  // namespace
+
+// ====================================================================== C API
+extern "C" {
+
+void orc_rys_roots(int n, double x, double *u, double *w) { rys_roots(n, x, u, w); }
+
+int orc_nao(int coord, const int *bas, int nbas) {
+  int n = 0;
+  for (int s = 0; s < nbas; ++s) n += shell_dim(coord, bas, s);
+  return n;
+}
+
+int orc_int2e_cart(double *out, const int *shls, const int *atm, int, const int *bas,
+                   int, const double *env) {
+  return quartet_block(out, 0, shls, atm, bas, env);
+}
+
+int orc_int2e_sph(double *out, const int *shls, const int *atm, int, const int *bas,
+                  int, const double *env) {
+  return quartet_block(out, 1, shls, atm, bas, env);
+}
+
+void orc_int2e_batch(double *out, int coord, const int *shls, long nq, const int *atm,
+                     int, const int *bas, int, const double *env, int nthreads) {
+  std::vector<size_t> off(nq + 1, 0);
+  for (long q = 0; q < nq; ++q) {
+    size_t d = 1;
+    for (int a = 0; a < 4; ++a) d *= shell_dim(coord, bas, shls[4 * q + a]);
+    off[q + 1] = off[q] + d;
+  }
+  const int nt = threads_or_default(nthreads);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nt)
+  for (long q = 0; q < nq; ++q) quartet_block(out + off[q], coord, shls + 4 * q, atm, bas, env);
+}
+
+void orc_int2e_tensor(double *out, int coord, const int *atm, int, const int *bas,
+                      int nbas, const double *env, int nthreads) {
+  const std::vector<int> off = shell_offsets(coord, bas, nbas);
+  const size_t n = off[nbas];
+  const int nt = threads_or_default(nthreads);
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<double> buf;
+#pragma omp for schedule(dynamic) collapse(2)
+    for (int i = 0; i < nbas; ++i)
+      for (int j = 0; j < nbas; ++j)
+        for (int k = 0; k < nbas; ++k)
+          for (int l = 0; l < nbas; ++l) {
+            const int shls[4] = {i, j, k, l};
+            const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
+            const int dk = off[k + 1] - off[k], dl = off[l + 1] - off[l];
+            buf.resize((size_t)di * dj * dk * dl);
+            quartet_block(buf.data(), coord, shls, atm, bas, env);
+            size_t c = 0;
+            for (int L = 0; L < dl; ++L)
+              for (int K = 0; K < dk; ++K)
+                for (int J = 0; J < dj; ++J)
+                  for (int I = 0; I < di; ++I, ++c)
+                    out[(((size_t)(off[i] + I) * n + off[j] + J) * n + off[k] + K) * n + off[l] + L] = buf[c];
+          }
+  }
+}
+
+void orc_int1e(double *out, int coord, int typec, const int *atm, int natm, const int *bas,
+               int nbas, const double *env) {
+  const std::vector<int> off = shell_offsets(coord, bas, nbas);
+  const int n = off[nbas];
+  std::vector<double> cart, sph;
+  for (int i = 0; i < nbas; ++i)
+    for (int j = 0; j < nbas; ++j) {
+      const Shell a = shell_of(i, atm, bas, env), b = shell_of(j, atm, bas, env);
+      cart.resize((size_t)ncart(a.l) * a.nctr * ncart(b.l) * b.nctr);
+      int1e_block(cart.data(), typec, a, b, atm, natm, env);
+      const double *blk = cart.data();
+      if (coord == 1) {
+        sph.resize((size_t)nsph(a.l) * a.nctr * nsph(b.l) * b.nctr);
+        cart2sph_2(sph.data(), cart.data(), a, b);
+        blk = sph.data();
+      }
+      const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
+      for (int J = 0; J < dj; ++J)
+        for (int I = 0; I < di; ++I) out[(size_t)(off[i] + I) * n + off[j] + J] = blk[I + di * J];
+    }
+}
+
+void orc_fock_G(double *G, const double *P, int coord, const int *atm, int, const int *bas,
+                int nbas, const double *env, int nthreads) {
+  const std::vector<int> off = shell_offsets(coord, bas, nbas);
+  const size_t n = off[nbas];
+  std::memset(G, 0, n * n * sizeof(double));
+  const int nt = threads_or_default(nthreads);
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<double> Gl(n * n, 0.0), buf;
+#pragma omp for schedule(dynamic) collapse(2)
+    for (int i = 0; i < nbas; ++i)
+      for (int j = 0; j < nbas; ++j)
+        for (int k = 0; k < nbas; ++k)
+          for (int l = 0; l < nbas; ++l) {
+            const int shls[4] = {i, j, k, l};
+            const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
+            const int dk = off[k + 1] - off[k], dl = off[l + 1] - off[l];
+            buf.resize((size_t)di * dj * dk * dl);
+            quartet_block(buf.data(), coord, shls, atm, bas, env);
+            size_t c = 0;
+            // slot (mu nu | sig lam): G[mu,nu] += P[lam,sig] v; G[mu,lam] -= P[nu,sig] v / 2
+            // (src/scf.rs:379-391)
+            for (int L = 0; L < dl; ++L)
+              for (int K = 0; K < dk; ++K)
+                for (int J = 0; J < dj; ++J)
+                  for (int I = 0; I < di; ++I, ++c) {
+                    const size_t mu = off[i] + I, nu = off[j] + J, sg = off[k] + K, lm = off[l] + L;
+                    const double v = buf[c];
+                    Gl[mu * n + nu] += P[lm * n + sg] * v;
+                    Gl[mu * n + lm] += -0.5 * P[nu * n + sg] * v;
+                  }
+          }
+#pragma omp critical
+    for (size_t x = 0; x < n * n; ++x) G[x] += Gl[x];
+  }
+}
+
+int orc_density(double *Pout, size_t nelec, int imax, double conv, const int *atm, int natm,
+                const int *bas, int nbas, const double *env, int nthreads, int *iters) {
+  const int n = orc_nao(0, bas, nbas);
+  const size_t nn = (size_t)n * n;
+  std::vector<double> S(nn), T(nn), V(nn), H(nn), G(nn);
+  orc_int1e(S.data(), 0, 0, atm, natm, bas, nbas, env);
+  orc_int1e(T.data(), 0, 1, atm, natm, bas, nbas, env);
+  orc_int1e(V.data(), 0, 2, atm, natm, bas, nbas, env);
+  for (size_t x = 0; x < nn; ++x) H[x] = T[x] + V[x];
+  // find_X (src/scf.rs:607-649): X = U s^-1/2, refuse s_min < 1e-8
+  std::vector<double> s, U;
+  eigh(n, S, s, U);
+  if (s[0] < 1e-8) return 1;
+  std::vector<double> X(nn), Xt(nn);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) X[(size_t)r * n + c] = U[(size_t)r * n + c] / std::sqrt(s[c]);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) Xt[(size_t)c * n + r] = X[(size_t)r * n + c];
+  // P = I (src/scf.rs:757-764); plain Roothaan iteration (src/scf.rs:774-784)
+  std::vector<double> P(nn, 0.0), Pold;
+  for (int i = 0; i < n; ++i) P[(size_t)i * n + i] = 1.0;
+  double delta = 1.0;
+  int it = 0;
+  while (delta > conv && it < imax) {
+    Pold = P;
+    orc_fock_G(G.data(), P.data(), 0, atm, natm, bas, nbas, env, nthreads);
+    std::vector<double> F(nn);
+    for (size_t x = 0; x < nn; ++x) F[x] = H[x] + G[x];
+    std::vector<double> Fp = matmul(n, matmul(n, Xt, F), X);
+    std::vector<double> e, Uf;
+    eigh(n, Fp, e, Uf);
+    std::vector<double> C = matmul(n, X, Uf);
+    std::fill(P.begin(), P.end(), 0.0);
+    for (int mu = 0; mu < n; ++mu)
+      for (int nu = 0; nu < n; ++nu) {
+        double v = 0.0;
+        for (size_t i = 0; i < nelec / 2; ++i) v += 2.0 * C[(size_t)mu * n + i] * C[(size_t)nu * n + i];
+        P[(size_t)mu * n + nu] = v;
+      }
+    double d = 0.0;
+    for (size_t x = 0; x < nn; ++x) d += (P[x] - Pold[x]) * (P[x] - Pold[x]);
+    delta = std::sqrt(d) / 2.0;
+    ++it;
+  }
+  if (iters) *iters = it;
+  if (delta > conv) return 2;
+  // check_density (src/scf.rs:572-600)
+  double tr = 0.0;
+  for (int mu = 0; mu < n; ++mu)
+    for (int nu = 0; nu < n; ++nu) tr += P[(size_t)mu * n + nu] * S[(size_t)nu * n + mu];
+  if (std::fabs(tr - (double)nelec) > 1e-6) return 3;
+  std::vector<double> PSP = matmul(n, matmul(n, P, S), P);
+  double idem = 0.0;
+  for (size_t x = 0; x < nn; ++x) idem = std::max(idem, std::fabs(PSP[x] - 2.0 * P[x]));
+  if (idem > 1e-6) return 3;
+  std::memcpy(Pout, P.data(), nn * sizeof(double));
+  return 0;
+}
+
+double orc_energy(const double *P, const int *atm, int natm, const int *bas, int nbas,
+                  const double *env, int nthreads) {
+  // energyfast (src/scf.rs:827-956): sum P (T+V) + 1/2 sum P G(P) + E_nn
+  const int n = orc_nao(0, bas, nbas);
+  const size_t nn = (size_t)n * n;
+  std::vector<double> T(nn), V(nn), G(nn);
+  orc_int1e(T.data(), 0, 1, atm, natm, bas, nbas, env);
+  orc_int1e(V.data(), 0, 2, atm, natm, bas, nbas, env);
+  orc_fock_G(G.data(), P, 0, atm, natm, bas, nbas, env, nthreads);
+  double e1 = 0.0, e2 = 0.0;
+  for (size_t x = 0; x < nn; ++x) {
+    e1 += P[x] * (T[x] + V[x]);
+    e2 += 0.5 * P[x] * G[x];
+  }
+  return e1 + e2 + nuclear_repulsion(atm, natm, env);
+}
+
+double orc_scf(size_t nelec, int imax, double conv, const int *atm, int natm, const int *bas,
+               int nbas, const double *env, int nthreads) {
+  const int n = orc_nao(0, bas, nbas);
+  std::vector<double> P((size_t)n * n);
+  if (orc_density(P.data(), nelec, imax, conv, atm, natm, bas, nbas, env, nthreads, nullptr) != 0)
+    return NAN;
+  return orc_energy(P.data(), atm, natm, bas, nbas, env, nthreads);
+}
+
+}  // extern "C"

@@ -1,0 +1,207 @@
+"""Generate the golden fixtures from the reference's own shipped library.
+
+The reference (librint) is a Rust crate that cannot be compiled here (no
+cargo/rustc, nightly Enzyme toolchain).  Its repository ships a prebuilt
+``python/librint/librint.so``; this script *calls* it through ctypes, exactly
+as ``python/librint/_bindings.py`` does, and stores the results as small
+``.npz`` fixtures next to this file.  The library is never inspected; only
+its exported C entry points are called (src/p2c.rs documents them).
+
+Notes on that binary, found while generating:
+* it predates the current source: it has no ``free_c`` (buffers are released
+  with libc ``free``, which is the Rust system allocator's ``free``);
+* for CH4/STO-3G its ``scf_c`` returns the non-variational fixed point
+  -40.3052 Eh that src/scf.rs:568-571 describes as fixed (the current source
+  rejects it; the true RHF energy is -39.7269);
+* for HF and C6H6 at conv 1e-10 its plain Roothaan loop does not converge and
+  it returns a finite number instead of NaN.
+Such values are stored under ``*_known_bad`` keys and are not goldens.
+
+Run (needs the reference checkout, only in the development container):
+    python tests/golden/make_golden.py [/path/to/reference]
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from librint_b200 import synthetic  # noqa: E402
+from librint_b200.basis import Molecule, read_molecule  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+P = ctypes.POINTER
+
+
+def load_ref():
+    lib = ctypes.CDLL(os.path.join(REF, "python", "librint", "librint.so"))
+    a6 = (P(ctypes.c_int), ctypes.c_size_t, P(ctypes.c_int), ctypes.c_size_t,
+          P(ctypes.c_double), ctypes.c_size_t)
+    lib.int2e_c.argtypes = a6 + (ctypes.c_int,)
+    lib.int2e_c.restype = ctypes.c_void_p
+    lib.int1e_c.argtypes = a6 + (ctypes.c_int, ctypes.c_int)
+    lib.int1e_c.restype = ctypes.c_void_p
+    lib.scf_c.argtypes = a6 + (ctypes.c_size_t, ctypes.c_int, ctypes.c_double)
+    lib.scf_c.restype = ctypes.c_double
+    lib.density_c.argtypes = a6 + (ctypes.c_size_t, ctypes.c_int, ctypes.c_double)
+    lib.density_c.restype = ctypes.c_void_p
+    lib.energy_c.argtypes = a6 + (P(ctypes.c_double), ctypes.c_size_t)
+    lib.energy_c.restype = ctypes.c_double
+    for f in ("danalytical_c", "dS_c", "dHcore_c", "dR_c"):
+        getattr(lib, f).argtypes = a6 + (P(ctypes.c_double), ctypes.c_size_t)
+        getattr(lib, f).restype = ctypes.c_void_p
+    return lib
+
+
+LIBC = ctypes.CDLL("libc.so.6")
+LIBC.free.argtypes = (ctypes.c_void_p,)
+
+
+def _args(m: Molecule):
+    atm = np.ascontiguousarray(m.atm, dtype=np.int32)
+    bas = np.ascontiguousarray(m.bas, dtype=np.int32)
+    env = np.ascontiguousarray(m.env, dtype=np.float64)
+    m._keep = (atm, bas, env)
+    return (atm.ctypes.data_as(P(ctypes.c_int)), atm.size, bas.ctypes.data_as(P(ctypes.c_int)),
+            bas.size, env.ctypes.data_as(P(ctypes.c_double)), env.size)
+
+
+def _take(ptr, n):
+    if not ptr:
+        return None
+    a = np.ctypeslib.as_array(ctypes.cast(ptr, P(ctypes.c_double)), shape=(n,)).copy()
+    LIBC.free(ptr)
+    return a
+
+
+# Runs where the shipped binary is known to fail (observed when this script
+# was written; the current reference source fixes both failure modes):
+#   ch4: non-variational fixed point (-40.3052 Eh instead of -39.7269);
+#   hf, c6h6 at conv 1e-10: prints "did not converge" and returns a finite,
+#   meaningless energy instead of NaN.
+# (h4 converges to a different self-consistent solution than the oracle's
+# lower one -- square H4 has a degenerate pair -- so its densities are stored
+# and the energy functional is compared at the reference density.)
+KNOWN_BAD = {"ch4/sto3g": ("scf", "scf6"), "hf/sto3g": ("scf",), "c6h6/sto3g": ("scf",)}
+
+
+def grad_len(m: Molecule) -> int:
+    """Length of env[s1:s2] (src/utils.rs:152-175 ``split``)."""
+    b = m.bas.reshape(-1, 8)
+    s1 = int(b[:, 5].min())
+    s2 = int((b[:, 6] + b[:, 2]).max())
+    return s2 - s1
+
+
+def mol_arrays(prefix, m):
+    return {f"{prefix}/atm": m.atm, f"{prefix}/bas": m.bas, f"{prefix}/env": m.env}
+
+
+def main():
+    lib = load_ref()
+    rng = np.random.default_rng(20261203)
+    out = {}
+
+    # --- reference fixture molecules -------------------------------------
+    names = ["h2/sto3g", "h4/sto3g", "lih/sto3g", "hf/sto3g", "h2o/sto3g", "h2o/def2svp",
+             "nh3/sto3g", "ch4/sto3g", "c/sto3g", "O/sto3g", "c6h6/sto3g"]
+    for name in names:
+        m = read_molecule(os.path.join(REF, "molecules", name + ".txt"))
+        key = "mol/" + name
+        out.update(mol_arrays(key, m))
+        for coord in (0, 1):
+            n = m.nao(coord)
+            for typec in (0, 1, 2):
+                out[f"{key}/int1e_{coord}{typec}"] = _take(lib.int1e_c(*_args(m), coord, typec),
+                                                           n * n).reshape(n, n)
+            if n <= 16:
+                t = _take(lib.int2e_c(*_args(m), coord), n ** 4)
+                out[f"{key}/int2e_{coord}"] = t.reshape(n, n, n, n)
+            elif n <= 40:
+                t = _take(lib.int2e_c(*_args(m), coord), n ** 4)
+                idx = np.sort(rng.choice(n ** 4, size=20000, replace=False))
+                out[f"{key}/int2e_{coord}_idx"] = idx
+                out[f"{key}/int2e_{coord}_val"] = t[idx]
+        for tag, conv in (("scf", 1e-10), ("scf6", 1e-6)):
+            e = lib.scf_c(*_args(m), m.nelec, 2000, conv)
+            bad = KNOWN_BAD.get(name, ())
+            out[f"{key}/{tag}_known_bad" if tag in bad else f"{key}/{tag}"] = e
+            if tag not in bad:
+                n0 = m.nao(0)
+                out[f"{key}/{tag}_P"] = _take(lib.density_c(*_args(m), m.nelec, 2000, conv),
+                                              n0 * n0).reshape(n0, n0)
+            print(name, "nao", m.nao(0), tag, "E", e, flush=True)
+
+    # --- C1 water-like --------------------------------------------------
+    m = synthetic.water_like()
+    out.update(mol_arrays("water_like", m))
+    for coord in (0, 1):
+        n = m.nao(coord)
+        out[f"water_like/int2e_{coord}"] = _take(lib.int2e_c(*_args(m), coord), n ** 4).reshape(
+            n, n, n, n)
+        for typec in (0, 1, 2):
+            out[f"water_like/int1e_{coord}{typec}"] = _take(
+                lib.int1e_c(*_args(m), coord, typec), n * n).reshape(n, n)
+    out["water_like/scf"] = lib.scf_c(*_args(m), m.nelec, 2000, 1e-10)
+    print("water_like E", out["water_like/scf"], flush=True)
+
+    # --- frozen-density gradients (Enzyme, form 2 checks) -----------------
+    for key, m in (("h2", read_molecule(os.path.join(REF, "molecules/h2/sto3g.txt"))),
+                   ("h2o", read_molecule(os.path.join(REF, "molecules/h2o/sto3g.txt"))),
+                   ("water_like", synthetic.water_like())):
+        n = m.nao(0)
+        Pp = lib.density_c(*_args(m), m.nelec, 2000, 1e-10)
+        Pm = _take(Pp, n * n)
+        out[f"grad/{key}/P"] = Pm.reshape(n, n)
+        out.update(mol_arrays(f"grad/{key}", m))
+        Pc = np.ascontiguousarray(Pm)
+        ng = grad_len(m)
+        for f in ("danalytical_c", "dS_c", "dHcore_c", "dR_c"):
+            r = getattr(lib, f)(*_args(m), Pc.ctypes.data_as(P(ctypes.c_double)), Pc.size)
+            out[f"grad/{key}/{f}"] = _take(r, ng)
+        out[f"grad/{key}/energy"] = lib.energy_c(*_args(m), Pc.ctypes.data_as(P(ctypes.c_double)),
+                                                 Pc.size)
+        print("grad", key, flush=True)
+
+    # --- per-class quartets from the ERI sweep distribution ----------------
+    classes = synthetic.canonical_classes(2)
+    nsamp = 6
+    for cls in classes:
+        mol, shls = synthetic.eri_sweep(cls, nsamp, seed=902)
+        b = mol.bas.reshape(-1, 8)
+        a = mol.atm.reshape(-1, 6)
+        blocks = {0: [], 1: []}
+        subs = []
+        for q in range(nsamp):
+            sh = shls[q]
+            # 4-atom, 4-shell molecule holding just this quartet
+            sub_atm = a[b[sh, 0]].copy()
+            sub_bas = b[sh].copy()
+            sub_bas[:, 0] = np.arange(4)
+            sm = Molecule(sub_atm.ravel(), sub_bas.ravel(), mol.env, 0)
+            subs.append((sub_atm, sub_bas))
+            for coord in (0, 1):
+                d = [((l + 1) * (l + 2) // 2 if coord == 0 else 2 * l + 1) for l in cls]
+                n = sum(d)
+                t = _take(lib.int2e_c(*_args(sm), coord), n ** 4).reshape(n, n, n, n)
+                o = np.cumsum([0] + d)
+                blocks[coord].append(t[o[0]:o[1], o[1]:o[2], o[2]:o[3], o[3]:o[4]].copy())
+        key = "cls/%d%d%d%d" % cls
+        out[f"{key}/atm"] = np.stack([s[0] for s in subs])
+        out[f"{key}/bas"] = np.stack([s[1] for s in subs])
+        out[f"{key}/env"] = mol.env
+        out[f"{key}/cart"] = np.stack(blocks[0])
+        out[f"{key}/sph"] = np.stack(blocks[1])
+        print("class", cls, flush=True)
+
+    np.savez_compressed(os.path.join(HERE, "reference_golden.npz"), **out)
+    print("wrote", os.path.join(HERE, "reference_golden.npz"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,125 @@
+"""Pins of the CPU oracle: golden vectors from the reference's own shipped
+library (tests/golden/make_golden.py), the energy truths of the reference's
+checks/truth directory, and 60-digit Rys rules."""
+import numpy as np
+import pytest
+
+import oracle
+from librint_b200.basis import Molecule
+from librint_b200 import synthetic
+from tests.conftest import assert_eri_close
+
+MOLS = ["h2/sto3g", "h4/sto3g", "lih/sto3g", "hf/sto3g", "h2o/sto3g", "h2o/def2svp",
+        "nh3/sto3g", "ch4/sto3g", "c/sto3g", "O/sto3g", "c6h6/sto3g"]
+
+
+def mol(golden, key):
+    return Molecule(golden[key + "/atm"], golden[key + "/bas"], golden[key + "/env"],
+                    int(golden[key + "/atm"].reshape(-1, 6)[:, 0].sum()))
+
+
+@pytest.mark.parametrize("name", MOLS)
+def test_int1e_vs_reference(golden, name):
+    m = mol(golden, "mol/" + name)
+    for coord in (0, 1):
+        for typec in (0, 1, 2):
+            ref = golden[f"mol/{name}/int1e_{coord}{typec}"]
+            got = oracle.int1e(m, typec, coord)
+            np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", MOLS)
+def test_int2e_vs_reference(golden, name):
+    m = mol(golden, "mol/" + name)
+    for coord in (0, 1):
+        k = f"mol/{name}/int2e_{coord}"
+        if k in golden:
+            assert_eri_close(oracle.int2e_tensor(m, coord), golden[k], what=k)
+        elif k + "_idx" in golden:
+            t = oracle.int2e_tensor(m, coord).ravel()
+            idx = golden[k + "_idx"]
+            assert_eri_close(t[idx], golden[k + "_val"], what=k)
+
+
+def test_water_like_vs_reference(golden):
+    m = synthetic.water_like()
+    np.testing.assert_array_equal(m.env, golden["water_like/env"])
+    for coord in (0, 1):
+        assert_eri_close(oracle.int2e_tensor(m, coord), golden[f"water_like/int2e_{coord}"])
+    e = oracle.scf(m, conv=1e-10, imax=500)
+    assert abs(e - golden["water_like/scf"]) < 1e-10
+
+
+@pytest.mark.parametrize("cls", synthetic.canonical_classes(2))
+def test_class_quartets_vs_reference(golden, cls):
+    key = "cls/%d%d%d%d" % cls
+    env = golden[key + "/env"]
+    for q in range(golden[key + "/atm"].shape[0]):
+        m = Molecule(golden[key + "/atm"][q].ravel(), golden[key + "/bas"][q].ravel(), env)
+        for coord, nm in ((0, "cart"), (1, "sph")):
+            got, _ = oracle.int2e_block(m, [0, 1, 2, 3], coord)
+            assert_eri_close(got, golden[f"{key}/{nm}"][q], what=f"{key} q{q} {nm}")
+
+
+# square H4 has two self-consistent RHF solutions; the reference lands on the
+# higher one (-1.778112), the oracle on the lower (-1.778348).  Its energy
+# functional is pinned below at the reference density instead.
+SCF_SAME_FIXED_POINT = [n for n in MOLS if n not in ("c6h6/sto3g", "h4/sto3g")]
+
+
+@pytest.mark.parametrize("name", MOLS)
+def test_energy_functional_at_reference_density(golden, name):
+    m = mol(golden, "mol/" + name)
+    for tag in ("scf", "scf6"):
+        if f"mol/{name}/{tag}_P" in golden:
+            e = oracle.energy(m, golden[f"mol/{name}/{tag}_P"])
+            assert abs(e - golden[f"mol/{name}/{tag}"]) < 1e-10, (name, tag)
+
+
+@pytest.mark.parametrize("name", SCF_SAME_FIXED_POINT)
+def test_scf_energy_vs_reference(golden, name):
+    m = mol(golden, "mol/" + name)
+    e = oracle.scf(m, conv=1e-10, imax=1000)
+    if f"mol/{name}/scf" in golden:
+        assert abs(e - golden[f"mol/{name}/scf"]) < 1e-10, (e, golden[f"mol/{name}/scf"])
+    if f"mol/{name}/scf6" in golden:
+        assert abs(e - golden[f"mol/{name}/scf6"]) < 1e-9
+
+
+def test_energy_truths(golden):
+    """checks/truth/h2/sto3g_E.txt and checks/truth/h2o/sto3g_E.txt: P from
+    density(conv=1e-6) then the energy (checks/energy.rs:182-196)."""
+    for name, truth in (("h2/sto3g", -0.8817324499460562), ("h2o/sto3g", -74.96102664501196)):
+        m = mol(golden, "mol/" + name)
+        P, _ = oracle.density(m, conv=1e-6, imax=1000)
+        assert abs(oracle.energy(m, P) - truth) < 1e-10
+
+
+def test_ch4_true_minimum(golden):
+    """The shipped binary returns the non-variational -40.3052 Eh for CH4; the
+    reference source (src/scf.rs:568-571) names -39.727 as the true energy."""
+    m = mol(golden, "mol/ch4/sto3g")
+    e = oracle.scf(m, conv=1e-10, imax=1000)
+    assert abs(e - (-39.727)) < 1e-3
+    assert abs(golden["mol/ch4/sto3g/scf_known_bad"] - (-40.305)) < 1e-3
+
+
+def test_rys_tables_vs_exact():
+    """Oracle roots/weights (the shared tables) vs 60-digit Gauss rules."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(__file__)),
+                                    "librint_b200", "csrc"))
+    import gen_rys_tables as gen
+    from mpmath import mpf
+    rng = np.random.default_rng(7)
+    for n in range(1, 10):
+        xs = np.concatenate([[0.0, 1e-9, 3e-7, 42.9 + 5 * n, 43.0 + 5 * n, 200.0],
+                             rng.uniform(0, 45 + 5 * n, 6)])
+        for x in xs:
+            u, w = oracle.rys_roots(n, x)
+            ue, we = gen.rys_rule(n, mpf(float(x)))
+            ue = np.array([float(v) for v in ue])
+            we = np.array([float(v) for v in we])
+            np.testing.assert_allclose(u, ue, rtol=4e-15, err_msg=f"n={n} x={x}")
+            np.testing.assert_allclose(w, we, rtol=4e-15, err_msg=f"n={n} x={x}")
