@@ -1,0 +1,382 @@
+"""Benchmark: Rys ERI sweep, shell quartets per second (FP64).
+
+Workload: 21 angular classes (ss|ss) .. (dd|dd), ``--nq`` independent shell
+quartets per class (default 2^20), every shell with its own centre uniform in
+a 10 A cube, 1..6 primitives, exponents log-uniform in [0.05, 5000],
+spherical output (seeded synthetic data of that distribution; no dataset).
+One step = one pass of the batched ERI path over all 21 classes with inputs
+resident in HBM.  Outputs (18 GB per step at 2^20) exceed the 126 MB L2, so
+no explicit L2 flush is needed between steps.
+
+Arms:
+  default          the CUDA library (librint_b200), one process per GPU;
+                   with torchrun each rank runs its own shard (weak scaling).
+  --impl reference the reference algorithm on the host cores (the CPU
+                   restatement in oracle/, since the Rust reference cannot be
+                   built here), rank 0 only, on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from librint_b200 import synthetic  # noqa: E402
+
+CLASSES = synthetic.canonical_classes(2)
+METRIC = "ERI shell quartets/s (FP64 Rys sweep, (ss|ss)..(dd|dd), K=1..6, spherical)"
+UNIT = "quartets/s"
+
+
+# ------------------------------------------------------------ workload
+def _gen(args):
+    cls, nq, seed = args
+    m, shls = synthetic.eri_sweep(cls, nq, seed=seed)
+    return cls, m.atm, m.bas, m.env, shls
+
+
+def generate(nq, seed, procs):
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(procs, len(CLASSES))) as pool:
+        return pool.map(_gen, [(c, nq, seed) for c in CLASSES])
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def nsph(l):
+    return 2 * l + 1
+
+
+def class_flops_bytes(cls, bas, shls):
+    """Fixed algorithmic FLOP / byte convention per shell quartet.
+
+    F = P [50 + n_r (64 + 15 (nmax+1)(mmax+1) + 6 H + 3 nf)] + C2S with
+    P = Ki Kj Kk Kl (unscreened), n_r = L/2 + 1, nmax = li+lj, mmax = lk+ll,
+    nf = prod ncart, H = sum_{i=1..li}(nmax-i+1)(mmax+1) + (lj+1)(li+1)
+    sum_{k=1..lk}(mmax-k+1), C2S = 2 [nsi nci ncj nck ncl + nsj ncj nsi nck ncl
+    + nsk nck nsi nsj ncl + nsl ncl nsi nsj nsk];
+    B = 8 prod ns written + 8 sum_shells (3 + 2K) read.
+    """
+    li, lj, lk, ll = cls
+    nmax, mmax = li + lj, lk + ll
+    nr = (nmax + mmax) // 2 + 1
+    nf = ncart(li) * ncart(lj) * ncart(lk) * ncart(ll)
+    H = sum((nmax - i + 1) * (mmax + 1) for i in range(1, li + 1)) + \
+        (lj + 1) * (li + 1) * sum(mmax - k + 1 for k in range(1, lk + 1))
+    nc = [ncart(l) for l in cls]
+    ns = [nsph(l) for l in cls]
+    c2s = 2 * (ns[0] * nc[0] * nc[1] * nc[2] * nc[3] + ns[1] * nc[1] * ns[0] * nc[2] * nc[3] +
+               ns[2] * nc[2] * ns[0] * ns[1] * nc[3] + ns[3] * nc[3] * ns[0] * ns[1] * ns[2])
+    per_prim = 50 + nr * (64 + 15 * (nmax + 1) * (mmax + 1) + 6 * H + 3 * nf)
+    k = bas.reshape(-1, 8)[:, 2].astype(np.float64)[shls]          # (nq, 4)
+    P = k.prod(axis=1)
+    flops = float((P * per_prim + c2s).sum())
+    nbytes = float(8 * np.prod(ns) * shls.shape[0] + 8 * (3 + 2 * k).sum())
+    return flops, nbytes
+
+
+# ------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU arms
+def cpu_sample(data, sample, threads):
+    """Oracle on the first `sample` quartets of every class; (quartets/s, s)."""
+    import oracle
+    from librint_b200.basis import Molecule
+    tot_q, tot_t = 0, 0.0
+    for cls, atm, bas, env, shls in data:
+        m = Molecule(atm, bas, env)
+        sh = np.ascontiguousarray(shls[:sample])
+        t0 = time.perf_counter()
+        oracle.int2e_batch(m, sh, 1, nthreads=threads)
+        tot_t += time.perf_counter() - t0
+        tot_q += sh.shape[0]
+    return tot_q / tot_t, tot_t
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def pick_sample(data, threads, budget_s=8.0):
+    """Sample size per class so one oracle pass takes about budget_s."""
+    probe = 16
+    _, t = cpu_sample(data, probe, threads)
+    s = int(probe * budget_s / max(t, 1e-3))
+    return max(16, min(s, data[0][4].shape[0]))
+
+
+# ------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--nq", type=int, default=1 << 20, help="quartets per class per rank")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = host_threads()
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world, threads)
+
+    # inputs generated on the host before any CUDA call (spawn pool)
+    data = generate(args.nq, 2 + 1000 * rank, procs=max(1, threads // max(world, 1)))
+
+    import torch
+    import torch.distributed as dist
+    from librint_b200 import _bindings as B
+    from librint_b200 import eri
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", world_size=world, rank=rank,
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    L = B.lib()
+
+    # device-resident inputs and outputs
+    dev_data = []
+    flops, nbytes = {}, {}
+    for cls, atm, bas, env, shls in data:
+        from librint_b200.basis import Molecule
+        n = eri.batch_len(Molecule(atm, bas, env), shls, 1)
+        t = dict(cls=cls, atm=torch.from_numpy(atm).to(dev), bas=torch.from_numpy(bas).to(dev),
+                 env=torch.from_numpy(env).to(dev), shls=torch.from_numpy(shls).to(dev),
+                 out=torch.empty(n, dtype=torch.float64, device=dev))
+        dev_data.append(t)
+        flops[cls], nbytes[cls] = class_flops_bytes(cls, bas, shls)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        for t in dev_data:
+            eri.int2e_batch_device(t["out"], 1, t["shls"], t["atm"], t["bas"], t["env"], stream)
+
+    fp64_peak = L.lrb_fp64_peak_probe(300)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    phys = vis.split(",")[local] if vis and vis.split(",")[local].strip().isdigit() else str(local)
+    sampler = ClockSampler(phys)
+    L.lrb_profile_read((__import__("ctypes").c_double * 64)(), 64)
+    L.lrb_profile_enable(1)
+    n0 = L.lrb_launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    L.lrb_profile_enable(0)
+    launches = L.lrb_launch_count() - n0
+    ms_arr = (__import__("ctypes").c_double * 64)()
+    L.lrb_profile_read(ms_arr, 64)
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    if world > 1:
+        tt = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    nq_total = world * len(CLASSES) * args.nq * args.steps
+    value = nq_total / elapsed
+
+    # dominant kernel: the class with the largest share of kernel time
+    cls_ms = {cls: ms_arr[i] / args.steps for i, cls in enumerate(CLASSES)}
+    top = max(cls_ms, key=cls_ms.get)
+    top_ms = cls_ms[top]
+    achieved_tf = flops[top] / (top_ms * 1e-3) / 1e12
+    total_kernel_ms = sum(cls_ms.values())
+
+    # end to end through the host API (pinned host buffers, copies timed)
+    e2e = None
+    if args.e2e_steps > 0:
+        from librint_b200.basis import Molecule
+        host = []
+        h2d = d2h = 0
+        for (cls, atm, bas, env, shls), t in zip(data, dev_data):
+            pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+            out = torch.empty(t["out"].numel(), dtype=torch.float64).pin_memory()
+            host.append((pin(atm), pin(bas), pin(env), pin(shls), out))
+            h2d += atm.nbytes + bas.nbytes + env.nbytes + shls.nbytes
+            d2h += out.numel() * 8
+        P_i, P_d = B.P_i, B.P_d
+        import ctypes
+
+        def e2e_step():
+            for (a, b, e, s, o) in host:
+                rc = L.lrb_int2e_batch(ctypes.cast(o.data_ptr(), P_d), 1,
+                                       ctypes.cast(s.data_ptr(), P_i), s.numel() // 4,
+                                       ctypes.cast(a.data_ptr(), P_i), a.numel() // 6,
+                                       ctypes.cast(b.data_ptr(), P_i), b.numel() // 8,
+                                       ctypes.cast(e.data_ptr(), P_d), e.numel())
+                B.check(rc, "lrb_int2e_batch")
+        e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([te], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": world * len(CLASSES) * args.nq * args.e2e_steps / te, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "note": "lrb_int2e_batch with pinned host buffers; all 21 classes per step"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        s = pick_sample(data, threads)
+        v, tcpu = cpu_sample(data, s, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"first {s} quartets of each of the 21 classes of the same workload "
+                         f"({21 * s} quartets, {tcpu:.1f} s), oracle/ C++ restatement, "
+                         f"OpenMP over quartets"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded, distribution of the ERI sweep config)",
+            "config": {"workload": "ERI sweep: 21 classes (ss|ss)..(dd|dd) x %d quartets per "
+                                   "class per GPU, K=1..6, exponents log-uniform [0.05,5000], "
+                                   "centres in a 10 A cube, spherical output" % args.nq,
+                       "quartets_per_step": len(CLASSES) * args.nq * world,
+                       "l2": "outputs (%.1f GB/step) exceed L2; no flush needed" %
+                             (sum(t['out'].numel() for t in dev_data) * 8 / 1e9),
+                       "parallelism": f"dp{world} (independent quartet shards)"},
+            "roofline": {"bound": "fp64", "kernel": "k_eri_out<%d,%d,%d,%d>" % top,
+                         "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": achieved_tf / fp64_peak if fp64_peak > 0 else None,
+                         "peak_source": "measured FP64 FMA probe (lrb_fp64_peak_probe) on this "
+                                        "GPU; MEASURED_PEAKS.json has no FP64 figure",
+                         "kernel_ms": top_ms, "kernel_share": top_ms / total_kernel_ms,
+                         "flop_convention": "fixed per-quartet count, see class_flops_bytes",
+                         "traffic": None},
+            "class_kernel_ms": {"%d%d%d%d" % c: round(v, 4) for c, v in cls_ms.items()},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world, threads):
+    if rank != 0:
+        return
+    data = generate(1 << 16, 2, procs=threads)
+    s = pick_sample(data, threads)
+    for _ in range(args.warmup):
+        cpu_sample(data, max(16, s // 8), threads)
+    vals, tt = [], 0.0
+    for _ in range(args.steps):
+        v, t = cpu_sample(data, s, threads)
+        vals.append(v)
+        tt += t
+    value = len(vals) * 21 * s / tt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, distribution of the ERI sweep config)",
+        "config": {"workload": "ERI sweep: 21 classes (ss|ss)..(dd|dd), bounded sample of "
+                               "%d quartets per class per step" % s},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{s} quartets per class per step; the reference (Rust) "
+                                   f"cannot be built here, so its CPU restatement in oracle/ "
+                                   f"runs with OpenMP over quartets"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

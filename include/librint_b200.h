@@ -1,0 +1,106 @@
+/* librint_b200: B200 (sm_100a) Rys-quadrature ERIs and RHF Fock builds behind
+ * librint's C ABI.
+ *
+ * Array conventions are librint's / libcint's: atm has 6 int32 slots per atom,
+ * bas 8 int32 slots per shell, env is the float64 pool they index into
+ * (reference src/p2c.rs:1-15).  coord = 0 cartesian, 1 spherical.
+ * Matrices are row-major n x n in AO order; ERI blocks are column-major
+ * (i fastest) like libcint.
+ *
+ * Errors: entry points of this library's own API return a status code
+ * (LRB_OK or a negative LRB_ERR_*); lrb_last_error() describes the last
+ * failure on the calling thread.  The reference-shaped entry points keep the
+ * reference's in-band conventions (NULL / NaN) and never exit the process.
+ */
+#ifndef LIBRINT_B200_H
+#define LIBRINT_B200_H
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define LRB_API __attribute__((visibility("default")))
+#else
+#define LRB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LRB_OK 0
+#define LRB_ERR_INPUT (-1)
+#define LRB_ERR_UNSUPPORTED (-2)
+#define LRB_ERR_ALLOC (-3)
+#define LRB_ERR_CUDA (-4)
+#define LRB_ERR_SCF (-5)
+#define LRB_ERR_TIMEOUT (-6)
+
+/* Text of the last error on this thread ("" if none). */
+LRB_API const char *lrb_last_error(void);
+
+/* ---------------------------------------------------------------------
+ * Batched shell-quartet ERIs -- the GPU entry for the per-quartet loops of
+ * src/scf.rs:102-118 (Basis::int2e) and src/scf.rs:253-307 (integral2e),
+ * each iteration of which calls cint2e_sph / cint2e_cart
+ * (src/cint2e.rs:2896, 2938).
+ *
+ * shls holds nq quartets (4 shell indices each).  Every quartet's block is
+ * written in libcint layout (out[i + ni*(j + nj*(k + nk*l))]) and the blocks
+ * are packed back to back in quartet order; lrb_int2e_batch_len gives the
+ * total length in doubles.  Shells: l <= 2, 1..31 primitives, nctr == 1.
+ * Screening is the reference's (expcutoff 60, src/cint2e.rs:367-393).
+ * -------------------------------------------------------------------*/
+LRB_API long long lrb_int2e_batch_len(int coord, const int *shls, long long nq, const int *bas, int nbas);
+
+/* Host pointers; copies in, computes on the current device, copies out. */
+LRB_API int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const int *atm,
+                    int natm, const int *bas, int nbas, const double *env, long long nenv);
+
+/* Device pointers; asynchronous on `stream` (a cudaStream_t, NULL = legacy
+ * default stream).  Returns after the work is queued. */
+LRB_API int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq,
+                           const int *atm, int natm, const int *bas, int nbas,
+                           const double *env, long long nenv, void *stream);
+
+/* Measurement hooks (no reference counterpart).  While enabled, every ERI
+ * class kernel is bracketed by CUDA events on its stream; lrb_profile_read
+ * adds the milliseconds per class id (canonical order (ss|ss), (ps|ss),
+ * (ps|ps), (pp|ss), ... (dd|dd)) into ms[0..n) and returns the number of
+ * kernels harvested.  lrb_launch_count counts this library's kernel
+ * launches; lrb_fp64_peak_probe measures FP64 FMA throughput (TFLOP/s). */
+LRB_API void lrb_profile_enable(int on);
+LRB_API int lrb_profile_read(double *ms, int n);
+LRB_API long long lrb_launch_count(void);
+LRB_API double lrb_fp64_peak_probe(int ms);
+
+/* ---------------------------------------------------------------------
+ * libcint per-quartet ABI (src/cint2e.rs:2896 int2e_sph, :2938 int2e_cart,
+ * :2927 int2e_optimizer; src/optimizer.rs:81 CINTdel_optimizer).
+ * out == NULL returns the scratch size in doubles (this implementation
+ * needs none and returns the block size); dims == NULL means a packed
+ * block; cache is ignored.  Returns 1 if the block is non-zero, else 0.
+ * An optimizer keeps device copies of atm/bas/env for later calls.
+ * -------------------------------------------------------------------*/
+typedef struct LrbCintOpt CINTOpt;
+LRB_API int int2e_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+              double *env, CINTOpt *opt, double *cache);
+LRB_API int int2e_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+               double *env, CINTOpt *opt, double *cache);
+LRB_API void int2e_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env);
+LRB_API void CINTdel_optimizer(CINTOpt **opt);
+
+/* ---------------------------------------------------------------------
+ * librint C ABI (src/p2c.rs).  Inputs are read as (pointer, element count)
+ * pairs and not retained.  Returned buffers are malloc'd and must be
+ * released with free_c(ptr, len) (src/p2c.rs:68).
+ * -------------------------------------------------------------------*/
+LRB_API void free_c(double *ptr, size_t len);
+
+/* Dense n^4 ERI tensor R[((mu*n+nu)*n+sig)*n+lam] (src/p2c.rs:109,
+ * src/scf.rs:215-311); NULL on failure. */
+LRB_API double *int2e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                size_t env_l, int coord);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

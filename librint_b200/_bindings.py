@@ -1,0 +1,79 @@
+"""ctypes bindings of librint_b200/_lib/librint_b200.so.
+
+Mirrors the reference's python/librint/_bindings.py (same p2c.rs entry points
+and argument types, LIBRINT_SO environment override), plus this library's
+own batched / device entry points.  Loading fails loudly: there is no CPU
+fallback for any compute path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO_PATH = os.environ.get("LIBRINT_SO", os.path.join(HERE, "_lib", "librint_b200.so"))
+
+c_int, c_ll, c_sz, c_d, c_vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_size_t, ctypes.c_double, ctypes.c_void_p
+P_i = ctypes.POINTER(ctypes.c_int)
+P_d = ctypes.POINTER(ctypes.c_double)
+
+_lib = None
+
+
+class LibrintError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(SO_PATH):
+        raise LibrintError(f"librint_b200 CUDA library not found at {SO_PATH}; "
+                           "build it with `python -m librint_b200.build`")
+    L = ctypes.CDLL(SO_PATH)
+    L.lrb_last_error.restype = ctypes.c_char_p
+    L.lrb_last_error.argtypes = ()
+    L.lrb_int2e_batch_len.restype = c_ll
+    L.lrb_int2e_batch_len.argtypes = (c_int, P_i, c_ll, P_i, c_int)
+    L.lrb_int2e_batch.restype = c_int
+    L.lrb_int2e_batch.argtypes = (P_d, c_int, P_i, c_ll, P_i, c_int, P_i, c_int, P_d, c_ll)
+    L.lrb_int2e_batch_device.restype = c_int
+    L.lrb_int2e_batch_device.argtypes = (c_vp, c_int, c_vp, c_ll, c_vp, c_int, c_vp, c_int, c_vp,
+                                         c_ll, c_vp)
+    for f in ("int2e_sph", "int2e_cart"):
+        getattr(L, f).restype = c_int
+        getattr(L, f).argtypes = (P_d, P_i, P_i, P_i, c_int, P_i, c_int, P_d, c_vp, P_d)
+    L.int2e_optimizer.restype = None
+    L.int2e_optimizer.argtypes = (ctypes.POINTER(c_vp), P_i, c_int, P_i, c_int, P_d)
+    L.CINTdel_optimizer.restype = None
+    L.CINTdel_optimizer.argtypes = (ctypes.POINTER(c_vp),)
+    # librint p2c.rs ABI
+    L.free_c.restype = None
+    L.free_c.argtypes = (P_d, c_sz)
+    L.int2e_c.restype = P_d
+    L.int2e_c.argtypes = (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_int)
+    _optional(L)
+    _lib = L
+    return L
+
+
+def _optional(L):
+    """Entry points added as the library grows; declared when present."""
+    sigs = {
+        "lrb_profile_enable": (None, (c_int,)),
+        "lrb_profile_read": (c_int, (P_d, c_int)),
+        "lrb_launch_count": (c_ll, ()),
+        "lrb_fp64_peak_probe": (c_d, (c_int,)),
+    }
+    for name, (res, args) in sigs.items():
+        if hasattr(L, name):
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+
+
+def check(rc: int, what: str = "librint_b200"):
+    if rc != 0:
+        msg = lib().lrb_last_error().decode()
+        raise LibrintError(f"{what} failed ({rc}): {msg}")

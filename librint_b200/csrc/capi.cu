@@ -1,0 +1,346 @@
+// C ABI of librint_b200: batched ERIs, the libcint int2e_* entry points and
+// librint's p2c.rs-shaped functions.  Every compute path runs on the GPU;
+// there is no CPU fallback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+#include "eri_device.cuh"
+
+using namespace lrb;
+
+namespace {
+
+#define CK(x)                                  \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) {                   \
+      set_error(cudaGetErrorString(e_));       \
+      return LRB_ERR_CUDA;                     \
+    }                                          \
+  } while (0)
+
+// Device copies of one molecule's atm/bas/env.
+struct DevMol {
+  int *atm = nullptr, *bas = nullptr;
+  double *env = nullptr;
+  int natm = 0, nbas = 0;
+  long long nenv = 0;
+  int upload(cudaStream_t st, const int *a, int na, const int *b, int nb, const double *e,
+             long long ne) {
+    natm = na; nbas = nb; nenv = ne;
+    CK(cudaMallocAsync((void **)&atm, sizeof(int) * 6 * (size_t)std::max(na, 1), st));
+    CK(cudaMallocAsync((void **)&bas, sizeof(int) * 8 * (size_t)std::max(nb, 1), st));
+    CK(cudaMallocAsync((void **)&env, sizeof(double) * (size_t)std::max(ne, 1LL), st));
+    CK(cudaMemcpyAsync(atm, a, sizeof(int) * 6 * (size_t)na, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(bas, b, sizeof(int) * 8 * (size_t)nb, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env, e, sizeof(double) * (size_t)ne, cudaMemcpyHostToDevice, st));
+    return LRB_OK;
+  }
+  void release(cudaStream_t st) {
+    if (atm) cudaFreeAsync(atm, st);
+    if (bas) cudaFreeAsync(bas, st);
+    if (env) cudaFreeAsync(env, st);
+    atm = bas = nullptr;
+    env = nullptr;
+  }
+};
+
+// env length implied by atm/bas (the libcint ABI passes no env length).
+long long env_extent(const int *atm, int natm, const int *bas, int nbas) {
+  long long n = 9;   // env[0..8] are read (expcutoff, omega)
+  for (int a = 0; a < natm; ++a) {
+    n = std::max(n, (long long)atm[6 * a + 1] + 3);
+    if (atm[6 * a + 2] == 2) n = std::max(n, (long long)atm[6 * a + 3] + 1);
+  }
+  for (int s = 0; s < nbas; ++s) {
+    const int *b = bas + 8 * s;
+    n = std::max(n, (long long)b[5] + b[2]);
+    n = std::max(n, (long long)b[6] + (long long)b[2] * b[3]);
+  }
+  return n;
+}
+
+int shell_dim(int coord, const int *bas, int s) {
+  const int l = bas[8 * s + 1];
+  return (coord == 0 ? ncart(l) : nsph(l)) * bas[8 * s + 3];
+}
+
+int check_common(const int *atm, int natm, const int *bas, int nbas, const double *env,
+                 long long nenv) {
+  if (!atm || !bas || !env || natm <= 0 || nbas <= 0 || nenv <= 0)
+    return set_error("empty or NULL atm/bas/env"), LRB_ERR_INPUT;
+  if (nenv > 8 && env[8] != 0.0)
+    return set_error("range-separated integrals (env[8] != 0) are not supported"),
+           LRB_ERR_UNSUPPORTED;
+  return LRB_OK;
+}
+
+// Dense symmetric tensor from canonical quartet blocks.
+__global__ void k_scatter8(const double *__restrict__ blocks, const long long *__restrict__ boff,
+                           const int *__restrict__ quart, const int *__restrict__ aooff,
+                           const int *__restrict__ dim, int nq, long long n, double *R) {
+  const int q = blockIdx.x;
+  if (q >= nq) return;
+  const int i = quart[4 * q], j = quart[4 * q + 1], k = quart[4 * q + 2], l = quart[4 * q + 3];
+  const int di = dim[i], dj = dim[j], dk = dim[k], dl = dim[l];
+  const int tot = di * dj * dk * dl;
+  const double *b = blocks + boff[q];
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    int t = e;
+    const int a = t % di; t /= di;
+    const int bb = t % dj; t /= dj;
+    const int c = t % dk;
+    const int d = t / dk;
+    const long long A = aooff[i] + a, B = aooff[j] + bb, Cc = aooff[k] + c, D = aooff[l] + d;
+    const double v = b[e];
+    R[((A * n + B) * n + Cc) * n + D] = v;
+    R[((B * n + A) * n + Cc) * n + D] = v;
+    R[((A * n + B) * n + D) * n + Cc] = v;
+    R[((B * n + A) * n + D) * n + Cc] = v;
+    R[((Cc * n + D) * n + A) * n + B] = v;
+    R[((D * n + Cc) * n + A) * n + B] = v;
+    R[((Cc * n + D) * n + B) * n + A] = v;
+    R[((D * n + Cc) * n + B) * n + A] = v;
+  }
+}
+
+}  // namespace
+
+struct LrbCintOpt {
+  DevMol mol;
+  const int *h_atm = nullptr, *h_bas = nullptr;
+  const double *h_env = nullptr;
+};
+
+extern "C" {
+
+long long lrb_int2e_batch_len(int coord, const int *shls, long long nq, const int *bas, int nbas) {
+  if (!shls || !bas || nq < 0) return -1;
+  for (long long q = 0; q < 4 * nq; ++q)
+    if (shls[q] < 0 || shls[q] >= nbas) return -1;
+  return eri_batch_out_len(coord, shls, nq, bas);
+}
+
+int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq,
+                           const int *atm, int natm, const int *bas, int nbas,
+                           const double *env, long long nenv, void *stream) {
+  if (nq == 0) return LRB_OK;
+  if (!out || !shls || nq < 0) return set_error("bad output or quartet list"), LRB_ERR_INPUT;
+  return eri_batch_device(engine(), out, coord, shls, nq, atm, natm, bas, nbas, env, nenv,
+                          (cudaStream_t)stream, nullptr);
+}
+
+int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const int *atm,
+                    int natm, const int *bas, int nbas, const double *env, long long nenv) {
+  if (nq == 0) return LRB_OK;
+  int rc = check_common(atm, natm, bas, nbas, env, nenv);
+  if (rc) return rc;
+  const long long len = lrb_int2e_batch_len(coord, shls, nq, bas, nbas);
+  if (len < 0) return set_error("shell index out of range"), LRB_ERR_INPUT;
+  cudaStream_t st = nullptr;
+  DevMol m;
+  rc = m.upload(st, atm, natm, bas, nbas, env, nenv);
+  int *d_shls = nullptr;
+  double *d_out = nullptr;
+  if (!rc) {
+    if (cudaMallocAsync((void **)&d_shls, sizeof(int) * 4 * (size_t)nq, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_out, sizeof(double) * (size_t)std::max(len, 1LL), st) != cudaSuccess) {
+      cudaGetLastError();
+      rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
+    }
+  }
+  if (!rc && cudaMemcpyAsync(d_shls, shls, sizeof(int) * 4 * (size_t)nq, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    rc = (set_error("copy failed"), LRB_ERR_CUDA);
+  if (!rc)
+    rc = eri_batch_device(engine(), d_out, coord, d_shls, nq, m.atm, natm, m.bas, nbas, m.env,
+                          nenv, st, nullptr);
+  if (!rc && cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    rc = (set_error("copy failed"), LRB_ERR_CUDA);
+  if (d_shls) cudaFreeAsync(d_shls, st);
+  if (d_out) cudaFreeAsync(d_out, st);
+  m.release(st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) {
+    set_error(cudaGetErrorString(cudaGetLastError()));
+    rc = LRB_ERR_CUDA;
+  }
+  return rc;
+}
+
+// ------------------------------------------------------------ libcint ABI
+static int int2e_one(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                     double *env, CINTOpt *opt, int coord) {
+  int d[4];
+  for (int a = 0; a < 4; ++a) {
+    if (shls[a] < 0 || shls[a] >= nbas) return set_error("shell index out of range"), -1;
+    d[a] = shell_dim(coord, bas, shls[a]);
+  }
+  const long long blk = (long long)d[0] * d[1] * d[2] * d[3];
+  if (!out) return (int)blk;
+  cudaStream_t st = nullptr;
+  DevMol local;
+  const DevMol *m = nullptr;
+  if (opt && opt->h_atm == atm && opt->h_bas == bas && opt->h_env == env) {
+    m = &opt->mol;
+  } else {
+    const long long nenv = env_extent(atm, natm, bas, nbas);
+    if (check_common(atm, natm, bas, nbas, env, nenv)) return -1;
+    if (local.upload(st, atm, natm, bas, nbas, env, nenv)) return -1;
+    m = &local;
+  }
+  int *d_sh = nullptr;
+  double *d_out = nullptr;
+  std::vector<double> blkbuf(blk);
+  int rc = 0;
+  if (cudaMallocAsync((void **)&d_sh, 4 * sizeof(int), st) != cudaSuccess ||
+      cudaMallocAsync((void **)&d_out, sizeof(double) * blk, st) != cudaSuccess) {
+    rc = -1;
+  } else {
+    cudaMemcpyAsync(d_sh, shls, 4 * sizeof(int), cudaMemcpyHostToDevice, st);
+    rc = eri_batch_device(engine(), d_out, coord, d_sh, 1, m->atm, m->natm, m->bas, m->nbas,
+                          m->env, m->nenv, st, nullptr);
+    if (!rc) cudaMemcpyAsync(blkbuf.data(), d_out, sizeof(double) * blk, cudaMemcpyDeviceToHost, st);
+  }
+  if (d_sh) cudaFreeAsync(d_sh, st);
+  if (d_out) cudaFreeAsync(d_out, st);
+  if (m == &local) local.release(st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+  if (rc) {
+    // reference behaviour on failure: zero block, 0 returned
+    if (!dims) std::memset(out, 0, sizeof(double) * blk);
+    return 0;
+  }
+  int nz = 0;
+  for (long long e = 0; e < blk; ++e) nz |= blkbuf[e] != 0.0;
+  if (!dims) {
+    std::memcpy(out, blkbuf.data(), sizeof(double) * blk);
+  } else {
+    long long e = 0;
+    for (int l = 0; l < d[3]; ++l)
+      for (int k = 0; k < d[2]; ++k)
+        for (int j = 0; j < d[1]; ++j)
+          for (int i = 0; i < d[0]; ++i, ++e)
+            out[i + (long long)dims[0] * (j + (long long)dims[1] * (k + (long long)dims[2] * l))] = blkbuf[e];
+  }
+  return nz;
+}
+
+int int2e_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+              double *env, CINTOpt *opt, double *cache) {
+  (void)cache;
+  return int2e_one(out, dims, shls, atm, natm, bas, nbas, env, opt, 1);
+}
+
+int int2e_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+               double *env, CINTOpt *opt, double *cache) {
+  (void)cache;
+  return int2e_one(out, dims, shls, atm, natm, bas, nbas, env, opt, 0);
+}
+
+void int2e_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env) {
+  if (!opt) return;
+  *opt = nullptr;
+  const long long nenv = env_extent(atm, natm, bas, nbas);
+  if (check_common(atm, natm, bas, nbas, env, nenv)) return;
+  LrbCintOpt *o = new LrbCintOpt();
+  if (o->mol.upload(nullptr, atm, natm, bas, nbas, env, nenv) ||
+      cudaStreamSynchronize(nullptr) != cudaSuccess) {
+    o->mol.release(nullptr);
+    delete o;
+    return;
+  }
+  o->h_atm = atm; o->h_bas = bas; o->h_env = env;
+  *opt = o;
+}
+
+void CINTdel_optimizer(CINTOpt **opt) {
+  if (!opt || !*opt) return;
+  (*opt)->mol.release(nullptr);
+  cudaStreamSynchronize(nullptr);
+  delete *opt;
+  *opt = nullptr;
+}
+
+// ------------------------------------------------------------ p2c ABI
+void free_c(double *ptr, size_t len) {
+  (void)len;
+  std::free(ptr);
+}
+
+double *int2e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, size_t env_l,
+                int coord) {
+  const int natm = (int)(atm_l / 6), nbas = (int)(bas_l / 8);
+  if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), nullptr;
+  if (check_common(atm_p, natm, bas_p, nbas, env_p, (long long)env_l)) return nullptr;
+  std::vector<int> aooff(nbas + 1, 0), dim(nbas);
+  for (int s = 0; s < nbas; ++s) {
+    dim[s] = shell_dim(coord, bas_p, s);
+    aooff[s + 1] = aooff[s] + dim[s];
+  }
+  const long long n = aooff[nbas];
+  const long long n4 = n * n * n * n;
+  // canonical quartets i>=j, k>=l, (ij)>=(kl)
+  std::vector<int> quart;
+  for (int i = 0; i < nbas; ++i)
+    for (int j = 0; j <= i; ++j)
+      for (int k = 0; k <= i; ++k)
+        for (int l = 0; l <= (k == i ? j : k); ++l) {
+          quart.push_back(i); quart.push_back(j); quart.push_back(k); quart.push_back(l);
+        }
+  const long long nq = (long long)quart.size() / 4;
+  std::vector<long long> boff(nq + 1, 0);
+  for (long long q = 0; q < nq; ++q)
+    boff[q + 1] = boff[q] + (long long)dim[quart[4 * q]] * dim[quart[4 * q + 1]] *
+                                dim[quart[4 * q + 2]] * dim[quart[4 * q + 3]];
+  double *R = (double *)std::malloc(sizeof(double) * (size_t)std::max(n4, 1LL));
+  if (!R) return set_error("host allocation failed"), nullptr;
+  cudaStream_t st = nullptr;
+  DevMol m;
+  int *d_q = nullptr, *d_ao = nullptr, *d_dim = nullptr;
+  long long *d_boff = nullptr;
+  double *d_blk = nullptr, *d_R = nullptr;
+  int rc = m.upload(st, atm_p, natm, bas_p, nbas, env_p, (long long)env_l);
+  auto al = [&](void **p, size_t b) {
+    if (rc) return;
+    if (cudaMallocAsync(p, std::max(b, (size_t)8), st) != cudaSuccess) {
+      cudaGetLastError();
+      rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
+    }
+  };
+  al((void **)&d_q, sizeof(int) * quart.size());
+  al((void **)&d_ao, sizeof(int) * aooff.size());
+  al((void **)&d_dim, sizeof(int) * dim.size());
+  al((void **)&d_boff, sizeof(long long) * boff.size());
+  al((void **)&d_blk, sizeof(double) * (size_t)boff[nq]);
+  al((void **)&d_R, sizeof(double) * (size_t)n4);
+  if (!rc) {
+    cudaMemcpyAsync(d_q, quart.data(), sizeof(int) * quart.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_ao, aooff.data(), sizeof(int) * aooff.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_dim, dim.data(), sizeof(int) * dim.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_boff, boff.data(), sizeof(long long) * boff.size(), cudaMemcpyHostToDevice, st);
+    rc = eri_batch_device(engine(), d_blk, coord, d_q, nq, m.atm, natm, m.bas, nbas, m.env,
+                          (long long)env_l, st, nullptr);
+  }
+  if (!rc) {
+    k_scatter8<<<(unsigned)nq, 128, 0, st>>>(d_blk, d_boff, d_q, d_ao, d_dim, (int)nq, n, d_R);
+    if (cudaGetLastError() != cudaSuccess) rc = LRB_ERR_CUDA;
+  }
+  if (!rc && cudaMemcpyAsync(R, d_R, sizeof(double) * (size_t)n4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    rc = LRB_ERR_CUDA;
+  for (void *p : {(void *)d_q, (void *)d_ao, (void *)d_dim, (void *)d_boff, (void *)d_blk, (void *)d_R})
+    if (p) cudaFreeAsync(p, st);
+  m.release(st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) rc = LRB_ERR_CUDA;
+  if (rc) {
+    std::free(R);
+    return nullptr;
+  }
+  return R;
+}
+
+}  // extern "C"

@@ -1,0 +1,123 @@
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "engine.h"
+
+namespace lrb {
+
+static thread_local std::string g_err;
+
+void set_error(const char *msg) { g_err = msg ? msg : ""; }
+const char *last_error() { return g_err.c_str(); }
+
+char *Arena::get(cudaStream_t st, size_t need) {
+  if (need <= size) return ptr;
+  if (ptr) cudaFreeAsync(ptr, st);
+  size_t sz = need + need / 4 + (1 << 20);
+  void *p = nullptr;
+  if (cudaMallocAsync(&p, sz, st) != cudaSuccess) {
+    cudaGetLastError();
+    ptr = nullptr;
+    size = 0;
+    return nullptr;
+  }
+  ptr = static_cast<char *>(p);
+  size = sz;
+  return ptr;
+}
+
+Engine &engine() {
+  static std::mutex mu;
+  static Engine *per_dev[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> g(mu);
+  if (!per_dev[dev]) per_dev[dev] = new Engine();
+  return *per_dev[dev];
+}
+
+// FP64 FMA throughput probe: 8 independent chains per thread keep the FP64
+// pipe busy without memory traffic; the result is written so the work stays.
+__global__ void k_fp64_probe(double *sink, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 12345.678) sink[0] = s;
+}
+
+}  // namespace lrb
+
+using namespace lrb;
+
+extern "C" {
+
+LRB_API const char *lrb_last_error(void) { return lrb::last_error(); }
+
+LRB_API void lrb_profile_enable(int on) {
+  Engine &e = engine();
+  e.profile = on != 0;
+}
+
+// Milliseconds per ERI class kernel accumulated since the last read, into
+// ms[0..n); returns the number of records harvested (waits for them).
+LRB_API int lrb_profile_read(double *ms, int n) {
+  Engine &e = engine();
+  for (int i = 0; i < n; ++i) ms[i] = 0.0;
+  int cnt = 0;
+  for (ProfRecord &r : e.prof) {
+    cudaEventSynchronize(r.stop);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, r.start, r.stop);
+    if (r.cls >= 0 && r.cls < n) ms[r.cls] += t;
+    cudaEventDestroy(r.start);
+    cudaEventDestroy(r.stop);
+    ++cnt;
+  }
+  e.prof.clear();
+  return cnt;
+}
+
+LRB_API long long lrb_launch_count(void) { return engine().launches; }
+
+// Measured FP64 FMA throughput of the current device in TFLOP/s (about
+// `ms` milliseconds of work, timed with CUDA events).
+LRB_API double lrb_fp64_peak_probe(int ms) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  double *sink = nullptr;
+  if (cudaMalloc(&sink, 8) != cudaSuccess) return -1.0;
+  const int threads = 256, blocks = nsm * 8;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int iters = 1 << 14;
+  float t = 0.f;
+  k_fp64_probe<<<blocks, threads>>>(sink, iters, 0.999999, 1e-9);   // warm-up
+  for (int rep = 0; rep < 8; ++rep) {
+    cudaEventRecord(a);
+    k_fp64_probe<<<blocks, threads>>>(sink, iters, 0.999999, 1e-9);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&t, a, b);
+    if (t >= ms) break;
+    iters *= 2;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(sink);
+  if (cudaGetLastError() != cudaSuccess || t <= 0.f) return -1.0;
+  const double flops = 2.0 * 8.0 * (double)iters * threads * blocks;
+  return flops / (t * 1e-3) / 1e12;
+}
+
+}  // extern "C"
+

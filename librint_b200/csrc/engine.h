@@ -1,0 +1,73 @@
+// Engine state shared by the kernels' host drivers: error reporting and a
+// grow-only, stream-ordered device workspace (cudaMallocAsync), one per
+// device.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <vector>
+
+#include "../../include/librint_b200.h"
+
+namespace lrb {
+
+constexpr int ERI_LMAX = 2;    // shells up to d in the compiled classes
+constexpr int ERI_KMAX = 31;   // primitives per shell (sort-key packing limit)
+
+void set_error(const char *msg);
+
+// Grow-only device arena; growth frees the old block on the same stream, so
+// work already queued on that stream finishes before the memory is reused.
+struct Arena {
+  char *ptr = nullptr;
+  size_t size = 0;
+  char *get(cudaStream_t st, size_t need);
+};
+
+struct Workspace {
+  Arena main, aux, pairs, extra;
+  char *reserve(cudaStream_t st, size_t n) { return main.get(st, n); }
+  void *reserve_aux(cudaStream_t st, size_t n) { return aux.get(st, n); }
+  void *reserve_pairs(cudaStream_t st, size_t n) { return pairs.get(st, n); }
+  void *reserve_extra(cudaStream_t st, size_t n) { return extra.get(st, n); }
+};
+
+// Carves 256-byte aligned sub-buffers out of one allocation.
+struct Carver {
+  char *p;
+  explicit Carver(char *base) : p(base) {}
+  template <class T>
+  T *take(size_t n) {
+    T *r = reinterpret_cast<T *>(p);
+    p += (n * sizeof(T) + 255) & ~size_t(255);
+    return r;
+  }
+};
+inline size_t carve_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+// Per-kernel timing for measurement: CUDA events recorded around each ERI
+// class kernel on its own stream while profiling is enabled.
+struct ProfRecord {
+  int cls;
+  cudaEvent_t start, stop;
+};
+
+struct Engine {
+  Workspace ws;
+  double expcutoff = 60.0;   // reference default, src/g2e.rs:83-92
+  bool profile = false;
+  std::vector<ProfRecord> prof;
+  long long launches = 0;    // kernels of this library launched so far
+};
+Engine &engine();          // for the current device
+
+struct EriBatchStats {
+  long long nq = 0, out_len = 0, prim_pairs = 0;
+};
+
+int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, long long nq,
+                     const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
+                     long long nenv, cudaStream_t st, EriBatchStats *stats);
+long long eri_batch_out_len(int coord, const int *shls, long long nq, const int *bas);
+
+}  // namespace lrb

@@ -1,0 +1,15 @@
+// Kernels of the classes with bra (pp| -- generated list, one TU per bra.
+#define RYS_OMIT_TAB
+#define RYS_CONST_QUAL __constant__
+#include "eri_classes.cuh"
+
+namespace lrb {
+
+void eri_register_bra2(ClassEntry *t, const double *c2s_host) {
+  cudaMemcpyToSymbol(c_c2s, c2s_host, sizeof(c_c2s));
+  t[class_id(1, 1, 0, 0)] = make_entry<1, 1, 0, 0>();
+  t[class_id(1, 1, 1, 0)] = make_entry<1, 1, 1, 0>();
+  t[class_id(1, 1, 1, 1)] = make_entry<1, 1, 1, 1>();
+}
+
+}  // namespace lrb

@@ -1,0 +1,46 @@
+// Class table of the ERI kernels: ids, dispatch entries and the per-bra
+// registration functions (one translation unit each, eri_bra<P>.cu, so the
+// kernels compile in parallel).
+#pragma once
+#include "engine.h"
+#include "eri_kernel.cuh"
+
+namespace lrb {
+
+// Canonical classes for l <= ERI_LMAX, id = P(P+1)/2 + Q with pair index
+// P = li(li+1)/2 + lj of the bra (li >= lj) and Q of the ket, P >= Q.
+__host__ __device__ inline int pair_index(int a, int b) { return a * (a + 1) / 2 + b; }
+__host__ __device__ inline int class_id(int li, int lj, int lk, int ll) {
+  const int P = pair_index(li, lj), Q = pair_index(lk, ll);
+  return P * (P + 1) / 2 + Q;
+}
+constexpr int NPAIRCLS = (ERI_LMAX + 1) * (ERI_LMAX + 2) / 2;
+constexpr int NCLASS = NPAIRCLS * (NPAIRCLS + 1) / 2;
+
+using EriKernelFn = void (*)(EriParams, const double *, int *);
+
+struct ClassEntry {
+  EriKernelFn fn;
+  size_t smem;
+  int slots, nr;
+};
+
+template <int LI, int LJ, int LK, int LL>
+ClassEntry make_entry() {
+  using C = EriClass<LI, LJ, LK, LL>;
+  ClassEntry e;
+  e.fn = k_eri_out<LI, LJ, LK, LL>;
+  e.smem = EriLayout<C>::SMEM;
+  e.slots = C::SLOTS;
+  e.nr = C::NR;
+  return e;
+}
+
+void eri_register_bra0(ClassEntry *t, const double *c2s_host);   // (ss|
+void eri_register_bra1(ClassEntry *t, const double *c2s_host);   // (ps|
+void eri_register_bra2(ClassEntry *t, const double *c2s_host);   // (pp|
+void eri_register_bra3(ClassEntry *t, const double *c2s_host);   // (ds|
+void eri_register_bra4(ClassEntry *t, const double *c2s_host);   // (dp|
+void eri_register_bra5(ClassEntry *t, const double *c2s_host);   // (dd|
+
+}  // namespace lrb

@@ -1,0 +1,151 @@
+// Device side of the Rys-quadrature ERI engine (sm_100a, FP64).
+//
+// Work decomposition for one angular class (LI LJ | LK LL), canonical order
+// LI >= LJ, LK >= LL, (LI,LJ) >= (LK,LL):
+//
+//  * The recurrence is built on the "base" centre of each pair (i if LI > LJ,
+//    else j; k if LK > LL, else l) as libcint does (reference
+//    src/g2e.rs:113-181).  A = bra base, B = bra partner, C/D likewise.
+//  * Per primitive quartet only the Rys roots, the 2D VRR table V(n, m),
+//    n <= LA+LB, m <= LC+LD, and the (e|f) product sum run:
+//        [e|f] += sum_r Vx_r[ex][fx] Vy_r[ey][fy] Vz_r[ez][fz]
+//    over cartesian e of momentum LA..LA+LB on A and f of LC..LC+LD on C.
+//    The horizontal recurrences (A->B, C->D) and the cart->sph transform are
+//    linear with shell-quartet constants, so they run once per contracted
+//    shell quartet in the epilogue ("HRR after contraction").
+//  * A warp holds SLOTS = 32 / NROW shell quartets; within a slot lane rho
+//    owns row e = rho of [e|f] and keeps its NCOL f-accumulators in
+//    registers.  Roots and VRR are computed cooperatively by the slot's
+//    lanes and exchanged through a small per-warp shared-memory area.
+//  * Roots/weights come from the piecewise polynomial tables of
+//    rys_tables.h, staged once per CTA in shared memory.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rys_tables.h"
+
+namespace lrb {
+
+// ------------------------------------------------------------------ shapes
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int nsph(int l) { return 2 * l + 1; }
+
+// cartesian component n of momentum l in libcint order (x-major descending)
+__host__ __device__ constexpr int cart_x(int l, int n) {
+  int c = 0;
+  for (int lx = l; lx >= 0; --lx)
+    for (int ly = l - lx; ly >= 0; --ly) {
+      if (c == n) return lx;
+      ++c;
+    }
+  return 0;
+}
+__host__ __device__ constexpr int cart_y(int l, int n) {
+  int c = 0;
+  for (int lx = l; lx >= 0; --lx)
+    for (int ly = l - lx; ly >= 0; --ly) {
+      if (c == n) return ly;
+      ++c;
+    }
+  return 0;
+}
+__host__ __device__ constexpr int cart_z(int l, int n) { return l - cart_x(l, n) - cart_y(l, n); }
+// position of (x, y, z) inside momentum x+y+z
+__host__ __device__ constexpr int cart_index(int x, int y, int z) {
+  return (y + z) * (y + z + 1) / 2 + z;
+}
+// components of all momenta lo..hi, concatenated
+__host__ __device__ constexpr int range_count(int lo, int hi) {
+  int n = 0;
+  for (int e = lo; e <= hi; ++e) n += ncart(e);
+  return n;
+}
+__host__ __device__ constexpr int range_offset(int lo, int e) {
+  int n = 0;
+  for (int k = lo; k < e; ++k) n += ncart(k);
+  return n;
+}
+__host__ __device__ constexpr int range_x(int lo, int r) {
+  int e = lo;
+  while (r >= ncart(e)) { r -= ncart(e); ++e; }
+  return cart_x(e, r);
+}
+__host__ __device__ constexpr int range_y(int lo, int r) {
+  int e = lo;
+  while (r >= ncart(e)) { r -= ncart(e); ++e; }
+  return cart_y(e, r);
+}
+__host__ __device__ constexpr int range_z(int lo, int r) {
+  int e = lo;
+  while (r >= ncart(e)) { r -= ncart(e); ++e; }
+  return cart_z(e, r);
+}
+__host__ __device__ constexpr int range_index(int lo, int x, int y, int z) {
+  return range_offset(lo, x + y + z) + cart_index(x, y, z);
+}
+__host__ __device__ constexpr int binom(int n, int k) {
+  int r = 1;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+
+// ------------------------------------------------------------------ data
+// One primitive pair of a shell pair: exponent sum, Gaussian product centre,
+// coefficient product times exp(-mu R^2) (class prefactor folded into the
+// ket side by the caller), and libcint's screening key
+// cce = mu R^2 - log_rr - log|c_i| - log|c_j| (reference
+// src/optimizer.rs:732-808).
+struct __align__(16) PrimPair {
+  double a, px, py, pz, fac, cce;
+};
+
+// One shell quartet of a class launch, canonical order.
+struct QuartetJob {
+  int pij_off, nij;       // bra primitive pairs
+  int pkl_off, nkl;       // ket primitive pairs
+  int ish, jsh, ksh, lsh; // canonical shells (centres)
+  long long out_off;      // first output element
+  int s_i, s_j, s_k, s_l; // output strides of the canonical indices
+};
+
+struct EriParams {
+  const QuartetJob *jobs;
+  const int *order;       // jobs to run, in launch order
+  int njobs;
+  const PrimPair *pp;
+  const double *centers;  // 3 doubles per shell
+  double *out;
+  double expcutoff;
+  int sph;                // 1: spherical output, 0: cartesian
+};
+
+// ------------------------------------------------------------------ roots
+// Rys nodes/weights for N roots at x from the shared-memory table `tab`
+// (layout of rys_tables.h for this N).  Function f < N is u_f, f >= N is
+// w_{f-N}.
+template <int N>
+__device__ __forceinline__ double rys_function(const double *tab, double x, int f) {
+  constexpr double XBREAK = 43.0 + 5.0 * N;
+  if (x >= XBREAK) {
+    constexpr int off = N * (N - 1) / 2;
+    if (f < N) {
+      const double r = RYS_LARGEX_R[off + f];
+      return r / (x - r);
+    }
+    return RYS_LARGEX_W[off + f - N] * sqrt(0.78539816339744831 / x);  // pi/4
+  }
+  // clamp keeps the table read in bounds even for NaN input (NaN propagates)
+  constexpr int NSEG = (43 + 5 * N + 3) / 4;
+  static_assert(RYS_SEG_WIDTH == 4.0, "segment count assumes width 4");
+  int seg = (int)(x * (1.0 / RYS_SEG_WIDTH));
+  seg = seg < 0 ? 0 : (seg >= NSEG ? NSEG - 1 : seg);
+  const double t = (x - (seg * RYS_SEG_WIDTH + 0.5 * RYS_SEG_WIDTH)) * (2.0 / RYS_SEG_WIDTH);
+  const double *c = tab + (seg * 2 * N + f) * RYS_NCOEF;
+  double r = c[RYS_DEG];
+#pragma unroll
+  for (int k = RYS_DEG - 1; k >= 0; --k) r = fma(r, t, c[k]);
+  return r;
+}
+
+}  // namespace lrb

@@ -191,6 +191,14 @@ def main():
     for n in range(1, NMAX + 1):
         lines.append(f"// nroots={n}: worst validated relative error {worst_by_n[n]:.2e}")
     lines.append("#pragma once")
+    lines.append("// CUDA translation units define RYS_TAB_QUAL as __device__ and")
+    lines.append("// RYS_CONST_QUAL as __constant__ before including this file.")
+    lines.append("#ifndef RYS_TAB_QUAL")
+    lines.append("#define RYS_TAB_QUAL")
+    lines.append("#endif")
+    lines.append("#ifndef RYS_CONST_QUAL")
+    lines.append("#define RYS_CONST_QUAL")
+    lines.append("#endif")
     lines.append(f"#define RYS_NMAX {NMAX}")
     lines.append(f"#define RYS_DEG {DEG}")
     lines.append(f"#define RYS_NCOEF {DEG + 1}")
@@ -201,16 +209,18 @@ def main():
         nseg = int(-(-xmax(n) // H))
         nsegs.append(nseg)
         offs.append(offs[-1] + nseg * 2 * n * (DEG + 1))
-    lines.append("static const int RYS_TAB_NSEG[RYS_NMAX + 1] = {0, " +
+    lines.append("static constexpr int RYS_TAB_NSEG[RYS_NMAX + 1] = {0, " +
                  ", ".join(str(s) for s in nsegs) + "};")
-    lines.append("static const int RYS_TAB_OFFSET[RYS_NMAX + 2] = {0, " +
+    lines.append("static constexpr int RYS_TAB_OFFSET[RYS_NMAX + 2] = {0, " +
                  ", ".join(str(o) for o in offs) + "};")
-    lines.append(f"static const double RYS_TAB[{offs[-1]}] = {{")
+    lines.append("#ifndef RYS_OMIT_TAB   // translation units that take the table by pointer")
+    lines.append(f"RYS_TAB_QUAL static const double RYS_TAB[{offs[-1]}] = {{")
     for n in range(1, NMAX + 1):
         for s in range(nsegs[n - 1]):
             for f in range(2 * n):
                 lines.append("  " + ", ".join(repr(v) for v in table[(n, s)][f]) + ",")
     lines.append("};")
+    lines.append("#endif")
     # large-x constants, packed per n at offset n(n-1)/2
     rr, cc, largex_err = [], [], []
     for n in range(1, NMAX + 1):
@@ -223,9 +233,9 @@ def main():
         cc += [float(v) for v in c]
     lines.append("// large-x limit, worst relative error at the breakpoint per nroots: " +
                  " ".join(f"{e:.1e}" for e in largex_err))
-    lines.append(f"static const double RYS_LARGEX_R[{len(rr)}] = {{" +
+    lines.append(f"RYS_CONST_QUAL static const double RYS_LARGEX_R[{len(rr)}] = {{" +
                  ", ".join(repr(v) for v in rr) + "};")
-    lines.append(f"static const double RYS_LARGEX_W[{len(cc)}] = {{" +
+    lines.append(f"RYS_CONST_QUAL static const double RYS_LARGEX_W[{len(cc)}] = {{" +
                  ", ".join(repr(v) for v in cc) + "};")
     with open(out, "w") as fh:
         fh.write("\n".join(lines) + "\n")

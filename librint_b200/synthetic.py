@@ -76,7 +76,11 @@ def eri_sweep(cls, nq: int, seed: int = 2, kmax: int = 6, cube_ang: float = 10.0
     e = np.take_along_axis(e, order, axis=1)
     c = np.take_along_axis(np.where(mask, raw_c, 0.0), order, axis=1)
     e = np.where(mask, e, 0.0)
-    cn = _normalise_many(ls, e, c, mask)
+    cn = np.empty_like(c)
+    step = 1 << 17
+    for a in range(0, nsh, step):
+        cn[a:a + step] = _normalise_many(ls[a:a + step], e[a:a + step], c[a:a + step],
+                                         mask[a:a + step])
     # env: 20 reserved, then per shell [x y z 0 | exps(K) | coefs(K)]
     per = 4 + 2 * ks
     start = 20 + np.concatenate([[0], np.cumsum(per)[:-1]])
@@ -85,8 +89,8 @@ def eri_sweep(cls, nq: int, seed: int = 2, kmax: int = 6, cube_ang: float = 10.0
     cols = np.arange(kmax)[None, :]
     pe = start + 4
     pc = pe + ks
-    env[np.where(mask, pe[:, None] + cols, 0)[mask]] = e[mask]
-    env[np.where(mask, pc[:, None] + cols, 0)[mask]] = cn[mask]
+    env[(pe[:, None] + cols)[mask]] = e[mask]
+    env[(pc[:, None] + cols)[mask]] = cn[mask]
     atm = np.zeros((nsh, 6), dtype=np.int32)
     atm[:, 1] = start
     atm[:, 2] = 1
@@ -106,11 +110,10 @@ def eri_sweep(cls, nq: int, seed: int = 2, kmax: int = 6, cube_ang: float = 10.0
 
 def _normalise_many(ls, e, c, mask):
     """Vectorised normalise_contraction over shells (rows)."""
-    ls = ls[:, None].astype(np.float64)
-    n1 = (2 * ls + 3) * 0.5
+    gtab = np.array([math.gamma(l + 1.5) for l in range(9)])
+    gam = gtab[ls][:, None]
+    n1 = (ls[:, None] + 1.5).astype(np.float64)
     # gto_norm(l, a) = 1/sqrt(gamma(l+3/2)/(2 (2a)^(l+3/2)))
-    g = math.gamma
-    gam = np.vectorize(lambda v: g(v))(n1)
     with np.errstate(divide="ignore", invalid="ignore"):
         nrm = np.where(mask, 1.0 / np.sqrt(gam / (2.0 * (2.0 * np.where(mask, e, 1.0)) ** n1)), 0.0)
     cs = c * nrm

@@ -1,0 +1,114 @@
+"""GPU parity of the batched ERI engine, through the C ABI, against the CPU
+oracle and the reference goldens (tolerance of tests/conftest.py)."""
+import numpy as np
+import pytest
+
+import oracle
+from librint_b200 import eri, synthetic
+from librint_b200 import _bindings as B
+from librint_b200.basis import Molecule
+from tests.conftest import assert_eri_close
+
+pytestmark = pytest.mark.gpu
+
+CLASSES = synthetic.canonical_classes(2)
+
+
+def _blocks(m, shls, coord):
+    """Oracle blocks for a quartet list, unpacked."""
+    packed = oracle.int2e_batch(m, shls, coord)
+    return packed
+
+
+@pytest.mark.parametrize("cls", CLASSES)
+def test_class_samples_vs_reference_golden(golden, cls):
+    key = "cls/%d%d%d%d" % cls
+    env = golden[key + "/env"]
+    for q in range(golden[key + "/atm"].shape[0]):
+        m = Molecule(golden[key + "/atm"][q].ravel(), golden[key + "/bas"][q].ravel(), env)
+        for coord, nm in ((0, "cart"), (1, "sph")):
+            got = eri.int2e_batch(m, [[0, 1, 2, 3]], coord)
+            ref = golden[f"{key}/{nm}"][q]
+            assert_eri_close(got, ref.transpose(3, 2, 1, 0).ravel(), what=f"{key} q{q} {nm}")
+
+
+@pytest.mark.parametrize("coord", [0, 1])
+def test_sweep_batch_vs_oracle(coord):
+    """All 21 classes, 400 random quartets each, in one mixed batch."""
+    for cls in CLASSES:
+        m, shls = synthetic.eri_sweep(cls, 400, seed=11)
+        got = eri.int2e_batch(m, shls, coord)
+        ref = oracle.int2e_batch(m, shls, coord)
+        assert_eri_close(got, ref, what=f"class {cls} coord {coord}")
+
+
+def test_permuted_shell_orders_vs_oracle():
+    """Non-canonical quartet orders are canonicalised and written back in the
+    requested layout."""
+    rng = np.random.default_rng(5)
+    for cls in [(2, 1, 1, 0), (2, 2, 2, 0), (1, 0, 1, 1), (2, 0, 2, 1)]:
+        m, shls = synthetic.eri_sweep(cls, 60, seed=12)
+        perms = [rng.permutation(4) for _ in range(shls.shape[0])]
+        sh = np.array([s[p] for s, p in zip(shls, perms)], dtype=np.int32)
+        for coord in (0, 1):
+            assert_eri_close(eri.int2e_batch(m, sh, coord), oracle.int2e_batch(m, sh, coord),
+                             what=f"perm {cls} {coord}")
+
+
+def test_mixed_molecule_batch(golden):
+    """Quartets of a real molecule (shared shells) in one batch."""
+    m = Molecule(golden["mol/h2o/def2svp/atm"], golden["mol/h2o/def2svp/bas"],
+                 golden["mol/h2o/def2svp/env"])
+    rng = np.random.default_rng(3)
+    sh = rng.integers(0, m.nbas, size=(3000, 4)).astype(np.int32)
+    for coord in (0, 1):
+        assert_eri_close(eri.int2e_batch(m, sh, coord), oracle.int2e_batch(m, sh, coord))
+
+
+@pytest.mark.parametrize("name", ["h2o/sto3g", "ch4/sto3g", "lih/sto3g"])
+def test_int2e_c_dense_vs_golden(golden, name):
+    key = "mol/" + name
+    m = Molecule(golden[key + "/atm"], golden[key + "/bas"], golden[key + "/env"])
+    for coord in (0, 1):
+        assert_eri_close(eri.int2e(m, coord), golden[f"{key}/int2e_{coord}"], what=name)
+
+
+def test_int2e_c_subsample_def2svp(golden):
+    key = "mol/h2o/def2svp"
+    m = Molecule(golden[key + "/atm"], golden[key + "/bas"], golden[key + "/env"])
+    for coord in (0, 1):
+        t = eri.int2e(m, coord).ravel()
+        assert_eri_close(t[golden[f"{key}/int2e_{coord}_idx"]], golden[f"{key}/int2e_{coord}_val"])
+
+
+def test_libcint_per_quartet_abi(golden):
+    m = synthetic.water_like()
+    for shls in ([0, 1, 2, 3], [2, 2, 2, 2], [4, 2, 0, 2]):
+        for coord in (0, 1):
+            got, nz = eri.int2e_block(m, shls, coord)
+            ref, _ = oracle.int2e_block(m, shls, coord)
+            assert nz == 1
+            assert_eri_close(got, ref)
+
+
+def test_errors_are_reported_not_fatal():
+    m, shls = synthetic.eri_sweep((1, 0, 0, 0), 4, seed=1)
+    # empty batch is a no-op
+    assert eri.int2e_batch(m, np.zeros((0, 4), np.int32)).size == 0
+    # shell index out of range
+    bad = shls.copy()
+    bad[0, 0] = m.nbas + 7
+    with pytest.raises(B.LibrintError):
+        eri.int2e_batch(m, bad)
+    # f shell: not compiled (l <= 2)
+    m2 = Molecule(m.atm.copy(), m.bas.copy(), m.env.copy())
+    m2.bas.reshape(-1, 8)[0, 1] = 3
+    with pytest.raises(B.LibrintError):
+        eri.int2e_batch(m2, shls[:1], 0)
+    # range separation (env[8] != 0) is out of scope
+    m3 = Molecule(m.atm.copy(), m.bas.copy(), m.env.copy())
+    m3.env[8] = 0.3
+    with pytest.raises(B.LibrintError):
+        eri.int2e_batch(m3, shls)
+    # the library still works afterwards
+    assert_eri_close(eri.int2e_batch(m, shls), oracle.int2e_batch(m, shls, 1))
