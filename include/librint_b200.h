@@ -100,6 +100,57 @@ LRB_API void free_c(double *ptr, size_t len);
 LRB_API double *int2e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
                 size_t env_l, int coord);
 
+/* ---------------------------------------------------------------------
+ * Molecule context, direct Fock build and SCF on the GPU.
+ * A context holds device copies of atm/bas/env, the shell-pair table with
+ * primitive-pair data and Schwarz factors; it is reused across Fock builds.
+ * Matrices are n x n (cartesian AOs, the reference's SCF basis).
+ * -------------------------------------------------------------------*/
+typedef struct LrbMol LrbMol;
+LRB_API int lrb_mol_create(LrbMol **out, const int *atm, int natm, const int *bas, int nbas,
+                           const double *env, long long nenv);
+LRB_API void lrb_mol_destroy(LrbMol *m);
+LRB_API int lrb_mol_nao(const LrbMol *m);
+
+/* G(P) = J - K/2 without the n^4 tensor -- the GPU form of integral2e_fock
+ * (src/scf.rs:316-410).  Quartets with Q_IJ Q_KL max|D| < tau are skipped
+ * (tau = 0 keeps every quartet the reference keeps).  Host or device. */
+LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long long *quartets);
+LRB_API int lrb_fock_G_device(LrbMol *m, const double *P, double *G, double tau, void *stream);
+
+typedef struct {
+  int max_iter;     /* reference imax */
+  double conv;      /* reference conv: ||P - P_old||_F / 2 */
+  int guess;        /* 0: P0 = I (reference), 1: core Hamiltonian */
+  int diis;         /* DIIS subspace (0 = plain Roothaan, as the reference) */
+  double tau;       /* quartet screening threshold */
+} LrbScfOptions;
+
+typedef struct {
+  double energy, e_nuc, delta, fock_ms, wall_ms;
+  int iterations, converged;
+  long long quartets;
+} LrbScfResult;
+
+/* RHF (src/scf.rs:743-969).  P_out (n*n host) and P0 (initial density,
+ * overrides guess) may be NULL. */
+LRB_API int lrb_scf(LrbMol *m, long long nelec, const LrbScfOptions *opt, LrbScfResult *res,
+                    double *P_out, const double *P0);
+/* Energy functional at a density (src/scf.rs:827-956, energyfast). */
+LRB_API int lrb_energy(LrbMol *m, const double *P, double tau, double *E);
+/* One-electron matrix: typec 0 overlap, 1 kinetic, 2 nuclear (src/scf.rs:149). */
+LRB_API int lrb_int1e(LrbMol *m, int typec, int coord, double *out);
+
+/* librint p2c.rs entry points (src/p2c.rs:86, 153, 186, 210). */
+LRB_API double *int1e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                        size_t env_l, int coord, int typec);
+LRB_API double *density_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                          size_t env_l, size_t nelec, int imax, double conv);
+LRB_API double energy_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                        size_t env_l, double *P_p, size_t P_l);
+LRB_API double scf_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                     size_t env_l, size_t nelec, int imax, double conv);
+
 #ifdef __cplusplus
 }
 #endif

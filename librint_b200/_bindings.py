@@ -58,6 +58,18 @@ def lib():
     return L
 
 
+class ScfOptions(ctypes.Structure):
+    _fields_ = [("max_iter", ctypes.c_int), ("conv", ctypes.c_double), ("guess", ctypes.c_int),
+                ("diis", ctypes.c_int), ("tau", ctypes.c_double)]
+
+
+class ScfResult(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("e_nuc", ctypes.c_double), ("delta", ctypes.c_double),
+                ("fock_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
+                ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("quartets", ctypes.c_longlong)]
+
+
 def _optional(L):
     """Entry points added as the library grows; declared when present."""
     sigs = {
@@ -65,6 +77,19 @@ def _optional(L):
         "lrb_profile_read": (c_int, (P_d, c_int)),
         "lrb_launch_count": (c_ll, ()),
         "lrb_fp64_peak_probe": (c_d, (c_int,)),
+        "lrb_mol_create": (c_int, (ctypes.POINTER(c_vp), P_i, c_int, P_i, c_int, P_d, c_ll)),
+        "lrb_mol_destroy": (None, (c_vp,)),
+        "lrb_mol_nao": (c_int, (c_vp,)),
+        "lrb_fock_G": (c_int, (c_vp, P_d, P_d, c_d, ctypes.POINTER(c_ll))),
+        "lrb_fock_G_device": (c_int, (c_vp, c_vp, c_vp, c_d, c_vp)),
+        "lrb_scf": (c_int, (c_vp, c_ll, ctypes.POINTER(ScfOptions), ctypes.POINTER(ScfResult),
+                            P_d, P_d)),
+        "lrb_energy": (c_int, (c_vp, P_d, c_d, P_d)),
+        "lrb_int1e": (c_int, (c_vp, c_int, c_int, P_d)),
+        "int1e_c": (P_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_int, c_int)),
+        "density_c": (P_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_sz, c_int, c_d)),
+        "energy_c": (c_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, P_d, c_sz)),
+        "scf_c": (c_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_sz, c_int, c_d)),
     }
     for name, (res, args) in sigs.items():
         if hasattr(L, name):

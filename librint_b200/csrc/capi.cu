@@ -11,6 +11,7 @@
 
 #include "engine.h"
 #include "eri_device.cuh"
+#include "fock.h"
 
 using namespace lrb;
 
@@ -341,6 +342,162 @@ double *int2e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_
     return nullptr;
   }
   return R;
+}
+
+// ------------------------------------------------------------ molecule / Fock / SCF
+struct LrbMol {
+  MolCtx ctx;
+};
+
+LRB_API int lrb_mol_create(LrbMol **out, const int *atm, int natm, const int *bas, int nbas,
+                           const double *env, long long nenv) {
+  if (!out) return set_error("NULL handle pointer"), LRB_ERR_INPUT;
+  *out = nullptr;
+  int rc = check_common(atm, natm, bas, nbas, env, nenv);
+  if (rc) return rc;
+  LrbMol *m = new LrbMol();
+  rc = mol_create(m->ctx, atm, natm, bas, nbas, env, nenv, nullptr);
+  if (rc) {
+    mol_destroy(m->ctx, nullptr);
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return LRB_OK;
+}
+
+LRB_API void lrb_mol_destroy(LrbMol *m) {
+  if (!m) return;
+  mol_destroy(m->ctx, nullptr);
+  delete m;
+}
+
+LRB_API int lrb_mol_nao(const LrbMol *m) { return m ? m->ctx.nao : -1; }
+
+LRB_API int lrb_fock_G_device(LrbMol *m, const double *P, double *G, double tau, void *stream) {
+  if (!m || !P || !G) return set_error("NULL argument"), LRB_ERR_INPUT;
+  return fock_build(m->ctx, P, G, tau, (cudaStream_t)stream, nullptr);
+}
+
+LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long long *quartets) {
+  if (!m || !P || !G) return set_error("NULL argument"), LRB_ERR_INPUT;
+  const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
+  cudaStream_t st = nullptr;
+  double *dP = nullptr, *dG = nullptr;
+  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
+      cudaMallocAsync((void **)&dG, nn * 8, st) != cudaSuccess)
+    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
+  FockStats fs;
+  int rc = fock_build(m->ctx, dP, dG, tau, st, &fs);
+  if (!rc) cudaMemcpyAsync(G, dG, nn * 8, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dP, st);
+  cudaFreeAsync(dG, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
+  if (quartets) *quartets = fs.quartets;
+  return rc;
+}
+
+LRB_API int lrb_scf(LrbMol *m, long long nelec, const LrbScfOptions *opt, LrbScfResult *res,
+                    double *P_out, const double *P0) {
+  if (!m) return set_error("NULL molecule"), LRB_ERR_INPUT;
+  ScfOptions o;
+  if (opt) {
+    o.max_iter = opt->max_iter; o.conv = opt->conv; o.guess = opt->guess; o.diis = opt->diis;
+    o.tau = opt->tau;
+  }
+  ScfResult r;
+  const int rc = scf_run(m->ctx, (size_t)nelec, o, &r, P_out, P0, nullptr);
+  if (res) {
+    res->energy = r.energy; res->e_nuc = r.e_nuc; res->delta = r.delta; res->fock_ms = r.fock_ms;
+    res->wall_ms = r.wall_ms; res->iterations = r.iterations; res->converged = r.converged;
+    res->quartets = r.quartets;
+  }
+  return rc;
+}
+
+LRB_API int lrb_energy(LrbMol *m, const double *P, double tau, double *E) {
+  if (!m || !P || !E) return set_error("NULL argument"), LRB_ERR_INPUT;
+  return energy_at(m->ctx, P, tau, E, nullptr);
+}
+
+LRB_API int lrb_int1e(LrbMol *m, int typec, int coord, double *out) {
+  if (!m || !out) return set_error("NULL argument"), LRB_ERR_INPUT;
+  if (typec < 0 || typec > 2 || coord < 0 || coord > 1) return set_error("bad typec/coord"), LRB_ERR_INPUT;
+  MolCtx &c = m->ctx;
+  int n = 0;
+  for (int s = 0; s < c.nbas; ++s) n += shell_dim(coord, c.h_bas.data(), s);
+  cudaStream_t st = nullptr;
+  double *d = nullptr;
+  if (cudaMallocAsync((void **)&d, sizeof(double) * (size_t)n * n, st) != cudaSuccess)
+    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  double c2s[5 * 9 * 15];
+  fill_c2s(c2s);
+  int rc = int1e_device(typec, coord, c.atm, c.natm, c.bas, c.nbas, c.env, c.h_bas.data(), d, st, c2s);
+  if (!rc) cudaMemcpyAsync(out, d, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(d, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
+  return rc;
+}
+
+// ---- p2c.rs shapes: inputs as (pointer, length), results malloc'd or in-band
+static LrbMol *mol_from_p2c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                            size_t env_l) {
+  LrbMol *m = nullptr;
+  if (lrb_mol_create(&m, atm_p, (int)(atm_l / 6), bas_p, (int)(bas_l / 8), env_p, (long long)env_l))
+    return nullptr;
+  return m;
+}
+
+double *int1e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, size_t env_l,
+                int coord, int typec) {
+  LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
+  if (!m) return nullptr;
+  int n = 0;
+  for (int s = 0; s < (int)(bas_l / 8); ++s) n += shell_dim(coord, bas_p, s);
+  double *out = (double *)std::malloc(sizeof(double) * (size_t)n * n);
+  if (!out || lrb_int1e(m, typec, coord, out)) {
+    std::free(out);
+    out = nullptr;
+  }
+  lrb_mol_destroy(m);
+  return out;
+}
+
+double *density_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, size_t env_l,
+                  size_t nelec, int imax, double conv) {
+  LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
+  if (!m) return nullptr;
+  const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
+  double *P = (double *)std::malloc(sizeof(double) * nn);
+  LrbScfOptions o{imax, conv, 0, 0, 0.0};
+  if (!P || lrb_scf(m, (long long)nelec, &o, nullptr, P, nullptr)) {
+    std::free(P);
+    P = nullptr;
+  }
+  lrb_mol_destroy(m);
+  return P;
+}
+
+double energy_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, size_t env_l,
+                double *P_p, size_t P_l) {
+  LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
+  if (!m) return NAN;
+  double E = NAN;
+  if ((size_t)m->ctx.nao * m->ctx.nao != P_l || lrb_energy(m, P_p, 0.0, &E)) E = NAN;
+  lrb_mol_destroy(m);
+  return E;
+}
+
+double scf_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, size_t env_l,
+             size_t nelec, int imax, double conv) {
+  LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
+  if (!m) return NAN;
+  LrbScfOptions o{imax, conv, 0, 0, 0.0};
+  LrbScfResult r;
+  const int rc = lrb_scf(m, (long long)nelec, &o, &r, nullptr, nullptr);
+  lrb_mol_destroy(m);
+  return rc ? NAN : r.energy;
 }
 
 }  // extern "C"

@@ -45,7 +45,8 @@ __global__ void k_fp64_probe(double *sink, int iters, double a, double b) {
   for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
   for (int i = 0; i < iters; ++i) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+    for (int k = 0; k < 8; ++k)
+      asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(x[k]) : "d"(a), "d"(b));
   }
   double s = 0.0;
 #pragma unroll

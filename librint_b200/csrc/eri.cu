@@ -164,7 +164,7 @@ __global__ void k_class_starts(const unsigned *__restrict__ keys, long long nq, 
 // Electronic-Structure Theory", eqs. 6.4.47-6.4.50, scaled by
 // sqrt((2l+1)/(4 pi)); s and p are the identity (p kept as x, y, z), the
 // reference's table is src/cart2sph.rs:26.
-static void fill_c2s(double *c) {
+void fill_c2s(double *c) {
   auto fact = [](int n) { double r = 1.0; for (int i = 2; i <= n; ++i) r *= i; return r; };
   auto bin = [](int n, int k) {
     if (k < 0 || k > n) return 0.0;
@@ -201,7 +201,7 @@ static void fill_c2s(double *c) {
 
 ClassEntry g_classes[NCLASS];
 
-static const ClassEntry *class_table() {
+const ClassEntry *class_table() {
   static bool init = false;
   if (!init) {
     double h[C2S_L * C2S_M * C2S_C];
@@ -213,8 +213,9 @@ static const ClassEntry *class_table() {
     eri_register_bra4(g_classes, h);
     eri_register_bra5(g_classes, h);
     for (int c = 0; c < NCLASS; ++c)
-      cudaFuncSetAttribute(g_classes[c].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)g_classes[c].smem);
+      for (int m = 0; m < 3; ++m)
+        cudaFuncSetAttribute(g_classes[c].fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)g_classes[c].smem[m]);
     init = true;
   }
   return g_classes;
@@ -330,7 +331,7 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
     prm.order = idx2 + cls_begin[c];
     prm.njobs = (int)(end - cls_begin[c]);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn, ERI_THREADS, ce.smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[0], ERI_THREADS, ce.smem[0]);
     if (per_sm < 1) per_sm = 1;
     const long long tasks = (prm.njobs + ce.slots - 1) / ce.slots;
     long long grid = (long long)nsm * per_sm;
@@ -342,8 +343,9 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
       cudaEventCreate(&rec.stop);
       cudaEventRecord(rec.start, st);
     }
-    ce.fn<<<(unsigned)grid, ERI_THREADS, ce.smem, st>>>(prm, rys + RYS_TAB_OFFSET[ce.nr],
-                                                         counters + c);
+    FockParams nofock{};
+    ce.fn[0]<<<(unsigned)grid, ERI_THREADS, ce.smem[0], st>>>(prm, nofock, rys + RYS_TAB_OFFSET[ce.nr],
+                                                              counters + c);
     LRB_CK(cudaGetLastError());
     ++eng.launches;
     if (eng.profile) {

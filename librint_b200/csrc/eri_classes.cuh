@@ -17,11 +17,11 @@ __host__ __device__ inline int class_id(int li, int lj, int lk, int ll) {
 constexpr int NPAIRCLS = (ERI_LMAX + 1) * (ERI_LMAX + 2) / 2;
 constexpr int NCLASS = NPAIRCLS * (NPAIRCLS + 1) / 2;
 
-using EriKernelFn = void (*)(EriParams, const double *, int *);
+using EriKernelFn = void (*)(EriParams, FockParams, const double *, int *);
 
 struct ClassEntry {
-  EriKernelFn fn;
-  size_t smem;
+  EriKernelFn fn[3];     // output (FP64), Fock digestion FP64, Fock digestion FP32
+  size_t smem[3];
   int slots, nr;
 };
 
@@ -29,12 +29,20 @@ template <int LI, int LJ, int LK, int LL>
 ClassEntry make_entry() {
   using C = EriClass<LI, LJ, LK, LL>;
   ClassEntry e;
-  e.fn = k_eri_out<LI, LJ, LK, LL>;
-  e.smem = EriLayout<C>::SMEM;
+  e.fn[0] = k_eri<LI, LJ, LK, LL, 0>;
+  e.fn[1] = k_eri<LI, LJ, LK, LL, 1>;
+  e.fn[2] = k_eri<LI, LJ, LK, LL, 1, float>;
+  e.smem[0] = EriLayout<C, 0>::SMEM;
+  e.smem[1] = EriLayout<C, 1>::SMEM;
+  e.smem[2] = EriLayout<C, 1>::SMEM;
   e.slots = C::SLOTS;
   e.nr = C::NR;
   return e;
 }
+
+// Class table (instantiates on first use; uploads the cart->sph table).
+const ClassEntry *class_table();
+void fill_c2s(double *c);
 
 void eri_register_bra0(ClassEntry *t, const double *c2s_host);   // (ss|
 void eri_register_bra1(ClassEntry *t, const double *c2s_host);   // (ps|

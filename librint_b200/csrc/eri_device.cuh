@@ -109,6 +109,23 @@ struct QuartetJob {
   int s_i, s_j, s_k, s_l; // output strides of the canonical indices
 };
 
+// A shell pair of a molecule's pair table (oriented l_i >= l_j).
+struct PairInfo {
+  int ish, jsh;           // shells
+  int pp_off, npp;        // primitive pairs in the PrimPair array
+};
+
+// Fock-build extras: density and the unsymmetrised accumulators
+// (G = J + J^T - (K + K^T)/2 is formed afterwards).
+struct FockParams {
+  const int2 *jobs;       // (bra pair, ket pair) with bra class >= ket class
+  const PairInfo *pairs;
+  const int *aooff;       // first AO of each shell
+  const double *P;        // n x n row-major
+  double *J, *K;          // n x n accumulators
+  int n;
+};
+
 struct EriParams {
   const QuartetJob *jobs;
   const int *order;       // jobs to run, in launch order
@@ -121,6 +138,17 @@ struct EriParams {
 };
 
 // ------------------------------------------------------------------ roots
+// Table geometry (segments of width 4 up to 43 + 5n), usable in device code.
+__host__ __device__ constexpr int rys_nseg(int n) { return (43 + 5 * n + 3) / 4; }
+__host__ __device__ constexpr int rys_tab_offset(int n) {
+  int o = 0;
+  for (int k = 1; k < n; ++k) o += rys_nseg(k) * 2 * k * RYS_NCOEF;
+  return o;
+}
+static_assert(rys_tab_offset(5) == RYS_TAB_OFFSET[5] && rys_tab_offset(10) == RYS_TAB_OFFSET[10] &&
+                  rys_nseg(9) == RYS_TAB_NSEG[9],
+              "table geometry out of sync with rys_tables.h");
+
 // Rys nodes/weights for N roots at x from the shared-memory table `tab`
 // (layout of rys_tables.h for this N).  Function f < N is u_f, f >= N is
 // w_{f-N}.
@@ -136,7 +164,7 @@ __device__ __forceinline__ double rys_function(const double *tab, double x, int 
     return RYS_LARGEX_W[off + f - N] * sqrt(0.78539816339744831 / x);  // pi/4
   }
   // clamp keeps the table read in bounds even for NaN input (NaN propagates)
-  constexpr int NSEG = (43 + 5 * N + 3) / 4;
+  constexpr int NSEG = rys_nseg(N);
   static_assert(RYS_SEG_WIDTH == 4.0, "segment count assumes width 4");
   int seg = (int)(x * (1.0 / RYS_SEG_WIDTH));
   seg = seg < 0 ? 0 : (seg >= NSEG ? NSEG - 1 : seg);

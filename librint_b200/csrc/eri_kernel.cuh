@@ -1,6 +1,23 @@
-// Templated Rys ERI kernel for one canonical angular class (see
-// eri_device.cuh for the decomposition).  Output mode writes every
-// contracted shell quartet as a libcint block (cartesian or spherical).
+// Templated Rys ERI kernel for one canonical angular class (LI LJ | LK LL),
+// LI >= LJ, LK >= LL, (LI,LJ) >= (LK,LL).
+//
+// Per primitive quartet and Rys root (reference src/g2e.rs:5539-5679 and
+// src/eri.rs:263-399):
+//   * roots/weights u_r, w_r from the piecewise tables staged in shared
+//     memory (one lane per node or weight);
+//   * one lane per (root, axis) builds the 2D table V(n, m) on the base
+//     centres A (bra) and C (ket) -- i if LI > LJ else j, k if LK > LL else
+//     l, as src/g2e.rs:113-181 chooses -- then shifts it to the partners by
+//     the horizontal recurrences on these 1D arrays, giving G[a][b][c][d];
+//   * gout: every lane owns one row of the final cartesian block (the smaller
+//     of the bra/ket sides) and accumulates all columns in registers:
+//     I(row, col) += Gx Gy Gz (src/cint2e.rs:2456-2895).
+// The recurrences stay per primitive (as the reference does) because shifting
+// after contraction acts on 3D products and loses ~2 digits for distant
+// centres.  A warp holds SLOTS = 32 / rows quartets; rows beyond 32 ((dd|dd))
+// are split across lanes by columns.  The epilogue transforms to spherical
+// harmonics and writes libcint blocks (MODE 0) or digests the cartesian block
+// into J/K (MODE 1).
 #pragma once
 #include "eri_device.cuh"
 
@@ -18,57 +35,193 @@ struct EriClass {
   static constexpr int LC = KB ? LK : LL, LD = KB ? LL : LK;
   static constexpr int NAB = LA + LB, NCD = LC + LD;
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
-  static constexpr int NROW = range_count(LA, NAB);   // e components
-  static constexpr int NCOL = range_count(LC, NCD);   // f components
-  static constexpr int SLOTS = 32 / NROW;
-  static constexpr int VSZ = (NAB + 1) * (NCD + 1);
+  static constexpr int NI = ncart(LI), NJ = ncart(LJ), NK = ncart(LK), NL = ncart(LL);
+  static constexpr int NBRA = NI * NJ, NKET = NK * NL;
+  static constexpr bool ROWKET = NKET <= NBRA;          // rows are ket components
+  static constexpr int NROWS = ROWKET ? NKET : NBRA;
+  static constexpr int NCOLS = ROWKET ? NBRA : NKET;
+  static constexpr int LANES = NROWS < 32 ? NROWS : 32;   // lanes per slot
+  static constexpr int SLOTS = 32 / LANES;
+  static constexpr int EXTRA = NROWS > 32 ? (NROWS - 32) * NCOLS : 0;   // split elements
+  static constexpr int NEX = (EXTRA + 31) / 32;                          // per lane
+  // G[a][b][c][d] sizes; row-side indices first, column side contiguous
+  static constexpr int BSZ = (LA + 1) * (LB + 1), KSZ = (LC + 1) * (LD + 1);
+  static constexpr int GSZ = BSZ * KSZ;
+  static constexpr int CW = ROWKET ? BSZ : KSZ;   // column values per axis
+  static constexpr int TSZ = BSZ * (NCD + 1);     // after the bra shift
+
+  // component c of cartesian function n of momentum l
+  static constexpr int cc(int l, int n, int axis) {
+    return axis == 0 ? cart_x(l, n) : (axis == 1 ? cart_y(l, n) : cart_z(l, n));
+  }
+  // bra (ic, jc) -> offset of (a, b) in a BSZ block for one axis
+  static constexpr int bra_off(int ic, int jc, int axis) {
+    return IB ? cc(LI, ic, axis) * (LB + 1) + cc(LJ, jc, axis)
+              : cc(LJ, jc, axis) * (LB + 1) + cc(LI, ic, axis);
+  }
+  static constexpr int ket_off(int kc, int lc, int axis) {
+    return KB ? cc(LK, kc, axis) * (LD + 1) + cc(LL, lc, axis)
+              : cc(LL, lc, axis) * (LD + 1) + cc(LK, kc, axis);
+  }
+  // column k (compile time) -> offset inside a row's CW values, per axis
+  static constexpr int col_off(int k, int axis) {
+    return ROWKET ? bra_off(k % NI, k / NI, axis) : ket_off(k % NK, k / NK, axis);
+  }
 };
 
-template <class C>
+template <class C, int MODE = 0>
 struct EriLayout {
-  static constexpr int NKC = ncart(C::LK) * ncart(C::LL);   // ket (cart) columns
-  // per-slot doubles: VRR tables + roots during the primitive loop; in the
-  // epilogue the contracted rows F[e][f] and the half-transformed E[e][kl]
-  static constexpr int LOOP = C::NR * 3 * C::VSZ + 2 * C::NR;
-  static constexpr int EPI = C::NROW * (C::NCOL + NKC);
+  static constexpr int NKO_MAX = C::NKET;   // cartesian >= spherical
+  // per-slot doubles: roots (2 NR), G (NR*3*GSZ) and per-unit bra-shift
+  // scratch (3*NR*TSZ) in the loop; block (NBRA*NKET) + ket-transformed
+  // block (NBRA*NKO) in the epilogue
+  static constexpr int LOOP = 2 * C::NR + C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ;
+  static constexpr int EPI = C::NBRA * C::NKET + (MODE == 0 ? C::NBRA * NKO_MAX : 0);
   static constexpr int SLOT = LOOP > EPI ? LOOP : EPI;
   static constexpr int WARP = C::SLOTS * SLOT;
   static constexpr int TAB = (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR]);
-  static constexpr size_t SMEM = sizeof(double) * (size_t)(TAB + ERI_WARPS * WARP);
+  static constexpr int C2S = 3 * 5 * 6;    // l <= 2, m, cart
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(TAB + C2S + ERI_WARPS * WARP);
 };
 
-// 2D VRR of one (root, axis) into V[n*(NCD+1)+m] (reference
-// src/g2e.rs:316-506 and src/eri.rs:308-365, built on the base centres).
-template <int NAB, int NCD>
-__device__ __forceinline__ void vrr_2d(double *V, double v00, double cn, double cm,
-                                       double b10, double b01, double b00) {
-  double g[NAB + 1][NCD + 1];
+// cart->sph coefficients, c2s[l][m][c] for l <= 4 (filled by the host from
+// the real-solid-harmonic closed form; libcint order and normalisation).
+// One copy per translation unit; each unit's registration uploads it.
+constexpr int C2S_L = 5, C2S_M = 9, C2S_C = 15;
+static __constant__ double c_c2s[C2S_L * C2S_M * C2S_C];
+
+// ---------------------------------------------------------------- unit
+// One (root, axis): 2D VRR on (A, C), bra shift A->B for every m, ket shift
+// C->D, result G[row side][column side] written to shared memory.
+template <class C, typename R>
+__device__ __forceinline__ void vrr_hrr_unit(R *G, R *T, R v00, R cn, R cm, R b10, R b01, R b00,
+                                             R ab, R cd) {
+  constexpr int NAB = C::NAB, NCD = C::NCD, LA = C::LA, LB = C::LB, LC = C::LC, LD = C::LD;
+  R g[NAB + 1][NCD + 1];
   g[0][0] = v00;
 #pragma unroll
   for (int m = 1; m <= NCD; ++m) {
-    double v = cm * g[0][m - 1];
-    if (m > 1) v = fma((m - 1) * b01, g[0][m - 2], v);
+    R v = cm * g[0][m - 1];
+    if (m > 1) v = fma(R(m - 1) * b01, g[0][m - 2], v);
     g[0][m] = v;
   }
 #pragma unroll
-  for (int n = 1; n <= NAB; ++n) {
+  for (int n = 1; n <= NAB; ++n)
 #pragma unroll
     for (int m = 0; m <= NCD; ++m) {
-      double v = cn * g[n - 1][m];
-      if (n > 1) v = fma((n - 1) * b10, g[n - 2][m], v);
-      if (m > 0) v = fma(m * b00, g[n - 1][m - 1], v);
+      R v = cn * g[n - 1][m];
+      if (n > 1) v = fma(R(n - 1) * b10, g[n - 2][m], v);
+      if (m > 0) v = fma(R(m) * b00, g[n - 1][m - 1], v);
       g[n][m] = v;
     }
+  // bra shift per m column: h[a][b] from g[a+b'][m], (x-B) = (x-A) + (A-B)
+#pragma unroll
+  for (int m = 0; m <= NCD; ++m) {
+    R h[NAB + 1][LB + 1];
+#pragma unroll
+    for (int n = 0; n <= NAB; ++n) h[n][0] = g[n][m];
+#pragma unroll
+    for (int b = 1; b <= LB; ++b)
+#pragma unroll
+      for (int a = 0; a <= NAB - b; ++a) h[a][b] = fma(ab, h[a][b - 1], h[a + 1][b - 1]);
+#pragma unroll
+    for (int a = 0; a <= LA; ++a)
+#pragma unroll
+      for (int b = 0; b <= LB; ++b) T[(a * (LB + 1) + b) * (NCD + 1) + m] = h[a][b];
   }
+  // ket shift per (a, b): k[c][d] from T[a][b][c+d']
 #pragma unroll
-  for (int n = 0; n <= NAB; ++n)
+  for (int a = 0; a <= LA; ++a)
 #pragma unroll
-    for (int m = 0; m <= NCD; ++m) V[n * (NCD + 1) + m] = g[n][m];
+    for (int b = 0; b <= LB; ++b) {
+      R k[NCD + 1][LD + 1];
+#pragma unroll
+      for (int m = 0; m <= NCD; ++m) k[m][0] = T[(a * (LB + 1) + b) * (NCD + 1) + m];
+#pragma unroll
+      for (int d = 1; d <= LD; ++d)
+#pragma unroll
+        for (int c = 0; c <= NCD - d; ++c) k[c][d] = fma(cd, k[c][d - 1], k[c + 1][d - 1]);
+#pragma unroll
+      for (int c = 0; c <= LC; ++c)
+#pragma unroll
+        for (int d = 0; d <= LD; ++d) {
+          const int bi = a * (LB + 1) + b, ki = c * (LD + 1) + d;
+          G[C::ROWKET ? ki * C::BSZ + bi : bi * C::KSZ + ki] = k[c][d];
+        }
+    }
 }
 
-// ---------------------------------------------------------------- epilogue
-// Runtime helpers (the epilogue runs once per contracted shell quartet, so
-// compact code beats full unrolling here).
+// acc[k] += x[col_x(k)] y[col_y(k)] z[col_z(k)] for all columns (compile-time
+// offsets by recursion).
+template <class C, typename R, int K>
+__device__ __forceinline__ void gout_cols(R (&acc)[C::NCOLS], const R (&x)[C::CW],
+                                          const R (&y)[C::CW], const R (&z)[C::CW]) {
+  if constexpr (K < C::NCOLS) {
+    constexpr int X = C::col_off(K, 0), Y = C::col_off(K, 1), Z = C::col_off(K, 2);
+    acc[K] = fma(x[X] * y[Y], z[Z], acc[K]);
+    gout_cols<C, R, K + 1>(acc, x, y, z);
+  }
+}
+
+// ---------------------------------------------------------------- digestion
+// J/K digestion of one cartesian block B[a + NI*(b + NJ*(c + NK*d))] with
+// the degeneracy weight w of its canonical shell quartet:
+//   Jacc[ab] += 2w sum_cd B P[cd],  Jacc[cd] += 2w sum_ab B P[ab],
+//   Kacc[ac] += w sum_bd B P[bd],   Kacc[bc] += w sum_ad B P[ad],
+//   Kacc[ad] += w sum_bc B P[bc],   Kacc[bd] += w sum_ac B P[ac];
+// G = (Jacc + Jacc^T) - (Kacc + Kacc^T)/2 then equals the reference's
+// G[mu nu] = sum P[ls](mu nu|s l) - 1/2 sum P[ns](mu l|s n) (src/scf.rs:379-391).
+template <int NI, int NJ, int NK, int NL, typename R>
+__device__ __forceinline__ void fock_digest(const R *B, const QuartetJob &q, double w,
+                                            const FockParams &fk, int rho, int nlanes) {
+  const int n = fk.n;
+  const int oi = fk.aooff[q.ish], oj = fk.aooff[q.jsh], ok = fk.aooff[q.ksh], ol = fk.aooff[q.lsh];
+  const double *P = fk.P;
+  auto blk = [&](int a, int b, int c, int d) { return B[a + NI * (b + NJ * (c + NK * d))]; };
+  for (int t = rho; t < NI * NJ; t += nlanes) {          // J[ab]
+    const int a = t % NI, b = t / NI;
+    R s = 0;
+    for (int d = 0; d < NL; ++d)
+      for (int c = 0; c < NK; ++c) s = fma(blk(a, b, c, d), (R)P[(long long)(ok + c) * n + ol + d], s);
+    atomicAdd(&fk.J[(long long)(oi + a) * n + oj + b], 2.0 * w * (double)s);
+  }
+  for (int t = rho; t < NK * NL; t += nlanes) {          // J[cd]
+    const int c = t % NK, d = t / NK;
+    R s = 0;
+    for (int b = 0; b < NJ; ++b)
+      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), (R)P[(long long)(oi + a) * n + oj + b], s);
+    atomicAdd(&fk.J[(long long)(ok + c) * n + ol + d], 2.0 * w * (double)s);
+  }
+  for (int t = rho; t < NI * NK; t += nlanes) {          // K[ac]
+    const int a = t % NI, c = t / NI;
+    R s = 0;
+    for (int d = 0; d < NL; ++d)
+      for (int b = 0; b < NJ; ++b) s = fma(blk(a, b, c, d), (R)P[(long long)(oj + b) * n + ol + d], s);
+    atomicAdd(&fk.K[(long long)(oi + a) * n + ok + c], w * (double)s);
+  }
+  for (int t = rho; t < NJ * NK; t += nlanes) {          // K[bc]
+    const int b = t % NJ, c = t / NJ;
+    R s = 0;
+    for (int d = 0; d < NL; ++d)
+      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), (R)P[(long long)(oi + a) * n + ol + d], s);
+    atomicAdd(&fk.K[(long long)(oj + b) * n + ok + c], w * (double)s);
+  }
+  for (int t = rho; t < NI * NL; t += nlanes) {          // K[ad]
+    const int a = t % NI, d = t / NI;
+    R s = 0;
+    for (int c = 0; c < NK; ++c)
+      for (int b = 0; b < NJ; ++b) s = fma(blk(a, b, c, d), (R)P[(long long)(oj + b) * n + ok + c], s);
+    atomicAdd(&fk.K[(long long)(oi + a) * n + ol + d], w * (double)s);
+  }
+  for (int t = rho; t < NJ * NL; t += nlanes) {          // K[bd]
+    const int b = t % NJ, d = t / NJ;
+    R s = 0;
+    for (int c = 0; c < NK; ++c)
+      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), (R)P[(long long)(oi + a) * n + ok + c], s);
+    atomicAdd(&fk.K[(long long)(oj + b) * n + ol + d], w * (double)s);
+  }
+}
+
 __device__ __forceinline__ void cart_comp_rt(int l, int n, int &x, int &y, int &z) {
   int t = 0;
   while ((t + 1) * (t + 2) / 2 <= n) ++t;
@@ -76,76 +229,97 @@ __device__ __forceinline__ void cart_comp_rt(int l, int n, int &x, int &y, int &
   y = t - z;
   x = l - t;
 }
-__device__ __forceinline__ int range_index_rt(int lo, int x, int y, int z) {
-  const int e = x + y + z;
-  const int off = e * (e + 1) * (e + 2) / 6 - lo * (lo + 1) * (lo + 2) / 6;
-  return off + (y + z) * (y + z + 1) / 2 + z;
-}
-__device__ __forceinline__ int binom_rt(int n, int k) {
-  return k == 0 || k == n ? 1 : (n == 2 ? 2 : (n == 3 ? 3 : (n == 4 ? (k == 2 ? 6 : 4) : n)));
-}
-// (x-R_B)^b = sum_t C(b,t) (R_A-R_B)^(b-t) (x-R_A)^t per axis applied to a
-// row of values indexed by momenta lo.. on the base centre (reference
-// src/g2e.rs:507-909 applies the same shift recursively).
-__device__ __forceinline__ double ipow_rt(double x, int k) {
-  double r = 1.0;
-  for (int i = 0; i < k; ++i) r *= x;
-  return r;
-}
-__device__ __forceinline__ double hrr_rt(const double *src, int stride, int lo, int ax, int ay,
-                                         int az, int bx, int by, int bz, double dx, double dy,
-                                         double dz) {
-  double s = 0.0;
-  for (int tx = 0; tx <= bx; ++tx)
-    for (int ty = 0; ty <= by; ++ty)
-      for (int tz = 0; tz <= bz; ++tz) {
-        const double c = (double)(binom_rt(bx, tx) * binom_rt(by, ty) * binom_rt(bz, tz)) *
-                         ipow_rt(dx, bx - tx) * ipow_rt(dy, by - ty) * ipow_rt(dz, bz - tz);
-        s = fma(c, src[stride * range_index_rt(lo, ax + tx, ay + ty, az + tz)], s);
-      }
-  return s;
-}
 
-// cart->sph coefficients, c2s[l][m][c] for l <= 4 (filled by the host from
-// the real-solid-harmonic closed form; libcint order and normalisation).
-constexpr int C2S_L = 5, C2S_M = 9, C2S_C = 15;
-// One copy per translation unit (no relocatable device code); each unit's
-// class-registration function uploads it.
-static __constant__ double c_c2s[C2S_L * C2S_M * C2S_C];
-__device__ __forceinline__ double c2s(int l, int m, int c) { return c_c2s[(l * C2S_M + m) * C2S_C + c]; }
-
-// Persistent kernel: warps pull tasks (SLOTS quartets each) from *counter.
-template <int LI, int LJ, int LK, int LL>
+// ---------------------------------------------------------------- kernel
+// Persistent: warps pull tasks (SLOTS quartets each) from *counter.
+// MODE 0 writes libcint blocks; MODE 1 digests each block into J/K.
+// R is the arithmetic type of the recurrences, the products and the
+// digestion (double, or float for the mixed-precision Fock build); roots,
+// weights and pair data are always evaluated in FP64 and rounded after.
+template <int LI, int LJ, int LK, int LL, int MODE, typename R = double>
 __global__ void __launch_bounds__(ERI_THREADS)
-k_eri_out(EriParams prm, const double *__restrict__ rys_tab_n, int *counter) {
+k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *counter) {
   using C = EriClass<LI, LJ, LK, LL>;
-  using L = EriLayout<C>;
+  using L = EriLayout<C, MODE>;
+  static_assert(MODE == 1 || sizeof(R) == 8, "output mode is FP64");
   extern __shared__ double smem[];
   double *tab = smem;
-  // stage this class's root table (same for every CTA)
+  double *c2s_s = smem + L::TAB;            // [3][5][6]
   for (int i = threadIdx.x; i < L::TAB; i += blockDim.x) tab[i] = rys_tab_n[i];
+  for (int i = threadIdx.x; i < L::C2S; i += blockDim.x) {
+    const int l = i / 30, m = (i / 6) % 5, c = i % 6;
+    c2s_s[i] = c_c2s[(l * C2S_M + m) * C2S_C + c];
+  }
   __syncthreads();
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double *wbuf = smem + L::TAB + warp * L::WARP;
-  const int slot = lane / C::NROW;
-  const int rho = lane - slot * C::NROW;
+  double *wbuf = smem + L::TAB + L::C2S + warp * L::WARP;
+  const int slot = lane / C::LANES;
+  const int rho = lane - slot * C::LANES;
   const bool lane_live = slot < C::SLOTS;
   const int myslot = lane_live ? slot : C::SLOTS - 1;
   double *sb = wbuf + myslot * L::SLOT;        // this slot's area
-  double *Vs = sb;                             // [NR][3][VSZ]
-  double *RW = sb + C::NR * 3 * C::VSZ;        // [2*NR]
-  // row components of this lane
-  int ex = 0, ey = 0, ez = 0;
+  double *RW = sb;                             // [2*NR] FP64 roots and weights
+  R *G = reinterpret_cast<R *>(sb + 2 * C::NR);            // [NR][3][GSZ]
+  R *Tsc = G + C::NR * 3 * C::GSZ;                         // [3*NR][TSZ]
+
+  // row offsets of this lane (row side indices, per axis)
+  int roff[3] = {0, 0, 0};
   {
-    int r = rho < C::NROW ? rho : 0, e = C::LA;
-    while (r >= ncart(e)) { r -= ncart(e); ++e; }
-    cart_comp_rt(e, r, ex, ey, ez);
+    const int r = rho < C::NROWS ? rho : 0;
+    const int p = C::ROWKET ? C::NK : C::NI;
+    const int lp = C::ROWKET ? C::LK : C::LI, lq = C::ROWKET ? C::LL : C::LJ;
+    int px, py, pz, qx, qy, qz;
+    cart_comp_rt(lp, r % p, px, py, pz);
+    cart_comp_rt(lq, r / p, qx, qy, qz);
+    const int pc[3] = {px, py, pz}, qc[3] = {qx, qy, qz};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      if (C::ROWKET) {   // row = (kc, lc) -> (c, d)
+        const int c = C::KB ? pc[ax] : qc[ax], d = C::KB ? qc[ax] : pc[ax];
+        roff[ax] = (c * (C::LD + 1) + d) * C::BSZ;
+      } else {           // row = (ic, jc) -> (a, b)
+        const int a = C::IB ? pc[ax] : qc[ax], b = C::IB ? qc[ax] : pc[ax];
+        roff[ax] = (a * (C::LB + 1) + b) * C::KSZ;
+      }
+    }
   }
-  const bool sph = prm.sph != 0;
-  constexpr int NI = ncart(LI), NJ = ncart(LJ), NK = ncart(LK), NL = ncart(LL);
-  const int NIo = sph ? nsph(LI) : NI, NJo = sph ? nsph(LJ) : NJ;
-  const int NKo = sph ? nsph(LK) : NK, NLo = sph ? nsph(LL) : NL;
+  // extra elements (rows >= 32, column split): row and column offsets
+  int xrow[C::NEX > 0 ? C::NEX : 1], xoff[C::NEX > 0 ? C::NEX : 1][3];
+  if constexpr (C::NEX > 0) {
+#pragma unroll
+    for (int k = 0; k < C::NEX; ++k) {
+      const int e = lane + 32 * k;
+      xrow[k] = e < C::EXTRA ? 32 + e / C::NCOLS : -1;
+      const int col = e < C::EXTRA ? e % C::NCOLS : 0;
+      const int row = e < C::EXTRA ? 32 + e / C::NCOLS : 0;
+      const int p = C::ROWKET ? C::NK : C::NI;
+      const int lp = C::ROWKET ? C::LK : C::LI, lq = C::ROWKET ? C::LL : C::LJ;
+      const int cp = C::ROWKET ? C::NI : C::NK;
+      const int lcp = C::ROWKET ? C::LI : C::LK, lcq = C::ROWKET ? C::LJ : C::LL;
+      int px, py, pz, qx, qy, qz, ux, uy, uz, vx, vy, vz;
+      cart_comp_rt(lp, row % p, px, py, pz);
+      cart_comp_rt(lq, row / p, qx, qy, qz);
+      cart_comp_rt(lcp, col % cp, ux, uy, uz);
+      cart_comp_rt(lcq, col / cp, vx, vy, vz);
+      const int pc[3] = {px, py, pz}, qc[3] = {qx, qy, qz}, uc[3] = {ux, uy, uz}, vc[3] = {vx, vy, vz};
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        if (C::ROWKET) {
+          const int c = C::KB ? pc[ax] : qc[ax], d = C::KB ? qc[ax] : pc[ax];
+          const int a = C::IB ? uc[ax] : vc[ax], b = C::IB ? vc[ax] : uc[ax];
+          xoff[k][ax] = (c * (C::LD + 1) + d) * C::BSZ + a * (C::LB + 1) + b;
+        } else {
+          const int a = C::IB ? pc[ax] : qc[ax], b = C::IB ? qc[ax] : pc[ax];
+          const int c = C::KB ? uc[ax] : vc[ax], d = C::KB ? vc[ax] : uc[ax];
+          xoff[k][ax] = (a * (C::LB + 1) + b) * C::KSZ + c * (C::LD + 1) + d;
+        }
+      }
+    }
+  }
+  const bool sph = MODE == 0 && prm.sph != 0;
+  const int NIo = sph ? nsph(LI) : C::NI, NJo = sph ? nsph(LJ) : C::NJ;
+  const int NKo = sph ? nsph(LK) : C::NK, NLo = sph ? nsph(LL) : C::NL;
   const int NKO = NKo * NLo, NBO = NIo * NJo;
   const int ntasks = (prm.njobs + C::SLOTS - 1) / C::SLOTS;
 
@@ -157,8 +331,21 @@ k_eri_out(EriParams prm, const double *__restrict__ rys_tab_n, int *counter) {
     const int jslot = task * C::SLOTS + myslot;
     const bool have = lane_live && jslot < prm.njobs;
     QuartetJob job;
-    if (have) job = prm.jobs[prm.order[jslot]];
-    else { job.nij = 0; job.nkl = 0; job.pij_off = job.pkl_off = 0; }
+    double wdeg = 1.0;   // Fock mode: 1/2 per coinciding shell / pair
+    if (!have) {
+      job.nij = 0; job.nkl = 0; job.pij_off = job.pkl_off = 0;
+    } else if (MODE == 0) {
+      job = prm.jobs[prm.order[jslot]];
+    } else {
+      const int2 jb = fk.jobs[prm.order[jslot]];
+      const PairInfo pb = fk.pairs[jb.x], pk = fk.pairs[jb.y];
+      job.ish = pb.ish; job.jsh = pb.jsh; job.pij_off = pb.pp_off; job.nij = pb.npp;
+      job.ksh = pk.ish; job.lsh = pk.jsh; job.pkl_off = pk.pp_off; job.nkl = pk.npp;
+      job.out_off = 0; job.s_i = job.s_j = job.s_k = job.s_l = 0;
+      if (pb.ish == pb.jsh) wdeg *= 0.5;
+      if (pk.ish == pk.jsh) wdeg *= 0.5;
+      if (jb.x == jb.y) wdeg *= 0.5;
+    }
     const int np = job.nij * job.nkl;
     int npmax = np;
 #pragma unroll
@@ -175,9 +362,12 @@ k_eri_out(EriParams prm, const double *__restrict__ rys_tab_n, int *counter) {
         rC[x] = prm.centers[3 * c + x]; rD[x] = prm.centers[3 * d + x];
       }
     }
-    double acc[C::NCOL];
+    R acc[C::NCOLS];
 #pragma unroll
-    for (int c = 0; c < C::NCOL; ++c) acc[c] = 0.0;
+    for (int c = 0; c < C::NCOLS; ++c) acc[c] = 0;
+    R xacc[C::NEX > 0 ? C::NEX : 1];
+#pragma unroll
+    for (int k = 0; k < (C::NEX > 0 ? C::NEX : 1); ++k) xacc[k] = 0;
 
     int ij = 0, kl = 0;
     for (int p = 0; p < npmax; ++p) {
@@ -199,105 +389,116 @@ k_eri_out(EriParams prm, const double *__restrict__ rys_tab_n, int *counter) {
         fac1 = sqrt(a0 / (a1 * a1 * a1)) * bra.fac * ket.fac;
         pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
         x = a0 * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
-        for (int f = rho; f < 2 * C::NR; f += C::NROW) RW[f] = rys_function<C::NR>(tab, x, f);
+        for (int f = rho; f < 2 * C::NR; f += C::LANES) RW[f] = rys_function<C::NR>(tab, x, f);
       }
       __syncwarp();
       if (run) {
         const double pa[3] = {bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2]};
         const double qc[3] = {ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2]};
-        for (int u = rho; u < 3 * C::NR; u += C::NROW) {
+        const double s_ab = aij + akl, p_ab = aij * akl;
+        for (int u = rho; u < 3 * C::NR; u += C::LANES) {
           const int r = u / 3, ax = u - 3 * r;
           const double u2 = a0 * RW[r];
-          const double tmp4 = 0.5 / (u2 * (aij + akl) + aij * akl);
+          const double tmp4 = 0.5 / (u2 * s_ab + p_ab);
           const double tmp5 = u2 * tmp4;
           const double b10 = tmp5 + tmp4 * akl;
           const double b01 = tmp5 + tmp4 * aij;
           const double cn = pa[ax] - 2.0 * tmp5 * akl * pq[ax];
           const double cm = qc[ax] + 2.0 * tmp5 * aij * pq[ax];
           const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;
-          vrr_2d<C::NAB, C::NCD>(Vs + (r * 3 + ax) * C::VSZ, v00, cn, cm, b10, b01, tmp5);
+          vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, (R)v00, (R)cn, (R)cm,
+                             (R)b10, (R)b01, (R)tmp5, (R)(rA[ax] - rB[ax]), (R)(rC[ax] - rD[ax]));
         }
       }
       __syncwarp();
-      if (run && rho < C::NROW) {
+      if (run) {
 #pragma unroll
         for (int r = 0; r < C::NR; ++r) {
-          const double *vxp = Vs + (r * 3 + 0) * C::VSZ + ex * (C::NCD + 1);
-          const double *vyp = Vs + (r * 3 + 1) * C::VSZ + ey * (C::NCD + 1);
-          const double *vzp = Vs + (r * 3 + 2) * C::VSZ + ez * (C::NCD + 1);
-          double vx[C::NCD + 1], vy[C::NCD + 1], vz[C::NCD + 1];
+          const R *gx = G + (r * 3 + 0) * C::GSZ, *gy = G + (r * 3 + 1) * C::GSZ;
+          const R *gz = G + (r * 3 + 2) * C::GSZ;
+          if (rho < C::NROWS) {
+            R vx[C::CW], vy[C::CW], vz[C::CW];
 #pragma unroll
-          for (int m = 0; m <= C::NCD; ++m) { vx[m] = vxp[m]; vy[m] = vyp[m]; vz[m] = vzp[m]; }
+            for (int m = 0; m < C::CW; ++m) {
+              vx[m] = gx[roff[0] + m]; vy[m] = gy[roff[1] + m]; vz[m] = gz[roff[2] + m];
+            }
+            gout_cols<C, R, 0>(acc, vx, vy, vz);
+          }
+          if constexpr (C::NEX > 0) {
 #pragma unroll
-          for (int c = 0; c < C::NCOL; ++c)
-            acc[c] = fma(vx[range_x(C::LC, c)] * vy[range_y(C::LC, c)], vz[range_z(C::LC, c)], acc[c]);
+            for (int k = 0; k < C::NEX; ++k)
+              if (xrow[k] >= 0) xacc[k] = fma(gx[xoff[k][0]] * gy[xoff[k][1]], gz[xoff[k][2]], xacc[k]);
+          }
         }
       }
       __syncwarp();
     }
 
     // ---------------------------------------------------------- epilogue
-    // HRR after contraction, then cart->sph, per shell quartet.
-    const double cdx = rC[0] - rD[0], cdy = rC[1] - rD[1], cdz = rC[2] - rD[2];
-    const double abx = rA[0] - rB[0], aby = rA[1] - rB[1], abz = rA[2] - rB[2];
-    double *F = sb;                            // [NROW][NCOL]
-    double *E = sb + C::NROW * C::NCOL;        // [NROW][NKO]
-    if (have && rho < C::NROW) {
-#pragma unroll
-      for (int c = 0; c < C::NCOL; ++c) F[rho * C::NCOL + c] = acc[c];
-    }
-    __syncwarp();
+    R *Bk = reinterpret_cast<R *>(sb);           // cartesian block, canonical
     if (have) {
-      // ket: [e|f] -> [e|kl] in output (k fastest) order
-      for (int t = rho; t < C::NROW * NKO; t += C::NROW) {
-        const int e = t / NKO, kap = t - e * NKO;
-        const int ko = kap % NKo, lo = kap / NKo;
-        double v = 0.0;
-        for (int kc = 0; kc < NK; ++kc) {
-          const double ck = sph ? c2s(LK, ko, kc) : (kc == ko ? 1.0 : 0.0);
-          if (ck == 0.0) continue;
-          int kx, ky, kz;
-          cart_comp_rt(LK, kc, kx, ky, kz);
-          for (int lc = 0; lc < NL; ++lc) {
-            const double cl = sph ? c2s(LL, lo, lc) : (lc == lo ? 1.0 : 0.0);
-            if (cl == 0.0) continue;
-            int lx, ly, lz;
-            cart_comp_rt(LL, lc, lx, ly, lz);
-            const double h = C::KB ? hrr_rt(F + e * C::NCOL, 1, C::LC, kx, ky, kz, lx, ly, lz, cdx, cdy, cdz)
-                                   : hrr_rt(F + e * C::NCOL, 1, C::LC, lx, ly, lz, kx, ky, kz, cdx, cdy, cdz);
-            v = fma(ck * cl, h, v);
-          }
+      if (rho < C::NROWS) {
+#pragma unroll
+        for (int c = 0; c < C::NCOLS; ++c)
+          Bk[C::ROWKET ? c + C::NBRA * rho : rho + C::NBRA * c] = acc[c];
+      }
+      if constexpr (C::NEX > 0) {
+#pragma unroll
+        for (int k = 0; k < C::NEX; ++k) {
+          if (xrow[k] < 0) continue;
+          const int e = lane + 32 * k, col = e % C::NCOLS;
+          Bk[C::ROWKET ? col + C::NBRA * xrow[k] : xrow[k] + C::NBRA * col] = xacc[k];
         }
-        E[t] = v;
       }
     }
     __syncwarp();
-    if (have) {
-      // bra: [e|kl] -> (ij|kl), written to global (i fastest -> coalesced)
-      for (int t = rho; t < NKO * NBO; t += C::NROW) {
+    if (MODE == 0 && have) {
+      // ket transform: T2[bra cart][ket out] (identity when cartesian)
+      R *T2 = Bk + C::NBRA * C::NKET;
+      for (int t = rho; t < C::NBRA * NKO; t += C::LANES) {
+        const int kap = t / C::NBRA, bc = t - kap * C::NBRA;
+        const int ko = kap % NKo, lo = kap / NKo;
+        R v = 0;
+        if (!sph) {
+          v = Bk[bc + C::NBRA * (ko + C::NK * lo)];
+        } else {
+          for (int kc = 0; kc < C::NK; ++kc) {
+            const double ck = LK < 2 ? (kc == ko ? 1.0 : 0.0) : c2s_s[(LK * 5 + ko) * 6 + kc];
+            if (ck == 0.0) continue;
+            for (int lc = 0; lc < C::NL; ++lc) {
+              const double cl = LL < 2 ? (lc == lo ? 1.0 : 0.0) : c2s_s[(LL * 5 + lo) * 6 + lc];
+              if (cl == 0.0) continue;
+              v = fma((R)(ck * cl), Bk[bc + C::NBRA * (kc + C::NK * lc)], v);
+            }
+          }
+        }
+        T2[t] = v;
+      }
+      __syncwarp();
+      // bra transform and store (i fastest -> coalesced for canonical order)
+      for (int t = rho; t < NBO * NKO; t += C::LANES) {
         const int kap = t / NBO, b = t - kap * NBO;
         const int io = b % NIo, jo = b / NIo;
         const int ko = kap % NKo, lo = kap / NKo;
-        double v = 0.0;
-        for (int ic = 0; ic < NI; ++ic) {
-          const double ci = sph ? c2s(LI, io, ic) : (ic == io ? 1.0 : 0.0);
-          if (ci == 0.0) continue;
-          int ix, iy, iz;
-          cart_comp_rt(LI, ic, ix, iy, iz);
-          for (int jc = 0; jc < NJ; ++jc) {
-            const double cj = sph ? c2s(LJ, jo, jc) : (jc == jo ? 1.0 : 0.0);
-            if (cj == 0.0) continue;
-            int jx, jy, jz;
-            cart_comp_rt(LJ, jc, jx, jy, jz);
-            const double h = C::IB ? hrr_rt(E + kap, NKO, C::LA, ix, iy, iz, jx, jy, jz, abx, aby, abz)
-                                   : hrr_rt(E + kap, NKO, C::LA, jx, jy, jz, ix, iy, iz, abx, aby, abz);
-            v = fma(ci * cj, h, v);
+        R v = 0;
+        if (!sph) {
+          v = T2[io + C::NI * jo + C::NBRA * kap];
+        } else {
+          for (int ic = 0; ic < C::NI; ++ic) {
+            const double ci = LI < 2 ? (ic == io ? 1.0 : 0.0) : c2s_s[(LI * 5 + io) * 6 + ic];
+            if (ci == 0.0) continue;
+            for (int jc = 0; jc < C::NJ; ++jc) {
+              const double cj = LJ < 2 ? (jc == jo ? 1.0 : 0.0) : c2s_s[(LJ * 5 + jo) * 6 + jc];
+              if (cj == 0.0) continue;
+              v = fma((R)(ci * cj), T2[ic + C::NI * jc + C::NBRA * kap], v);
+            }
           }
         }
         prm.out[job.out_off + (long long)io * job.s_i + (long long)jo * job.s_j +
-                (long long)ko * job.s_k + (long long)lo * job.s_l] = v;
+                (long long)ko * job.s_k + (long long)lo * job.s_l] = (double)v;
       }
     }
+    if (MODE == 1 && have) fock_digest<C::NI, C::NJ, C::NK, C::NL, R>(Bk, job, wdeg, fk, rho, C::LANES);
     __syncwarp();
   }
 }

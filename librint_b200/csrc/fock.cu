@@ -1,0 +1,386 @@
+// Direct Fock build G(P) on the GPU: the reference's integral2e_fock
+// (src/scf.rs:316-410) without the dense tensor and with 8-fold symmetry.
+//
+//  * molecule context: device copies of atm/bas/env, AO offsets, and a pair
+//    table of all shell pairs I >= J (oriented l_first >= l_second) with their
+//    primitive pairs and Schwarz factors Q_IJ = sqrt(max |(ab|ab)|);
+//  * per build: shell-block density maxima, quartet screening
+//    Q_IJ Q_KL max(2D_IJ, 2D_KL, D_IK, D_IL, D_JK, D_JL) >= tau over canonical
+//    pair pairs, compaction into a job list sorted by class and primitive
+//    count, per-class digestion kernels (k_eri<..., 1>), symmetrisation.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#define RYS_OMIT_TAB
+#define RYS_CONST_QUAL __constant__
+#include "eri_classes.cuh"
+#include "fock.h"
+
+namespace lrb {
+
+const double *rys_table_device();
+
+#define FK_CK(x)                                  \
+  do {                                            \
+    cudaError_t e_ = (x);                         \
+    if (e_ != cudaSuccess) {                      \
+      set_error(cudaGetErrorString(e_));          \
+      return LRB_ERR_CUDA;                        \
+    }                                             \
+  } while (0)
+
+namespace {
+
+__device__ inline double fac_sp_d(int l) {
+  return l == 0 ? 0.28209479177387814 : (l == 1 ? 0.48860251190291992 : 1.0);
+}
+
+// Primitive pairs of every table pair (one thread per primitive pair).
+// sqrt(2 pi^2.5) is folded into every pair so bra.fac * ket.fac carries the
+// class prefactor 2 pi^3 / sqrt(pi) (reference src/g2e.rs:74-82).
+__global__ void k_mol_pairs(const PairInfo *__restrict__ pairs, int npairs,
+                            const int *__restrict__ atm, const int *__restrict__ bas,
+                            const double *__restrict__ env, PrimPair *pp, int npp_total) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npp_total) return;
+  int lo = 0, hi = npairs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pairs[mid].pp_off <= t) lo = mid; else hi = mid - 1;
+  }
+  const PairInfo pr = pairs[lo];
+  const int *bi = bas + 8 * pr.ish, *bj = bas + 8 * pr.jsh;
+  const int ki = bi[2], kj = bj[2];
+  const int e = t - pr.pp_off;
+  const int ip = e % ki, jp = e / ki;
+  const double *ri = env + atm[6 * bi[0] + 1], *rj = env + atm[6 * bj[0] + 1];
+  const double ai = env[bi[5] + ip], aj = env[bj[5] + jp];
+  const double ci = env[bi[6] + ip], cj = env[bj[6] + jp];
+  const double dx = ri[0] - rj[0], dy = ri[1] - rj[1], dz = ri[2] - rj[2];
+  const double rr = dx * dx + dy * dy + dz * dz;
+  const double aij = ai + aj, inv = 1.0 / aij;
+  const double eij = rr * ai * aj * inv;
+  const int lij = bi[1] + bj[1];
+  double log_rr = 1.7 - 1.5 * log(env[bi[5] + ki - 1] + env[bj[5] + kj - 1]);
+  if (lij > 0) log_rr += lij * log(sqrt(rr) + 1.0);
+  PrimPair o;
+  o.a = aij;
+  const double wj = aj * inv;
+  o.px = ri[0] + wj * (rj[0] - ri[0]);
+  o.py = ri[1] + wj * (rj[1] - ri[1]);
+  o.pz = ri[2] + wj * (rj[2] - ri[2]);
+  o.fac = ci * cj * exp(-eij) * fac_sp_d(bi[1]) * fac_sp_d(bj[1]) * 5.9149671727956129;
+  o.cce = eij - log_rr - log(fabs(ci)) - log(fabs(cj));
+  pp[t] = o;
+}
+
+// Q_IJ from the diagonal of the (IJ|IJ) cartesian blocks.
+__global__ void k_schwarz(const double *__restrict__ blocks, const long long *__restrict__ boff,
+                          const int *__restrict__ dims, int npairs, double *Q) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const int ni = dims[2 * p], nj = dims[2 * p + 1];
+  const double *b = blocks + boff[p];
+  double m = 0.0;
+  for (int a = 0; a < ni; ++a)
+    for (int c = 0; c < nj; ++c) {
+      const long long e = a + (long long)ni * (c + (long long)nj * (a + (long long)ni * c));
+      m = fmax(m, fabs(b[e]));
+    }
+  Q[p] = sqrt(m);
+}
+
+// Shell-block maxima of |P|.
+__global__ void k_dens_max(const double *__restrict__ P, int n, const int *__restrict__ aooff,
+                           int nbas, double *Dsh) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nbas * nbas) return;
+  const int I = t / nbas, J = t % nbas;
+  double m = 0.0;
+  for (int a = aooff[I]; a < aooff[I + 1]; ++a)
+    for (int b = aooff[J]; b < aooff[J + 1]; ++b) m = fmax(m, fabs(P[(long long)a * n + b]));
+  Dsh[t] = m;
+}
+
+__device__ inline int pair_cls_of(int li, int lj) { return li * (li + 1) / 2 + lj; }
+
+// Screen canonical pair pairs (b >= k) and append survivors.
+__global__ void k_screen(const PairInfo *__restrict__ pairs, const int *__restrict__ pcls,
+                         const double *__restrict__ Q, const double *__restrict__ Dsh, int nbas,
+                         long long ncand, int npairs, double tau, int2 *jobs, unsigned *keys,
+                         int *idx, unsigned long long *count, unsigned long long cap) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  bool keep = false;
+  int b = 0, k = 0;
+  unsigned key = 0;
+  if (t < ncand) {
+    b = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((long long)b * (b + 1) / 2 > t) --b;
+    while ((long long)(b + 1) * (b + 2) / 2 <= t) ++b;
+    k = (int)(t - (long long)b * (b + 1) / 2);
+    const PairInfo pb = pairs[b], pk = pairs[k];
+    const int I = pb.ish, J = pb.jsh, K = pk.ish, L = pk.jsh;
+    const double d = fmax(fmax(2.0 * Dsh[I * nbas + J], 2.0 * Dsh[K * nbas + L]),
+                          fmax(fmax(Dsh[I * nbas + K], Dsh[I * nbas + L]),
+                               fmax(Dsh[J * nbas + K], Dsh[J * nbas + L])));
+    keep = Q[b] * Q[k] * d >= tau;
+    if (keep) {
+      int cb = pcls[b], ck = pcls[k];
+      if (cb < ck) {   // bra class must not be below the ket class
+        const int tmp = b; b = k; k = tmp;
+        const int tc = cb; cb = ck; ck = tc;
+      }
+      const int cid = cb * (cb + 1) / 2 + ck;
+      const int kprod = pairs[b].npp * pairs[k].npp;
+      key = ((unsigned)cid << 20) | (unsigned)(0xfffff - kprod);
+    }
+  }
+  // warp-aggregated append
+  const unsigned mask = __ballot_sync(0xffffffffu, keep);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  unsigned long long base = 0;
+  if (lane == __ffs(mask) - 1) base = atomicAdd(count, (unsigned long long)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+  if (keep) {
+    const unsigned long long pos = base + __popc(mask & ((1u << lane) - 1));
+    if (pos < cap) {
+      jobs[pos] = make_int2(b, k);
+      keys[pos] = key;
+      idx[pos] = (int)pos;
+    }
+  }
+}
+
+__global__ void k_class_starts_f(const unsigned *__restrict__ keys, long long n, int ncls,
+                                 long long *starts) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ncls) return;
+  long long lo = 0, hi = n;
+  const unsigned key = (unsigned)c << 20;
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (keys[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  starts[c] = lo;
+}
+
+__global__ void k_symmetrize(const double *__restrict__ J, const double *__restrict__ K, int n,
+                             double *G) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int a = (int)(t / n), b = (int)(t % n);
+  const long long tt = (long long)b * n + a;
+  G[t] = J[t] + J[tt] - 0.5 * (K[t] + K[tt]);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ context
+int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, const double *env,
+               long long nenv, cudaStream_t st) {
+  m.natm = natm; m.nbas = nbas; m.nenv = nenv;
+  m.h_atm.assign(atm, atm + 6 * natm);
+  m.h_bas.assign(bas, bas + 8 * nbas);
+  m.h_env.assign(env, env + nenv);
+  for (int s = 0; s < nbas; ++s) {
+    const int *b = bas + 8 * s;
+    if (b[1] < 0 || b[1] > ERI_LMAX || b[3] != 1 || b[2] < 1 || b[2] > ERI_KMAX)
+      return set_error("molecule: shells must have l <= 2, 1..31 primitives, nctr == 1"),
+             LRB_ERR_UNSUPPORTED;
+    if (b[0] < 0 || b[0] >= natm || b[5] < 0 || b[6] < 0 || (long long)b[5] + b[2] > nenv ||
+        (long long)b[6] + b[2] > nenv)
+      return set_error("molecule: bas index out of range"), LRB_ERR_INPUT;
+  }
+  for (int a = 0; a < natm; ++a)
+    if (atm[6 * a + 1] < 0 || (long long)atm[6 * a + 1] + 3 > nenv)
+      return set_error("molecule: atm coordinate pointer out of range"), LRB_ERR_INPUT;
+  if (nenv > 8 && env[8] != 0.0)
+    return set_error("range-separated integrals (env[8] != 0) are not supported"),
+           LRB_ERR_UNSUPPORTED;
+  m.h_aooff.assign(nbas + 1, 0);
+  for (int s = 0; s < nbas; ++s) m.h_aooff[s + 1] = m.h_aooff[s] + ncart(bas[8 * s + 1]);
+  m.nao = m.h_aooff[nbas];
+  // pair table
+  std::vector<PairInfo> pr;
+  std::vector<int> pc;
+  int npp = 0;
+  for (int I = 0; I < nbas; ++I)
+    for (int J = 0; J <= I; ++J) {
+      int a = I, b = J;
+      if (bas[8 * a + 1] < bas[8 * b + 1]) std::swap(a, b);
+      PairInfo p;
+      p.ish = a; p.jsh = b; p.pp_off = npp; p.npp = bas[8 * a + 2] * bas[8 * b + 2];
+      npp += p.npp;
+      pr.push_back(p);
+      const int la = bas[8 * a + 1], lb = bas[8 * b + 1];
+      pc.push_back(la * (la + 1) / 2 + lb);
+    }
+  m.npairs = (int)pr.size();
+  m.npp = npp;
+  m.h_pairs = pr;
+  auto al = [&](void **p, size_t n) {
+    return cudaMallocAsync(p, std::max(n, (size_t)16), st) == cudaSuccess;
+  };
+  if (!al((void **)&m.atm, sizeof(int) * 6 * natm) || !al((void **)&m.bas, sizeof(int) * 8 * nbas) ||
+      !al((void **)&m.env, sizeof(double) * nenv) || !al((void **)&m.aooff, sizeof(int) * (nbas + 1)) ||
+      !al((void **)&m.pairs, sizeof(PairInfo) * m.npairs) || !al((void **)&m.pcls, sizeof(int) * m.npairs) ||
+      !al((void **)&m.pp, sizeof(PrimPair) * npp) || !al((void **)&m.Q, sizeof(double) * m.npairs) ||
+      !al((void **)&m.Dsh, sizeof(double) * nbas * nbas))
+    return set_error("molecule: device allocation failed"), LRB_ERR_ALLOC;
+  FK_CK(cudaMemcpyAsync(m.atm, atm, sizeof(int) * 6 * natm, cudaMemcpyHostToDevice, st));
+  FK_CK(cudaMemcpyAsync(m.bas, bas, sizeof(int) * 8 * nbas, cudaMemcpyHostToDevice, st));
+  FK_CK(cudaMemcpyAsync(m.env, env, sizeof(double) * nenv, cudaMemcpyHostToDevice, st));
+  FK_CK(cudaMemcpyAsync(m.aooff, m.h_aooff.data(), sizeof(int) * (nbas + 1), cudaMemcpyHostToDevice, st));
+  FK_CK(cudaMemcpyAsync(m.pairs, pr.data(), sizeof(PairInfo) * m.npairs, cudaMemcpyHostToDevice, st));
+  FK_CK(cudaMemcpyAsync(m.pcls, pc.data(), sizeof(int) * m.npairs, cudaMemcpyHostToDevice, st));
+  k_mol_pairs<<<(npp + 255) / 256, 256, 0, st>>>(m.pairs, m.npairs, m.atm, m.bas, m.env, m.pp, npp);
+  engine().launches++;
+  FK_CK(cudaGetLastError());
+  // Schwarz factors from (IJ|IJ) cartesian blocks
+  std::vector<int> quart(4 * (size_t)m.npairs), dims(2 * (size_t)m.npairs);
+  std::vector<long long> boff(m.npairs + 1, 0);
+  for (int p = 0; p < m.npairs; ++p) {
+    const int I = pr[p].ish, J = pr[p].jsh;
+    quart[4 * p] = I; quart[4 * p + 1] = J; quart[4 * p + 2] = I; quart[4 * p + 3] = J;
+    const int ni = ncart(bas[8 * I + 1]), nj = ncart(bas[8 * J + 1]);
+    dims[2 * p] = ni; dims[2 * p + 1] = nj;
+    boff[p + 1] = boff[p] + (long long)ni * nj * ni * nj;
+  }
+  int *d_q = nullptr, *d_dims = nullptr;
+  long long *d_boff = nullptr;
+  double *d_blk = nullptr;
+  if (!al((void **)&d_q, sizeof(int) * quart.size()) || !al((void **)&d_dims, sizeof(int) * dims.size()) ||
+      !al((void **)&d_boff, sizeof(long long) * boff.size()) ||
+      !al((void **)&d_blk, sizeof(double) * (size_t)boff[m.npairs]))
+    return set_error("molecule: device allocation failed"), LRB_ERR_ALLOC;
+  FK_CK(cudaMemcpyAsync(d_q, quart.data(), sizeof(int) * quart.size(), cudaMemcpyHostToDevice, st));
+  FK_CK(cudaMemcpyAsync(d_dims, dims.data(), sizeof(int) * dims.size(), cudaMemcpyHostToDevice, st));
+  FK_CK(cudaMemcpyAsync(d_boff, boff.data(), sizeof(long long) * boff.size(), cudaMemcpyHostToDevice, st));
+  int rc = eri_batch_device(engine(), d_blk, 0, d_q, m.npairs, m.atm, natm, m.bas, nbas, m.env,
+                            nenv, st, nullptr);
+  if (rc) return rc;
+  k_schwarz<<<(m.npairs + 255) / 256, 256, 0, st>>>(d_blk, d_boff, d_dims, m.npairs, m.Q);
+  engine().launches++;
+  FK_CK(cudaGetLastError());
+  cudaFreeAsync(d_q, st);
+  cudaFreeAsync(d_dims, st);
+  cudaFreeAsync(d_boff, st);
+  cudaFreeAsync(d_blk, st);
+  FK_CK(cudaStreamSynchronize(st));
+  return LRB_OK;
+}
+
+void mol_destroy(MolCtx &m, cudaStream_t st) {
+  for (void *p : {(void *)m.atm, (void *)m.bas, (void *)m.env, (void *)m.aooff, (void *)m.pairs,
+                  (void *)m.pcls, (void *)m.pp, (void *)m.Q, (void *)m.Dsh})
+    if (p) cudaFreeAsync(p, st);
+  cudaStreamSynchronize(st);
+}
+
+// ------------------------------------------------------------ build
+int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t st,
+               FockStats *stats) {
+  Engine &eng = engine();
+  const ClassEntry *tab = class_table();
+  const int n = m.nao, nbas = m.nbas;
+  const long long ncand = (long long)m.npairs * (m.npairs + 1) / 2;
+  // job capacity: all candidates (worst case, no screening)
+  const size_t cap = (size_t)ncand;
+  const size_t need = carve_size(sizeof(int2) * cap) + 2 * carve_size(sizeof(unsigned) * cap) +
+                      2 * carve_size(sizeof(int) * cap) + 2 * carve_size(sizeof(double) * (size_t)n * n) +
+                      carve_size(sizeof(long long) * 64) + carve_size(sizeof(unsigned long long)) +
+                      carve_size(sizeof(int) * 64);
+  char *base = eng.ws.reserve_extra(st, need) ? (char *)eng.ws.extra.ptr : nullptr;
+  if (!base) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
+  Carver cv(base);
+  int2 *jobs = cv.take<int2>(cap);
+  unsigned *keys = cv.take<unsigned>(cap), *keys2 = cv.take<unsigned>(cap);
+  int *idx = cv.take<int>(cap), *idx2 = cv.take<int>(cap);
+  double *J = cv.take<double>((size_t)n * n), *K = cv.take<double>((size_t)n * n);
+  long long *starts = cv.take<long long>(64);
+  unsigned long long *count = cv.take<unsigned long long>(1);
+  int *counters = cv.take<int>(64);
+  FK_CK(cudaMemsetAsync(J, 0, sizeof(double) * (size_t)n * n, st));
+  FK_CK(cudaMemsetAsync(K, 0, sizeof(double) * (size_t)n * n, st));
+  FK_CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
+  FK_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 64, st));
+  k_dens_max<<<(nbas * nbas + 255) / 256, 256, 0, st>>>(dP, n, m.aooff, nbas, m.Dsh);
+  k_screen<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(m.pairs, m.pcls, m.Q, m.Dsh, nbas, ncand,
+                                                            m.npairs, tau, jobs, keys, idx, count, cap);
+  eng.launches += 2;
+  FK_CK(cudaGetLastError());
+  unsigned long long nj = 0;
+  FK_CK(cudaMemcpyAsync(&nj, count, sizeof(nj), cudaMemcpyDeviceToHost, st));
+  FK_CK(cudaStreamSynchronize(st));
+  if (nj > cap) nj = cap;
+  if (nj > 0) {
+    size_t tmpb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st);
+    void *tmp = eng.ws.reserve_aux(st, tmpb + 64);
+    if (!tmp) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
+    FK_CK(cub::DeviceRadixSort::SortPairs(tmp, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st));
+    k_class_starts_f<<<1, 64, 0, st>>>(keys2, (long long)nj, NCLASS, starts);
+    eng.launches++;
+    long long cls_begin[NCLASS + 1];
+    FK_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * (NCLASS + 1), cudaMemcpyDeviceToHost, st));
+    FK_CK(cudaStreamSynchronize(st));
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const double *rys = rys_table_device();
+    EriParams prm{};
+    prm.pp = m.pp;
+    prm.expcutoff = eng.expcutoff;
+    prm.sph = 0;
+    FockParams fk;
+    fk.jobs = jobs;
+    fk.pairs = m.pairs;
+    fk.aooff = m.aooff;
+    fk.P = dP;
+    fk.J = J;
+    fk.K = K;
+    fk.n = n;
+    for (int c = 0; c < NCLASS; ++c) {
+      const long long b0 = cls_begin[c], b1 = cls_begin[c + 1];
+      if (b1 <= b0) continue;
+      const ClassEntry &ce = tab[c];
+      prm.order = idx2 + b0;
+      prm.njobs = (int)(b1 - b0);
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[1], ERI_THREADS, ce.smem[1]);
+      if (per_sm < 1) per_sm = 1;
+      const long long tasks = (prm.njobs + ce.slots - 1) / ce.slots;
+      long long grid = (long long)nsm * per_sm;
+      const long long needg = (tasks + ERI_WARPS - 1) / ERI_WARPS;
+      if (grid > needg) grid = needg;
+      ProfRecord rec{c, nullptr, nullptr};
+      if (eng.profile) {
+        cudaEventCreate(&rec.start);
+        cudaEventCreate(&rec.stop);
+        cudaEventRecord(rec.start, st);
+      }
+      ce.fn[1]<<<(unsigned)grid, ERI_THREADS, ce.smem[1], st>>>(prm, fk, rys + RYS_TAB_OFFSET[ce.nr],
+                                                                counters + c);
+      FK_CK(cudaGetLastError());
+      eng.launches++;
+      if (eng.profile) {
+        cudaEventRecord(rec.stop, st);
+        eng.prof.push_back(rec);
+      }
+    }
+  }
+  k_symmetrize<<<(unsigned)(((long long)n * n + 255) / 256), 256, 0, st>>>(J, K, n, dG);
+  eng.launches++;
+  FK_CK(cudaGetLastError());
+  if (stats) {
+    stats->candidates = ncand;
+    stats->quartets = (long long)nj;
+  }
+  return LRB_OK;
+}
+
+}  // namespace lrb

@@ -1,0 +1,123 @@
+"""RHF on the GPU: the reference's python/librint/scf.py functions (int1e,
+int2e, density, energy, scf) over this library's C ABI, plus a molecule
+context for repeated Fock builds."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _bindings as B
+from .basis import Molecule
+from .eri import int2e  # noqa: F401  (reference scf.int2e)
+
+
+def _arr(m: Molecule):
+    return (np.ascontiguousarray(m.atm, dtype=np.int32), np.ascontiguousarray(m.bas, dtype=np.int32),
+            np.ascontiguousarray(m.env, dtype=np.float64))
+
+
+class MolContext:
+    """Device-resident molecule: pair table, Schwarz factors, Fock builds."""
+
+    def __init__(self, m: Molecule):
+        self.m = m
+        atm, bas, env = _arr(m)
+        self._keep = (atm, bas, env)
+        h = ctypes.c_void_p()
+        rc = B.lib().lrb_mol_create(ctypes.byref(h), atm.ctypes.data_as(B.P_i), atm.size // 6,
+                                    bas.ctypes.data_as(B.P_i), bas.size // 8,
+                                    env.ctypes.data_as(B.P_d), env.size)
+        B.check(rc, "lrb_mol_create")
+        self.h = h
+        self.nao = B.lib().lrb_mol_nao(h)
+
+    def close(self):
+        if self.h:
+            B.lib().lrb_mol_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def fock_G(self, P, tau: float = 0.0):
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        G = np.empty_like(P)
+        nq = ctypes.c_longlong(0)
+        rc = B.lib().lrb_fock_G(self.h, P.ctypes.data_as(B.P_d), G.ctypes.data_as(B.P_d), tau,
+                                ctypes.byref(nq))
+        B.check(rc, "lrb_fock_G")
+        return G
+
+    def int1e(self, typec: int, coord: int = 0):
+        n = self.m.nao(coord)
+        out = np.empty((n, n))
+        B.check(B.lib().lrb_int1e(self.h, typec, coord, out.ctypes.data_as(B.P_d)), "lrb_int1e")
+        return out
+
+    def scf(self, nelec=None, max_iter=100, conv=1e-10, guess=0, diis=0, tau=0.0, P0=None,
+            return_density=False):
+        nelec = self.m.nelec if nelec is None else nelec
+        o = B.ScfOptions(max_iter, conv, guess, diis, tau)
+        r = B.ScfResult()
+        P = np.empty((self.nao, self.nao))
+        p0 = None if P0 is None else np.ascontiguousarray(P0, dtype=np.float64).ctypes.data_as(B.P_d)
+        rc = B.lib().lrb_scf(self.h, nelec, ctypes.byref(o), ctypes.byref(r),
+                             P.ctypes.data_as(B.P_d), p0)
+        B.check(rc, "lrb_scf")
+        return (r, P) if return_density else r
+
+    def energy(self, P, tau: float = 0.0):
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        E = ctypes.c_double()
+        B.check(B.lib().lrb_energy(self.h, P.ctypes.data_as(B.P_d), tau, ctypes.byref(E)), "lrb_energy")
+        return E.value
+
+
+# --- reference python/librint/scf.py shapes (arrays in, arrays out) -------
+def _p2c(m: Molecule):
+    atm, bas, env = _arr(m)
+    return (atm.ctypes.data_as(B.P_i), atm.size, bas.ctypes.data_as(B.P_i), bas.size,
+            env.ctypes.data_as(B.P_d), env.size), (atm, bas, env)
+
+
+def _take(ptr, n):
+    if not ptr:
+        raise B.LibrintError(B.lib().lrb_last_error().decode() or "NULL result")
+    a = np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+    B.lib().free_c(ptr, n)
+    return a
+
+
+def int1e(m: Molecule, typec: int, coord: int = 0):
+    args, _keep = _p2c(m)
+    n = m.nao(coord)
+    return _take(B.lib().int1e_c(*args, coord, typec), n * n).reshape(n, n)
+
+
+def density(m: Molecule, nelec=None, imax: int = 100, conv: float = 1e-6):
+    args, _keep = _p2c(m)
+    n = m.nao(0)
+    nelec = m.nelec if nelec is None else nelec
+    return _take(B.lib().density_c(*args, nelec, imax, conv), n * n).reshape(n, n)
+
+
+def energy(m: Molecule, P):
+    args, _keep = _p2c(m)
+    P = np.ascontiguousarray(P, dtype=np.float64)
+    e = B.lib().energy_c(*args, P.ctypes.data_as(B.P_d), P.size)
+    if np.isnan(e):
+        raise B.LibrintError(B.lib().lrb_last_error().decode())
+    return e
+
+
+def scf(m: Molecule, nelec=None, imax: int = 100, conv: float = 1e-6):
+    args, _keep = _p2c(m)
+    nelec = m.nelec if nelec is None else nelec
+    e = B.lib().scf_c(*args, nelec, imax, conv)
+    if np.isnan(e):
+        raise B.LibrintError(B.lib().lrb_last_error().decode())
+    return e

@@ -1,0 +1,106 @@
+"""GPU Fock builds, one-electron integrals and SCF against the oracle and the
+reference goldens, through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle
+from librint_b200 import scf, synthetic
+from librint_b200.basis import Molecule
+
+pytestmark = pytest.mark.gpu
+
+MOLS = ["h2/sto3g", "lih/sto3g", "hf/sto3g", "h2o/sto3g", "h2o/def2svp", "nh3/sto3g",
+        "ch4/sto3g", "c/sto3g", "O/sto3g", "c6h6/sto3g"]
+
+
+def mol(golden, key):
+    return Molecule(golden[key + "/atm"], golden[key + "/bas"], golden[key + "/env"],
+                    int(golden[key + "/atm"].reshape(-1, 6)[:, 0].sum()))
+
+
+@pytest.mark.parametrize("name", MOLS)
+def test_int1e_vs_reference(golden, name):
+    m = mol(golden, "mol/" + name)
+    ctx = scf.MolContext(m)
+    for coord in (0, 1):
+        for typec in (0, 1, 2):
+            np.testing.assert_allclose(ctx.int1e(typec, coord), golden[f"mol/{name}/int1e_{coord}{typec}"],
+                                       rtol=1e-12, atol=1e-12)
+    # the p2c-shaped entry point too
+    np.testing.assert_allclose(scf.int1e(m, 2, 1), golden[f"mol/{name}/int1e_12"], rtol=1e-12,
+                               atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["h2o/sto3g", "h2o/def2svp", "ch4/sto3g", "c6h6/sto3g"])
+def test_fock_G_vs_oracle(golden, name):
+    """Direct J/K digestion vs the oracle's integral2e_fock restatement, at a
+    random symmetric density and with no screening (tau = 0)."""
+    m = mol(golden, "mol/" + name)
+    n = m.nao(0)
+    rng = np.random.default_rng(1)
+    A = rng.standard_normal((n, n))
+    P = (A + A.T) / np.sqrt(n)
+    G = scf.MolContext(m).fock_G(P, tau=0.0)
+    Gr = oracle.fock_G(m, P)
+    np.testing.assert_allclose(G, Gr, rtol=1e-11, atol=1e-12 * np.abs(Gr).max())
+
+
+def test_fock_G_water_like_and_screening(golden):
+    m = synthetic.water_like()
+    P, _ = oracle.density(m, conv=1e-8)
+    ctx = scf.MolContext(m)
+    Gr = oracle.fock_G(m, P)
+    np.testing.assert_allclose(ctx.fock_G(P, 0.0), Gr, rtol=1e-11, atol=1e-13)
+    # screening at 1e-14 changes G by far less than the screening bound
+    np.testing.assert_allclose(ctx.fock_G(P, 1e-14), Gr, rtol=0, atol=1e-11)
+
+
+@pytest.mark.parametrize("name", [n for n in MOLS if n not in ("c6h6/sto3g",)])
+def test_scf_reference_algorithm_vs_golden(golden, name):
+    """P0 = I, plain Roothaan (the reference's algorithm) -> same fixed point."""
+    m = mol(golden, "mol/" + name)
+    e = scf.scf(m, imax=1000, conv=1e-10)
+    if f"mol/{name}/scf" in golden:
+        assert abs(e - golden[f"mol/{name}/scf"]) < 1e-10
+    e_orc = oracle.scf(m, conv=1e-10, imax=1000)
+    assert abs(e - e_orc) < 1e-10
+
+
+def test_energy_truths(golden):
+    for name, truth in (("h2/sto3g", -0.8817324499460562), ("h2o/sto3g", -74.96102664501196)):
+        m = mol(golden, "mol/" + name)
+        P = scf.density(m, conv=1e-6, imax=1000)
+        assert abs(scf.energy(m, P) - truth) < 1e-10
+
+
+@pytest.mark.parametrize("name", MOLS)
+def test_energy_functional_at_reference_density(golden, name):
+    m = mol(golden, "mol/" + name)
+    for tag in ("scf", "scf6"):
+        if f"mol/{name}/{tag}_P" in golden:
+            assert abs(scf.energy(m, golden[f"mol/{name}/{tag}_P"]) - golden[f"mol/{name}/{tag}"]) < 1e-10
+
+
+def test_diis_core_guess_same_energy(golden):
+    """The B200 defaults (core-H guess + DIIS) change iterations, not the energy."""
+    for name in ("h2o/def2svp", "c6h6/sto3g", "nh3/sto3g"):
+        m = mol(golden, "mol/" + name)
+        ctx = scf.MolContext(m)
+        r0 = ctx.scf(conv=1e-10, max_iter=1000)
+        r1 = ctx.scf(conv=1e-10, guess=1, diis=8)
+        assert abs(r0.energy - r1.energy) < 1e-9
+        assert r1.iterations <= r0.iterations
+
+
+def test_water_like_scf(golden):
+    m = synthetic.water_like()
+    assert abs(scf.scf(m, imax=1000, conv=1e-10) - golden["water_like/scf"]) < 1e-10
+
+
+def test_scf_failures_in_band(golden):
+    """Non-convergence and bad input come back as NaN / exceptions, never a crash."""
+    m = mol(golden, "mol/h2o/sto3g")
+    assert np.isnan(__import__("librint_b200._bindings", fromlist=["x"]).lib().scf_c(
+        *scf._p2c(m)[0], m.nelec, 2, 1e-14))
+    with pytest.raises(Exception):
+        scf.scf(m, nelec=11)
