@@ -119,17 +119,21 @@ LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long l
 LRB_API int lrb_fock_G_device(LrbMol *m, const double *P, double *G, double tau, void *stream);
 
 typedef struct {
-  int max_iter;     /* reference imax */
-  double conv;      /* reference conv: ||P - P_old||_F / 2 */
-  int guess;        /* 0: P0 = I (reference), 1: core Hamiltonian */
-  int diis;         /* DIIS subspace (0 = plain Roothaan, as the reference) */
-  double tau;       /* quartet screening threshold */
+  int max_iter;       /* reference imax */
+  double conv;        /* reference conv: ||P - P_old||_F / 2 */
+  int guess;          /* 0: P0 = I (reference), 1: core Hamiltonian */
+  int diis;           /* DIIS subspace (0 = plain Roothaan, as the reference) */
+  double tau;         /* quartet screening threshold */
+  int mixed;          /* 1: incremental Fock builds, FP32 for small quartets */
+  double fp32_until;  /* all-FP32 builds while ||dP|| is above this */
+  double tau32;       /* then FP32 only for Schwarz x |dD| bounds below this */
+  int rebuild_every;  /* full (non-incremental) Fock build period */
 } LrbScfOptions;
 
 typedef struct {
   double energy, e_nuc, delta, fock_ms, wall_ms;
   int iterations, converged;
-  long long quartets;
+  long long quartets, fp32_quartets;
 } LrbScfResult;
 
 /* RHF (src/scf.rs:743-969).  P_out (n*n host) and P0 (initial density,
@@ -150,6 +154,33 @@ LRB_API double energy_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, doub
                         size_t env_l, double *P_p, size_t P_l);
 LRB_API double scf_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
                      size_t env_l, size_t nelec, int imax, double conv);
+
+/* ---------------------------------------------------------------------
+ * Frozen-density gradient with respect to env[s1:s2] -- the exponents and
+ * contraction coefficients (src/utils.rs:152-175 split, src/dscf.rs:320-565):
+ *   out = cH dH + cR dR + cS dS,  dH = sum P (dT + dV),
+ *   dR = d/dtheta 1/2 sum (P P - P P / 2)(ij|kl),  dS = sum (P F P) dS.
+ * dR comes from an adjoint ERI kernel contracted with the density in-kernel
+ * (replacing the Enzyme reverse passes of src/dscf.rs:370-515).
+ * -------------------------------------------------------------------*/
+LRB_API int lrb_grad_len(const LrbMol *m);
+LRB_API int lrb_grad(LrbMol *m, const double *P, double cH, double cR, double cS, double tau,
+                     double *out);
+
+/* src/p2c.rs:240, 267, 294, 321, 348, 376: buffers of lrb_grad_len doubles,
+ * release with free_c; NULL on failure. */
+LRB_API double *grad_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                       size_t env_l, double *P_p, size_t P_l);
+LRB_API double *dS_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                     size_t env_l, double *P_p, size_t P_l);
+LRB_API double *dHcore_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                         size_t env_l, double *P_p, size_t P_l);
+LRB_API double *dR_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                     size_t env_l, double *P_p, size_t P_l);
+LRB_API double *danalytical_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l,
+                              double *env_p, size_t env_l, double *P_p, size_t P_l);
+LRB_API double *denergy_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                          size_t env_l, double *P_p, size_t P_l);
 
 #ifdef __cplusplus
 }

@@ -60,14 +60,16 @@ def lib():
 
 class ScfOptions(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv", ctypes.c_double), ("guess", ctypes.c_int),
-                ("diis", ctypes.c_int), ("tau", ctypes.c_double)]
+                ("diis", ctypes.c_int), ("tau", ctypes.c_double), ("mixed", ctypes.c_int),
+                ("fp32_until", ctypes.c_double), ("tau32", ctypes.c_double),
+                ("rebuild_every", ctypes.c_int)]
 
 
 class ScfResult(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("e_nuc", ctypes.c_double), ("delta", ctypes.c_double),
                 ("fock_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
                 ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
-                ("quartets", ctypes.c_longlong)]
+                ("quartets", ctypes.c_longlong), ("fp32_quartets", ctypes.c_longlong)]
 
 
 def _optional(L):
@@ -90,8 +92,12 @@ def _optional(L):
         "density_c": (P_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_sz, c_int, c_d)),
         "energy_c": (c_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, P_d, c_sz)),
         "scf_c": (c_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_sz, c_int, c_d)),
+        "lrb_grad_len": (c_int, (c_vp,)),
+        "lrb_grad": (c_int, (c_vp, P_d, c_d, c_d, c_d, c_d, P_d)),
     }
-    for name, (res, args) in sigs.items():
+    for name in ("grad_c", "dS_c", "dHcore_c", "dR_c", "danalytical_c", "denergy_c"):
+        sigs[name] = (P_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, P_d, c_sz))
+    for name, (res, args) in list(sigs.items()):
         if hasattr(L, name):
             f = getattr(L, name)
             f.restype = res

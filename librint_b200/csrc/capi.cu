@@ -12,6 +12,7 @@
 #include "engine.h"
 #include "eri_device.cuh"
 #include "fock.h"
+#include "grad.h"
 
 using namespace lrb;
 
@@ -404,14 +405,15 @@ LRB_API int lrb_scf(LrbMol *m, long long nelec, const LrbScfOptions *opt, LrbScf
   ScfOptions o;
   if (opt) {
     o.max_iter = opt->max_iter; o.conv = opt->conv; o.guess = opt->guess; o.diis = opt->diis;
-    o.tau = opt->tau;
+    o.tau = opt->tau; o.mixed = opt->mixed; o.fp32_until = opt->fp32_until;
+    o.tau32 = opt->tau32; o.rebuild_every = opt->rebuild_every > 0 ? opt->rebuild_every : 6;
   }
   ScfResult r;
   const int rc = scf_run(m->ctx, (size_t)nelec, o, &r, P_out, P0, nullptr);
   if (res) {
     res->energy = r.energy; res->e_nuc = r.e_nuc; res->delta = r.delta; res->fock_ms = r.fock_ms;
     res->wall_ms = r.wall_ms; res->iterations = r.iterations; res->converged = r.converged;
-    res->quartets = r.quartets;
+    res->quartets = r.quartets; res->fp32_quartets = r.fp32_quartets;
   }
   return rc;
 }
@@ -470,7 +472,7 @@ double *density_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *en
   if (!m) return nullptr;
   const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
   double *P = (double *)std::malloc(sizeof(double) * nn);
-  LrbScfOptions o{imax, conv, 0, 0, 0.0};
+  LrbScfOptions o{imax, conv, 0, 0, 0.0, 0, 0.0, 0.0, 6};
   if (!P || lrb_scf(m, (long long)nelec, &o, nullptr, P, nullptr)) {
     std::free(P);
     P = nullptr;
@@ -493,11 +495,100 @@ double scf_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, 
              size_t nelec, int imax, double conv) {
   LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
   if (!m) return NAN;
-  LrbScfOptions o{imax, conv, 0, 0, 0.0};
+  LrbScfOptions o{imax, conv, 0, 0, 0.0, 0, 0.0, 0.0, 6};
   LrbScfResult r;
   const int rc = lrb_scf(m, (long long)nelec, &o, &r, nullptr, nullptr);
   lrb_mol_destroy(m);
   return rc ? NAN : r.energy;
+}
+
+// ---- gradients with respect to env[s1:s2] (src/utils.rs:152-175 split)
+// The reference's split: s1 = min PTR_EXP; s2 updated to PTR_COEFF + NPRIM
+// whenever a shell's PTR_COEFF exceeds the current s2 (kept as written).
+static void env_split(const int *bas, int nbas, int &s1, int &s2) {
+  s1 = -1;
+  s2 = -1;
+  for (int s = 0; s < nbas; ++s) {
+    const int ngto = bas[8 * s + 2], ex = bas[8 * s + 5], co = bas[8 * s + 6];
+    if (s1 == -1 || s1 > ex) s1 = ex;
+    if (s2 == -1) s2 = co + ngto;
+    else if (s2 < co) s2 = co + ngto;
+  }
+}
+
+LRB_API int lrb_grad_len(const LrbMol *m) {
+  if (!m) return -1;
+  int s1, s2;
+  env_split(m->ctx.h_bas.data(), m->ctx.nbas, s1, s2);
+  return s2 - s1;
+}
+
+LRB_API int lrb_grad(LrbMol *m, const double *P, double cH, double cR, double cS, double tau,
+                     double *out) {
+  if (!m || !P || !out) return set_error("NULL argument"), LRB_ERR_INPUT;
+  MolCtx &c = m->ctx;
+  int s1, s2;
+  env_split(c.h_bas.data(), c.nbas, s1, s2);
+  const size_t glen = (size_t)(c.nenv - s1), nn = (size_t)c.nao * c.nao;
+  cudaStream_t st = nullptr;
+  double *dP = nullptr, *dg = nullptr;
+  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
+      cudaMallocAsync((void **)&dg, glen * 8, st) != cudaSuccess)
+    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(dg, 0, glen * 8, st);
+  int rc = grad_run(c, dP, cH, cR, cS, tau, dg, s1, st);
+  if (!rc) cudaMemcpyAsync(out, dg, sizeof(double) * (size_t)(s2 - s1), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dP, st);
+  cudaFreeAsync(dg, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
+  return rc;
+}
+
+static double *grad_p2c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                        size_t env_l, double *P_p, size_t P_l, double cH, double cR, double cS) {
+  LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
+  if (!m) return nullptr;
+  double *out = nullptr;
+  const int len = lrb_grad_len(m);
+  if ((size_t)m->ctx.nao * m->ctx.nao == P_l && len > 0) {
+    out = (double *)std::malloc(sizeof(double) * len);
+    if (out && lrb_grad(m, P_p, cH, cR, cS, 0.0, out)) {
+      std::free(out);
+      out = nullptr;
+    }
+  } else {
+    set_error("density size does not match the basis");
+  }
+  lrb_mol_destroy(m);
+  return out;
+}
+
+// src/p2c.rs:240 grad_c = dHcore + dR (src/dscf.rs:547-557)
+double *grad_c(int *a, size_t al, int *b, size_t bl, double *e, size_t el, double *P, size_t Pl) {
+  return grad_p2c(a, al, b, bl, e, el, P, Pl, 1.0, 1.0, 0.0);
+}
+// src/p2c.rs:267 dS_c = sum (PFP) dS (src/dscf.rs:354-368)
+double *dS_c(int *a, size_t al, int *b, size_t bl, double *e, size_t el, double *P, size_t Pl) {
+  return grad_p2c(a, al, b, bl, e, el, P, Pl, 0.0, 0.0, 1.0);
+}
+// src/p2c.rs:294 dHcore_c (src/dscf.rs:320-336)
+double *dHcore_c(int *a, size_t al, int *b, size_t bl, double *e, size_t el, double *P, size_t Pl) {
+  return grad_p2c(a, al, b, bl, e, el, P, Pl, 1.0, 0.0, 0.0);
+}
+// src/p2c.rs:321 dR_c (src/dscf.rs:370-524)
+double *dR_c(int *a, size_t al, int *b, size_t bl, double *e, size_t el, double *P, size_t Pl) {
+  return grad_p2c(a, al, b, bl, e, el, P, Pl, 0.0, 1.0, 0.0);
+}
+// src/p2c.rs:348 danalytical_c = dH + dR - dS/2 (src/dscf.rs:526-537)
+double *danalytical_c(int *a, size_t al, int *b, size_t bl, double *e, size_t el, double *P,
+                      size_t Pl) {
+  return grad_p2c(a, al, b, bl, e, el, P, Pl, 1.0, 1.0, -0.5);
+}
+// src/p2c.rs:376 denergy_c delegates to the same assembly (src/dscf.rs:559-565)
+double *denergy_c(int *a, size_t al, int *b, size_t bl, double *e, size_t el, double *P,
+                  size_t Pl) {
+  return grad_p2c(a, al, b, bl, e, el, P, Pl, 1.0, 1.0, -0.5);
 }
 
 }  // extern "C"

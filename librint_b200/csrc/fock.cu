@@ -108,10 +108,13 @@ __global__ void k_dens_max(const double *__restrict__ P, int n, const int *__res
 __device__ inline int pair_cls_of(int li, int lj) { return li * (li + 1) / 2 + lj; }
 
 // Screen canonical pair pairs (b >= k) and append survivors.
+// prec: 0 all FP64, 1 all FP32, 2 FP32 when the bound is below tau32.
+// FP32 quartets get class ids offset by NCLASS.
 __global__ void k_screen(const PairInfo *__restrict__ pairs, const int *__restrict__ pcls,
                          const double *__restrict__ Q, const double *__restrict__ Dsh, int nbas,
-                         long long ncand, int npairs, double tau, int2 *jobs, unsigned *keys,
-                         int *idx, unsigned long long *count, unsigned long long cap) {
+                         long long ncand, int npairs, double tau, int prec, double tau32,
+                         int2 *jobs, unsigned *keys, int *idx, unsigned long long *count,
+                         unsigned long long cap) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   bool keep = false;
   int b = 0, k = 0;
@@ -126,14 +129,16 @@ __global__ void k_screen(const PairInfo *__restrict__ pairs, const int *__restri
     const double d = fmax(fmax(2.0 * Dsh[I * nbas + J], 2.0 * Dsh[K * nbas + L]),
                           fmax(fmax(Dsh[I * nbas + K], Dsh[I * nbas + L]),
                                fmax(Dsh[J * nbas + K], Dsh[J * nbas + L])));
-    keep = Q[b] * Q[k] * d >= tau;
+    const double bound = Q[b] * Q[k] * d;
+    keep = bound >= tau;
     if (keep) {
+      const bool f32 = prec == 1 || (prec == 2 && bound < tau32);
       int cb = pcls[b], ck = pcls[k];
       if (cb < ck) {   // bra class must not be below the ket class
         const int tmp = b; b = k; k = tmp;
         const int tc = cb; cb = ck; ck = tc;
       }
-      const int cid = cb * (cb + 1) / 2 + ck;
+      const int cid = cb * (cb + 1) / 2 + ck + (f32 ? NCLASS : 0);
       const int kprod = pairs[b].npp * pairs[k].npp;
       key = ((unsigned)cid << 20) | (unsigned)(0xfffff - kprod);
     }
@@ -169,15 +174,21 @@ __global__ void k_class_starts_f(const unsigned *__restrict__ keys, long long n,
 }
 
 __global__ void k_symmetrize(const double *__restrict__ J, const double *__restrict__ K, int n,
-                             double *G) {
+                             double *G, bool accumulate) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)n * n) return;
   const int a = (int)(t / n), b = (int)(t % n);
   const long long tt = (long long)b * n + a;
-  G[t] = J[t] + J[tt] - 0.5 * (K[t] + K[tt]);
+  const double g = J[t] + J[tt] - 0.5 * (K[t] + K[tt]);
+  G[t] = accumulate ? G[t] + g : g;
 }
 
 }  // namespace
+
+void dens_max_device(MolCtx &m, const double *dP, cudaStream_t st) {
+  k_dens_max<<<(m.nbas * m.nbas + 255) / 256, 256, 0, st>>>(dP, m.nao, m.aooff, m.nbas, m.Dsh);
+  engine().launches++;
+}
 
 // ------------------------------------------------------------ context
 int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, const double *env,
@@ -229,7 +240,8 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
       !al((void **)&m.env, sizeof(double) * nenv) || !al((void **)&m.aooff, sizeof(int) * (nbas + 1)) ||
       !al((void **)&m.pairs, sizeof(PairInfo) * m.npairs) || !al((void **)&m.pcls, sizeof(int) * m.npairs) ||
       !al((void **)&m.pp, sizeof(PrimPair) * npp) || !al((void **)&m.Q, sizeof(double) * m.npairs) ||
-      !al((void **)&m.Dsh, sizeof(double) * nbas * nbas))
+      !al((void **)&m.Dsh, sizeof(double) * nbas * nbas) ||
+      !al((void **)&m.centers, sizeof(double) * 3 * nbas))
     return set_error("molecule: device allocation failed"), LRB_ERR_ALLOC;
   FK_CK(cudaMemcpyAsync(m.atm, atm, sizeof(int) * 6 * natm, cudaMemcpyHostToDevice, st));
   FK_CK(cudaMemcpyAsync(m.bas, bas, sizeof(int) * 8 * nbas, cudaMemcpyHostToDevice, st));
@@ -237,6 +249,13 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
   FK_CK(cudaMemcpyAsync(m.aooff, m.h_aooff.data(), sizeof(int) * (nbas + 1), cudaMemcpyHostToDevice, st));
   FK_CK(cudaMemcpyAsync(m.pairs, pr.data(), sizeof(PairInfo) * m.npairs, cudaMemcpyHostToDevice, st));
   FK_CK(cudaMemcpyAsync(m.pcls, pc.data(), sizeof(int) * m.npairs, cudaMemcpyHostToDevice, st));
+  {
+    std::vector<double> cen(3 * (size_t)nbas);
+    for (int s = 0; s < nbas; ++s)
+      for (int d = 0; d < 3; ++d) cen[3 * s + d] = env[atm[6 * bas[8 * s] + 1] + d];
+    FK_CK(cudaMemcpyAsync(m.centers, cen.data(), sizeof(double) * 3 * nbas, cudaMemcpyHostToDevice, st));
+    FK_CK(cudaStreamSynchronize(st));   // cen goes out of scope
+  }
   k_mol_pairs<<<(npp + 255) / 256, 256, 0, st>>>(m.pairs, m.npairs, m.atm, m.bas, m.env, m.pp, npp);
   engine().launches++;
   FK_CK(cudaGetLastError());
@@ -276,14 +295,14 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
 
 void mol_destroy(MolCtx &m, cudaStream_t st) {
   for (void *p : {(void *)m.atm, (void *)m.bas, (void *)m.env, (void *)m.aooff, (void *)m.pairs,
-                  (void *)m.pcls, (void *)m.pp, (void *)m.Q, (void *)m.Dsh})
+                  (void *)m.pcls, (void *)m.pp, (void *)m.Q, (void *)m.Dsh, (void *)m.centers})
     if (p) cudaFreeAsync(p, st);
   cudaStreamSynchronize(st);
 }
 
 // ------------------------------------------------------------ build
 int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t st,
-               FockStats *stats) {
+               FockStats *stats, int prec, double tau32, bool accumulate) {
   Engine &eng = engine();
   const ClassEntry *tab = class_table();
   const int n = m.nao, nbas = m.nbas;
@@ -310,10 +329,12 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
   FK_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 64, st));
   k_dens_max<<<(nbas * nbas + 255) / 256, 256, 0, st>>>(dP, n, m.aooff, nbas, m.Dsh);
   k_screen<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(m.pairs, m.pcls, m.Q, m.Dsh, nbas, ncand,
-                                                            m.npairs, tau, jobs, keys, idx, count, cap);
+                                                            m.npairs, tau, prec, tau32, jobs, keys,
+                                                            idx, count, cap);
   eng.launches += 2;
   FK_CK(cudaGetLastError());
   unsigned long long nj = 0;
+  long long n32 = 0;
   FK_CK(cudaMemcpyAsync(&nj, count, sizeof(nj), cudaMemcpyDeviceToHost, st));
   FK_CK(cudaStreamSynchronize(st));
   if (nj > cap) nj = cap;
@@ -323,10 +344,11 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     void *tmp = eng.ws.reserve_aux(st, tmpb + 64);
     if (!tmp) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
     FK_CK(cub::DeviceRadixSort::SortPairs(tmp, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st));
-    k_class_starts_f<<<1, 64, 0, st>>>(keys2, (long long)nj, NCLASS, starts);
+    k_class_starts_f<<<1, 64, 0, st>>>(keys2, (long long)nj, 2 * NCLASS, starts);
     eng.launches++;
-    long long cls_begin[NCLASS + 1];
-    FK_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * (NCLASS + 1), cudaMemcpyDeviceToHost, st));
+    long long cls_begin[2 * NCLASS + 1];
+    FK_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * (2 * NCLASS + 1),
+                          cudaMemcpyDeviceToHost, st));
     FK_CK(cudaStreamSynchronize(st));
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -334,6 +356,7 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     const double *rys = rys_table_device();
     EriParams prm{};
     prm.pp = m.pp;
+    prm.centers = m.centers;
     prm.expcutoff = eng.expcutoff;
     prm.sph = 0;
     FockParams fk;
@@ -344,27 +367,29 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     fk.J = J;
     fk.K = K;
     fk.n = n;
-    for (int c = 0; c < NCLASS; ++c) {
-      const long long b0 = cls_begin[c], b1 = cls_begin[c + 1];
+    for (int cc = 0; cc < 2 * NCLASS; ++cc) {
+      const long long b0 = cls_begin[cc], b1 = cls_begin[cc + 1];
       if (b1 <= b0) continue;
+      const int c = cc % NCLASS, fi = cc < NCLASS ? 1 : 2;
+      if (fi == 2) n32 += b1 - b0;
       const ClassEntry &ce = tab[c];
       prm.order = idx2 + b0;
       prm.njobs = (int)(b1 - b0);
       int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[1], ERI_THREADS, ce.smem[1]);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[fi], ERI_THREADS, ce.smem[fi]);
       if (per_sm < 1) per_sm = 1;
       const long long tasks = (prm.njobs + ce.slots - 1) / ce.slots;
       long long grid = (long long)nsm * per_sm;
       const long long needg = (tasks + ERI_WARPS - 1) / ERI_WARPS;
       if (grid > needg) grid = needg;
-      ProfRecord rec{c, nullptr, nullptr};
+      ProfRecord rec{cc, nullptr, nullptr};
       if (eng.profile) {
         cudaEventCreate(&rec.start);
         cudaEventCreate(&rec.stop);
         cudaEventRecord(rec.start, st);
       }
-      ce.fn[1]<<<(unsigned)grid, ERI_THREADS, ce.smem[1], st>>>(prm, fk, rys + RYS_TAB_OFFSET[ce.nr],
-                                                                counters + c);
+      ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(prm, fk, rys + RYS_TAB_OFFSET[ce.nr],
+                                                                  counters + cc);
       FK_CK(cudaGetLastError());
       eng.launches++;
       if (eng.profile) {
@@ -373,12 +398,13 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
       }
     }
   }
-  k_symmetrize<<<(unsigned)(((long long)n * n + 255) / 256), 256, 0, st>>>(J, K, n, dG);
+  k_symmetrize<<<(unsigned)(((long long)n * n + 255) / 256), 256, 0, st>>>(J, K, n, dG, accumulate);
   eng.launches++;
   FK_CK(cudaGetLastError());
   if (stats) {
     stats->candidates = ncand;
     stats->quartets = (long long)nj;
+    stats->fp32_quartets = n32;
   }
   return LRB_OK;
 }

@@ -1,0 +1,42 @@
+// Gradient driver and adjoint-kernel class table (see grad.cu).
+#pragma once
+#include <cublas_v2.h>
+
+#include "fock.h"
+#include "grad_kernel.cuh"
+
+namespace lrb {
+
+// gradient classes: X (differentiated, first) and its pair partner Y in
+// any order (3 x 3), the other pair in table orientation (6 pair classes)
+constexpr int NGRADCLS = 54;
+
+using GradKernelFn = void (*)(GradParams, const double *, int *);
+struct GradEntry {
+  GradKernelFn fn;
+  size_t smem;
+  int slots, nr;
+};
+
+template <int LX, int LY, int LZ, int LW, int RAISE>
+GradEntry make_grad_entry() {
+  using C = EriClass<LX + RAISE, LY, LZ, LW>;
+  GradEntry e;
+  e.fn = k_eri_grad<LX, LY, LZ, LW, RAISE>;
+  e.smem = GradLayout<C>::SMEM;
+  e.slots = C::SLOTS;
+  e.nr = C::NR;
+  return e;
+}
+
+// t is GradEntry[NGRADCLS][2] (RAISE 0, 2); id = (lx*3 + ly)*6 + ket pair class
+void grad_register_x0(GradEntry *t);
+void grad_register_x1(GradEntry *t);
+void grad_register_x2(GradEntry *t);
+
+cublasHandle_t grad_blas();
+// d_grad[t] += cH dH + cR dR + cS dS for env[s1 + t]; d_P on the device.
+int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, double tau,
+             double *d_grad, int s1, cudaStream_t st);
+
+}  // namespace lrb

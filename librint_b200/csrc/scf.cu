@@ -253,14 +253,36 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
   int it = 0;
   int nd = 0;
   double fock_ms = 0.0;
-  long long quartets = 0;
-  std::vector<double> Bm;
+  long long quartets = 0, q32 = 0;
+  // incremental (mixed) mode: Gc holds G(Pb), Pb the density it was built for
+  double *Gc = o.mixed ? dv.alloc<double>(nn) : nullptr;
+  double *Pb = o.mixed ? dv.alloc<double>(nn) : nullptr;
+  double *dPm = o.mixed ? dv.alloc<double>(nn) : nullptr;
+  if (!dv.ok) return set_error("scf: device allocation failed"), LRB_ERR_ALLOC;
+  int since_full = 1 << 30, phase = -1;   // phase 1: all FP32, 2: split
   while (delta > o.conv && it < o.max_iter) {
     cudaMemcpyAsync(Pold, P, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
     const auto tf = std::chrono::steady_clock::now();
     FockStats fs;
-    if ((rc = fock_build(m, P, G, o.tau, st, &fs))) return rc;
+    if (!o.mixed) {
+      if ((rc = fock_build(m, P, G, o.tau, st, &fs))) return rc;
+    } else {
+      const int want = delta > o.fp32_until && it > 0 ? 1 : (it == 0 ? 1 : 2);
+      const bool full = want != phase || since_full >= o.rebuild_every;
+      if (full) {
+        if ((rc = fock_build(m, P, Gc, o.tau, st, &fs, want, o.tau32, false))) return rc;
+        since_full = 0;
+        phase = want;
+      } else {
+        k_axpby<<<gb, 256, 0, st>>>(P, Pb, dPm, 1.0, -1.0, nn);
+        if ((rc = fock_build(m, dPm, Gc, o.tau, st, &fs, phase, o.tau32, true))) return rc;
+        ++since_full;
+      }
+      cudaMemcpyAsync(Pb, P, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(G, Gc, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
+    }
     quartets += fs.quartets;
+    q32 += fs.fp32_quartets;
     k_axpby<<<gb, 256, 0, st>>>(H, G, F, 1.0, 1.0, nn);
     cudaStreamSynchronize(st);
     fock_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tf).count();
@@ -305,6 +327,7 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
     res->delta = delta;
     res->converged = delta <= o.conv;
     res->quartets = quartets;
+    res->fp32_quartets = q32;
     res->fock_ms = fock_ms;
   }
   if (delta > o.conv) return set_error("SCF did not converge"), LRB_ERR_SCF;
@@ -355,6 +378,34 @@ int energy_at(MolCtx &m, const double *h_P, double tau, double *E, cudaStream_t 
   const double et = dot(P, T, nn, st, scr), ev = dot(P, V, nn, st, scr), eg = dot(P, G, nn, st, scr);
   *E = et + ev + 0.5 * eg + nuclear_repulsion(m);
   return LRB_OK;
+}
+
+}  // namespace lrb
+
+namespace lrb {
+
+// F = T + V + G(P) with every quartet in FP64 (no screening).
+int scf_dense_fock(MolCtx &m, const double *P, double *F, cudaStream_t st) {
+  const long long nn = (long long)m.nao * m.nao;
+  double *T = nullptr, *V = nullptr, *G = nullptr;
+  if (cudaMallocAsync((void **)&T, sizeof(double) * nn, st) != cudaSuccess ||
+      cudaMallocAsync((void **)&V, sizeof(double) * nn, st) != cudaSuccess ||
+      cudaMallocAsync((void **)&G, sizeof(double) * nn, st) != cudaSuccess)
+    return set_error("fock: allocation failed"), LRB_ERR_ALLOC;
+  double c2s[5 * 9 * 15];
+  fill_c2s(c2s);
+  int rc = int1e_device(1, 0, m.atm, m.natm, m.bas, m.nbas, m.env, m.h_bas.data(), T, st, c2s);
+  if (!rc) rc = int1e_device(2, 0, m.atm, m.natm, m.bas, m.nbas, m.env, m.h_bas.data(), V, st, c2s);
+  if (!rc) rc = fock_build(m, P, G, 0.0, st, nullptr);
+  if (!rc) {
+    const unsigned gb = (unsigned)((nn + 255) / 256);
+    k_axpby<<<gb, 256, 0, st>>>(T, V, F, 1.0, 1.0, nn);
+    k_axpby<<<gb, 256, 0, st>>>(F, G, F, 1.0, 1.0, nn);
+  }
+  cudaFreeAsync(T, st);
+  cudaFreeAsync(V, st);
+  cudaFreeAsync(G, st);
+  return rc;
 }
 
 }  // namespace lrb

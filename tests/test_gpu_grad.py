@@ -1,0 +1,62 @@
+"""Adjoint-kernel gradients (exponents and coefficients) against the
+reference's Enzyme gradients and central finite differences."""
+import numpy as np
+import pytest
+
+from librint_b200 import dscf, scf, synthetic
+from librint_b200.basis import Molecule
+
+pytestmark = pytest.mark.gpu
+
+
+def gmol(golden, key):
+    return Molecule(golden[f"grad/{key}/atm"], golden[f"grad/{key}/bas"], golden[f"grad/{key}/env"],
+                    int(golden[f"grad/{key}/atm"].reshape(-1, 6)[:, 0].sum()))
+
+
+@pytest.mark.parametrize("key", ["h2", "h2o", "water_like"])
+@pytest.mark.parametrize("fn,ref", [("dRf", "dR_c"), ("dHcoref", "dHcore_c"), ("dSf", "dS_c"),
+                                    ("danalyticalf", "danalytical_c")])
+def test_vs_reference_enzyme(golden, key, fn, ref):
+    m = gmol(golden, key)
+    P = golden[f"grad/{key}/P"]
+    got = getattr(dscf, fn)(m, P)
+    want = golden[f"grad/{key}/{ref}"]
+    np.testing.assert_allclose(got, want, rtol=1e-8, atol=1e-9 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("key", ["h2o", "water_like"])
+def test_frozen_density_gradient_vs_central_differences(golden, key):
+    """grad_c = d/dtheta of the energy functional at fixed P (h = 1e-5)."""
+    m = gmol(golden, key)
+    P = golden[f"grad/{key}/P"]
+    g = dscf.grad(m, P)
+    s1, s2 = dscf.split(m.bas)
+    h = 1e-5
+    b = m.bas.reshape(-1, 8)
+    params = sorted(set(int(b[s, 5]) + k for s in range(len(b)) for k in range(b[s, 2])) |
+                    set(int(b[s, 6]) + k for s in range(len(b)) for k in range(b[s, 2])))
+    for t in params[:: max(1, len(params) // 12)]:
+        ep = m.env.copy(); ep[t] += h
+        em = m.env.copy(); em[t] -= h
+        fd = (scf.energy(Molecule(m.atm, m.bas, ep), P) - scf.energy(Molecule(m.atm, m.bas, em), P)) / (2 * h)
+        assert abs(fd - g[t - s1]) < 1e-6 * max(1.0, abs(fd)), (t, fd, g[t - s1])
+
+
+def test_analytical_gradient_vs_scf_differences():
+    """danalytical = total derivative of the converged SCF energy."""
+    m = synthetic.water_like()
+    ctx = scf.MolContext(m)
+    r, P = ctx.scf(conv=1e-11, guess=1, diis=8, return_density=True)
+    g = dscf.danalyticalf(m, P)
+    s1, _ = dscf.split(m.bas)
+    b = m.bas.reshape(-1, 8)
+    h = 1e-5
+    for t in (int(b[0, 5]), int(b[2, 5]) + 1, int(b[3, 6]), int(b[2, 6]) + 2):
+        es = []
+        for sgn in (1, -1):
+            e2 = m.env.copy(); e2[t] += sgn * h
+            es.append(scf.MolContext(Molecule(m.atm, m.bas, e2, m.nelec)).scf(
+                conv=1e-11, guess=1, diis=8).energy)
+        fd = (es[0] - es[1]) / (2 * h)
+        assert abs(fd - g[t - s1]) < 2e-6 * max(1.0, abs(fd)), (t, fd, g[t - s1])
