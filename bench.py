@@ -183,9 +183,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--rhf", type=int, default=1,
+    ap.add_argument("--rhf", type=int, default=0,
                     help="also time RHF on the 60-atom C/H cluster (plain FP64 vs mixed)")
+    ap.add_argument("--classes", default="",
+                    help="comma list of classes to run, e.g. 2222,2221 (default: all 21)")
     args = ap.parse_args()
+    global CLASSES
+    if args.classes:
+        CLASSES = [tuple(int(ch) for ch in c.strip()) for c in args.classes.split(",")]
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -307,15 +312,16 @@ def main():
             te = float(tt.item())
         e2e = {"value": world * len(CLASSES) * args.nq * args.e2e_steps / te, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "note": "lrb_int2e_batch with pinned host buffers; all 21 classes per step"}
+               "note": "lrb_int2e_batch with pinned host buffers; all %d classes per step"
+                       % len(CLASSES)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         s = pick_sample(data, threads)
         v, tcpu = cpu_sample(data, s, threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"first {s} quartets of each of the 21 classes of the same workload "
-                         f"({21 * s} quartets, {tcpu:.1f} s), oracle/ C++ restatement, "
+               "sample": f"first {s} quartets of each of the {len(CLASSES)} classes of the same "
+                         f"workload ({len(CLASSES) * s} quartets, {tcpu:.1f} s), oracle/ C++ restatement, "
                          f"OpenMP over quartets"}
 
     rhf = run_rhf() if (args.rhf and rank == 0) else None
@@ -327,9 +333,12 @@ def main():
             "ms_per_step": elapsed / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded, distribution of the ERI sweep config)",
-            "config": {"workload": "ERI sweep: 21 classes (ss|ss)..(dd|dd) x %d quartets per "
+            "config": {"workload": "ERI sweep: %s x %d quartets per "
                                    "class per GPU, K=1..6, exponents log-uniform [0.05,5000], "
-                                   "centres in a 10 A cube, spherical output" % args.nq,
+                                   "centres in a 10 A cube, spherical output"
+                                   % ("21 classes (ss|ss)..(dd|dd)" if len(CLASSES) == 21 else
+                                      "classes " + ",".join("%d%d%d%d" % c for c in CLASSES),
+                                      args.nq),
                        "quartets_per_step": len(CLASSES) * args.nq * world,
                        "l2": "outputs (%.1f GB/step) exceed L2; no flush needed" %
                              (sum(t['out'].numel() for t in dev_data) * 8 / 1e9),

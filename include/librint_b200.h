@@ -182,6 +182,22 @@ LRB_API double *danalytical_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l
 LRB_API double *denergy_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
                           size_t env_l, double *P_p, size_t P_l);
 
+/* ---------------------------------------------------------------------
+ * Learned initial guess: MLP kernels (FP32, device pointers, async on
+ * `stream`).  No reference counterpart (the reference starts from P = I,
+ * src/scf.rs:757-764).  A layer is Y = act(X W^T + b), X (M x K), W (N x K);
+ * act 0 identity, 1 SiLU.
+ * -------------------------------------------------------------------*/
+LRB_API int lrb_mlp_forward(const float *X, int M, int K, const float *W, const float *b, int N,
+                            int act, float *Z, float *Y, void *stream);
+LRB_API int lrb_mlp_backward(const float *X, int M, int K, const float *W, int N, int act,
+                             const float *Z, const float *dY, float *dZ, float *dW, float *db,
+                             float *dX, void *stream);
+LRB_API int lrb_mse(const float *Y, const float *T, const float *Wt, long long n, float inv_count,
+                    float *dY, float *loss, void *stream);
+LRB_API int lrb_adam(float *p, const float *g, float *m, float *v, long long n, float lr,
+                     float b1, float b2, float eps, int step, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,6 +94,13 @@ def _optional(L):
         "scf_c": (c_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_sz, c_int, c_d)),
         "lrb_grad_len": (c_int, (c_vp,)),
         "lrb_grad": (c_int, (c_vp, P_d, c_d, c_d, c_d, c_d, P_d)),
+        "lrb_mlp_forward": (c_int, (c_vp, c_int, c_int, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
+                                    c_vp)),
+        "lrb_mlp_backward": (c_int, (c_vp, c_int, c_int, c_vp, c_int, c_int, c_vp, c_vp, c_vp,
+                                     c_vp, c_vp, c_vp, c_vp)),
+        "lrb_mse": (c_int, (c_vp, c_vp, c_vp, c_ll, ctypes.c_float, c_vp, c_vp, c_vp)),
+        "lrb_adam": (c_int, (c_vp, c_vp, c_vp, c_vp, c_ll, ctypes.c_float, ctypes.c_float,
+                             ctypes.c_float, ctypes.c_float, c_int, c_vp)),
     }
     for name in ("grad_c", "dS_c", "dHcore_c", "dR_c", "danalytical_c", "denergy_c"):
         sigs[name] = (P_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, P_d, c_sz))

@@ -452,9 +452,11 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
       }
     }
     __syncwarp();
+    // Every warp barrier below is reached by all 32 lanes: lanes without a
+    // job (the tail of the last task) skip only the work, never a barrier.
+    R *T2 = Bk + C::NBRA * C::NKET;
     if (MODE == 0 && have) {
       // ket transform: T2[bra cart][ket out] (identity when cartesian)
-      R *T2 = Bk + C::NBRA * C::NKET;
       for (int t = rho; t < C::NBRA * NKO; t += C::LANES) {
         const int kap = t / C::NBRA, bc = t - kap * C::NBRA;
         const int ko = kap % NKo, lo = kap / NKo;
@@ -474,7 +476,9 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
         }
         T2[t] = v;
       }
-      __syncwarp();
+    }
+    if (MODE == 0) __syncwarp();
+    if (MODE == 0 && have) {
       // bra transform and store (i fastest -> coalesced for canonical order)
       for (int t = rho; t < NBO * NKO; t += C::LANES) {
         const int kap = t / NBO, b = t - kap * NBO;

@@ -1,0 +1,551 @@
+"""Learned initial density for RHF: a small MLP over atom-pair features.
+
+The reference starts every SCF from P = I (src/scf.rs:757-764).  This module
+predicts the converged density block by block instead:
+
+* every unordered atom pair (A, B), A == B included, gets a local frame F
+  (orthonormal rows e1, e2, e3).  Off the diagonal e1 points from A to B and
+  the origin O is the bond midpoint; on the diagonal O = R_A and e1 points to
+  the nearest atom of another element (the nearest atom if there is none).
+  e2 lies in the plane of e1 and the nearest third atom that is not on the
+  e1 axis, pointing towards it; e3 = e1 x e2.
+* features: the pair type (one-hot over element pairs and diagonal
+  elements), r_AB, exp(-r_AB / 2), and for each element and each radial
+  Gaussian g_k the sums over the other atoms j of g_k(|d_j|) [1, d_j/|d_j|],
+  with d_j = F (R_j - O).  They are invariant under rotation and translation
+  of the molecule.
+* target: the block rotated into the frame, P_loc = A_A(F)^T P_AB A_B(F),
+  with A(Q) the matrix that carries cartesian GTOs through the rotation Q
+  (libcint cartesian order), stored in an nmax x nmax grid with a mask.
+
+Prediction inverts the rotation, P_AB = A_A(F^T)^T P_loc A_B(F^T), fills the
+lower triangle from the upper one and scales P so that tr(P S) = N_elec.
+The network (FP32, SiLU hidden layers, linear output) runs and trains on the
+GPU through this library's own kernels (lrb_mlp_forward / lrb_mlp_backward /
+lrb_mse / lrb_adam); torch only holds the device memory.  The guess is tied
+to one basis per element; ``LearnedGuess.applies`` says whether a molecule
+matches and the SCF falls back to the core-Hamiltonian guess when it does not.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .basis import Molecule, ncart
+
+RADIAL_CENTRES = np.array([1.0, 2.5, 4.0, 5.5, 7.0, 8.5, 10.0])   # bohr
+RADIAL_WIDTH = 1.2
+
+
+# ----------------------------------------------------------------- rotations
+def cart_exponents(l: int):
+    """libcint cartesian order: x power descending, then y descending."""
+    return [(lx, ly, l - lx - ly) for lx in range(l, -1, -1) for ly in range(l - lx, -1, -1)]
+
+
+# d monomials xx, xy, xz, yy, yz, zz as axis pairs (libcint order)
+_D_PAIRS = ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))
+
+
+def cart_rotation(l: int, Q: np.ndarray) -> np.ndarray:
+    """A with phi_mu(Q^T v) = sum_nu A[mu, nu] phi_nu(v) for the cartesian
+    monomials of degree l; A(Q1 Q2) = A(Q2) A(Q1)."""
+    if l == 0:
+        return np.ones((1, 1))
+    if l == 1:
+        return np.ascontiguousarray(Q.T)
+    if l == 2:
+        # (Q^T v)_i (Q^T v)_j = sum_kl Q[k,i] Q[l,j] v_k v_l
+        A = np.empty((6, 6))
+        for mu, (i, j) in enumerate(_D_PAIRS):
+            for nu, (k, m) in enumerate(_D_PAIRS):
+                A[mu, nu] = Q[k, i] * Q[m, j] + (Q[m, i] * Q[k, j] if k != m else 0.0)
+        return A
+    exps = cart_exponents(l)
+    index = {e: i for i, e in enumerate(exps)}
+    A = np.zeros((len(exps), len(exps)))
+    for mu, e in enumerate(exps):
+        poly = {(0, 0, 0): 1.0}
+        for axis, power in enumerate(e):
+            for _ in range(power):
+                nxt = {}
+                for mono, c in poly.items():
+                    for j in range(3):
+                        q = Q[j, axis]          # (Q^T v)_axis = sum_j Q[j, axis] v_j
+                        if q == 0.0:
+                            continue
+                        m2 = list(mono)
+                        m2[j] += 1
+                        m2 = tuple(m2)
+                        nxt[m2] = nxt.get(m2, 0.0) + c * q
+                poly = nxt
+        for mono, c in poly.items():
+            A[mu, index[mono]] += c
+    return A
+
+
+def _atom_layout(m: Molecule):
+    """Per atom: (ao offset, [l of each shell], ncart total)."""
+    bas = np.asarray(m.bas).reshape(-1, 8)
+    off = 0
+    atoms = {}
+    for b in bas:
+        a, l = int(b[0]), int(b[1])
+        nc = ncart(l) * int(b[3])
+        atoms.setdefault(a, [None, [], 0])
+        if atoms[a][0] is None:
+            atoms[a][0] = off
+        if off != atoms[a][0] + atoms[a][2]:
+            raise ValueError("shells of one atom must be contiguous")
+        atoms[a][1].append(l)
+        atoms[a][2] += nc
+        off += nc
+    return [tuple(atoms[a]) for a in range(len(atoms))]
+
+
+def _atom_prims(m: Molecule):
+    """Per atom: its shells' exponents and coefficients, concatenated."""
+    bas = np.asarray(m.bas).reshape(-1, 8)
+    env = np.asarray(m.env)
+    out = {}
+    for b in bas:
+        k = int(b[2]) * 1
+        v = np.concatenate([env[b[5]:b[5] + k], env[b[6]:b[6] + k * int(b[3])]])
+        out.setdefault(int(b[0]), []).append(v)
+    return [np.concatenate(out[a]) for a in range(len(out))]
+
+
+def atom_rotation(ls, Q):
+    n = sum(ncart(l) for l in ls)
+    A = np.zeros((n, n))
+    o = 0
+    for l in ls:
+        k = ncart(l)
+        A[o:o + k, o:o + k] = cart_rotation(l, Q)
+        o += k
+    return A
+
+
+# ------------------------------------------------------------------ features
+def molecule_geometry(m: Molecule):
+    atm = np.asarray(m.atm).reshape(-1, 6)
+    env = np.asarray(m.env)
+    z = atm[:, 0].astype(int)
+    xyz = np.stack([env[p:p + 3] for p in atm[:, 1]])
+    return z, xyz
+
+
+def _frame(xyz, z, a, b):
+    n = len(xyz)
+    if a != b:
+        o = 0.5 * (xyz[a] + xyz[b])
+        e1 = xyz[b] - xyz[a]
+    else:
+        o = xyz[a]
+        d = np.linalg.norm(xyz - o, axis=1)
+        d[a] = np.inf
+        other = np.where(z != z[a], d, np.inf)
+        j = int(np.argmin(other)) if np.isfinite(other).any() else int(np.argmin(d))
+        e1 = xyz[j] - o
+    e1 = e1 / np.linalg.norm(e1)
+    d = np.linalg.norm(xyz - o, axis=1)
+    order = np.argsort(d, kind="stable")
+    e2 = None
+    for j in order:
+        if j in (a, b):
+            continue
+        t = xyz[j] - o
+        perp = t - (t @ e1) * e1
+        if np.linalg.norm(perp) > 0.1:
+            e2 = perp / np.linalg.norm(perp)
+            break
+    if e2 is None:                       # linear molecule: any perpendicular
+        t = np.array([1.0, 0.0, 0.0]) if abs(e1[0]) < 0.9 else np.array([0.0, 1.0, 0.0])
+        e2 = t - (t @ e1) * e1
+        e2 /= np.linalg.norm(e2)
+    e3 = np.cross(e1, e2)
+    return o, np.stack([e1, e2, e3])
+
+
+@dataclass
+class PairSet:
+    pairs: np.ndarray        # (np, 2) atom indices, a <= b after type ordering
+    types: np.ndarray        # (np,) type index
+    frames: np.ndarray       # (np, 3, 3)
+    X: np.ndarray            # (np, nfeat) float64
+
+
+class PairModel:
+    """Element set and per-element AO layout a network is built for."""
+
+    def __init__(self, elements, layouts, prims=None):
+        self.elements = tuple(sorted(elements, reverse=True))
+        self.layouts = {int(k): tuple(v) for k, v in layouts.items()}   # Z -> shell ls
+        # Z -> concatenated (exponents, coefficients) of its shells, or None
+        self.prims = {int(k): np.asarray(v) for k, v in (prims or {}).items()}
+        self.nao = {zz: sum(ncart(l) for l in self.layouts[zz]) for zz in self.elements}
+        self.nmax = max(self.nao.values())
+        pt = [(p, q) for i, p in enumerate(self.elements) for q in self.elements[i:]]
+        self.type_names = [f"{p}-{q}" for p, q in pt] + [f"{p}" for p in self.elements]
+        self.type_index = {pq: i for i, pq in enumerate(pt)}
+        for i, p in enumerate(self.elements):
+            self.type_index[(p,)] = len(pt) + i
+        self.ntypes = len(self.type_names)
+        self.nfeat = self.ntypes + 2 + len(self.elements) * len(RADIAL_CENTRES) * 4
+        self.nout = self.nmax * self.nmax
+
+    @staticmethod
+    def from_molecule(m: Molecule) -> "PairModel":
+        z, _ = molecule_geometry(m)
+        lay, prims = {}, {}
+        ap = _atom_prims(m)
+        for a, (_, ls, _) in enumerate(_atom_layout(m)):
+            zz = int(z[a])
+            if zz in lay and (tuple(lay[zz]) != tuple(ls) or not np.array_equal(prims[zz], ap[a])):
+                raise ValueError("atoms of one element carry different shells")
+            lay[zz] = tuple(ls)
+            prims[zz] = ap[a]
+        return PairModel(sorted(set(int(v) for v in z)), lay, prims)
+
+    def applies(self, m: Molecule) -> bool:
+        """Same elements (a subset), the same shells per element and (when the
+        model records them) the same exponents and coefficients."""
+        z, _ = molecule_geometry(m)
+        try:
+            lay = _atom_layout(m)
+        except ValueError:
+            return False
+        bas = np.asarray(m.bas).reshape(-1, 8)
+        if not (bas[:, 3] == 1).all():
+            return False
+        ap = _atom_prims(m)
+        for a, (_, ls, _) in enumerate(lay):
+            zz = int(z[a])
+            if zz not in self.layouts or tuple(ls) != self.layouts[zz]:
+                return False
+            ref = self.prims.get(zz)
+            if ref is not None and (ref.shape != ap[a].shape or
+                                    not np.allclose(ref, ap[a], rtol=1e-12, atol=0.0)):
+                return False
+        return True
+
+    def pairs(self, m: Molecule) -> PairSet:
+        z, xyz = molecule_geometry(m)
+        n = len(z)
+        pl, tl, fl, xl = [], [], [], []
+        nk = len(RADIAL_CENTRES)
+        for a in range(n):
+            for b in range(a, n):
+                aa, bb = a, b
+                if z[b] > z[a]:
+                    aa, bb = b, a           # heavier element first
+                if aa == bb:
+                    t = self.type_index[(int(z[aa]),)]
+                else:
+                    t = self.type_index[(int(z[aa]), int(z[bb]))]
+                o, F = _frame(xyz, z, aa, bb)
+                x = np.zeros(self.nfeat)
+                x[t] = 1.0
+                if aa != bb:
+                    r = np.linalg.norm(xyz[bb] - xyz[aa])
+                    x[self.ntypes] = r
+                    x[self.ntypes + 1] = math.exp(-0.5 * r)
+                base = self.ntypes + 2
+                for j in range(n):
+                    if j in (aa, bb):
+                        continue
+                    d = F @ (xyz[j] - o)
+                    rj = np.linalg.norm(d)
+                    g = np.exp(-((rj - RADIAL_CENTRES) / RADIAL_WIDTH) ** 2)
+                    e = self.elements.index(int(z[j]))
+                    blk = base + e * nk * 4
+                    u = d / max(rj, 1e-12)
+                    x[blk:blk + nk] += g
+                    x[blk + nk:blk + 2 * nk] += g * u[0]
+                    x[blk + 2 * nk:blk + 3 * nk] += g * u[1]
+                    x[blk + 3 * nk:blk + 4 * nk] += g * u[2]
+                pl.append((aa, bb))
+                tl.append(t)
+                fl.append(F)
+                xl.append(x)
+        return PairSet(np.array(pl, dtype=np.int64), np.array(tl, dtype=np.int64),
+                       np.array(fl), np.array(xl))
+
+    def _rot(self, zz, F):
+        return atom_rotation(self.layouts[zz], F)
+
+    def to_local(self, m: Molecule, P: np.ndarray, ps: PairSet):
+        """(np, nmax*nmax) targets and masks from a density."""
+        z, _ = molecule_geometry(m)
+        lay = _atom_layout(m)
+        Y = np.zeros((len(ps.pairs), self.nmax, self.nmax))
+        M = np.zeros_like(Y)
+        for i, ((a, b), F) in enumerate(zip(ps.pairs, ps.frames)):
+            oa, _, na = lay[a]
+            ob, _, nb = lay[b]
+            blk = P[oa:oa + na, ob:ob + nb]
+            loc = self._rot(int(z[a]), F).T @ blk @ self._rot(int(z[b]), F)
+            Y[i, :na, :nb] = loc
+            M[i, :na, :nb] = 1.0
+        return Y.reshape(len(ps.pairs), -1), M.reshape(len(ps.pairs), -1)
+
+    def to_density(self, m: Molecule, Yloc: np.ndarray, ps: PairSet):
+        z, _ = molecule_geometry(m)
+        lay = _atom_layout(m)
+        n = lay[-1][0] + lay[-1][2]
+        P = np.zeros((n, n))
+        Y = Yloc.reshape(len(ps.pairs), self.nmax, self.nmax)
+        for i, ((a, b), F) in enumerate(zip(ps.pairs, ps.frames)):
+            oa, _, na = lay[a]
+            ob, _, nb = lay[b]
+            Ft = F.T
+            blk = self._rot(int(z[a]), Ft).T @ Y[i, :na, :nb] @ self._rot(int(z[b]), Ft)
+            if a == b:
+                blk = 0.5 * (blk + blk.T)
+            P[oa:oa + na, ob:ob + nb] = blk
+            P[ob:ob + nb, oa:oa + na] = blk.T
+        return P
+
+
+# ------------------------------------------------------------------- network
+class MLP:
+    """Fully connected network; FP32 parameters on the GPU, this library's
+    kernels for forward, backward, loss and Adam."""
+
+    def __init__(self, sizes, seed=0, device="cuda"):
+        import torch
+        self.torch = torch
+        self.sizes = list(sizes)
+        g = np.random.default_rng(seed)
+        self.W, self.b = [], []
+        for k, n in zip(self.sizes[:-1], self.sizes[1:]):
+            w = g.normal(0.0, math.sqrt(1.0 / k), size=(n, k)).astype(np.float32)
+            self.W.append(torch.tensor(w, device=device))
+            self.b.append(torch.zeros(n, dtype=torch.float32, device=device))
+        self.device = device
+
+    @property
+    def params(self):
+        return [p for pair in zip(self.W, self.b) for p in pair]
+
+    def state(self):
+        return {f"p{i}": p.detach().cpu().numpy() for i, p in enumerate(self.params)}
+
+    def load(self, st):
+        ps = self.params
+        for i, p in enumerate(ps):
+            p.copy_(self.torch.tensor(st[f"p{i}"], device=self.device))
+
+    def forward(self, X, keep=False):
+        from . import _bindings as B
+        torch = self.torch
+        lib = B.lib()
+        stream = torch.cuda.current_stream().cuda_stream
+        h = X.contiguous()
+        acts, zs = [h], []
+        L = len(self.W)
+        for i, (W, b) in enumerate(zip(self.W, self.b)):
+            n = W.shape[0]
+            y = torch.empty((h.shape[0], n), dtype=torch.float32, device=self.device)
+            z = torch.empty_like(y) if keep else None
+            act = 1 if i < L - 1 else 0
+            rc = lib.lrb_mlp_forward(_fp(h), h.shape[0], h.shape[1], _fp(W), _fp(b), n, act,
+                                     _fp(z) if z is not None else None, _fp(y),
+                                     ctypes.c_void_p(stream))
+            B.check(rc, "lrb_mlp_forward")
+            acts.append(y)
+            zs.append(z)
+            h = y
+        return (h, acts, zs) if keep else h
+
+    def backward(self, acts, zs, dY):
+        """Gradients of every parameter from dLoss/dOutput."""
+        from . import _bindings as B
+        torch = self.torch
+        lib = B.lib()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        grads = [None] * (2 * len(self.W))
+        g = dY
+        L = len(self.W)
+        for i in range(L - 1, -1, -1):
+            W = self.W[i]
+            n, k = W.shape
+            X = acts[i]
+            M = X.shape[0]
+            dZ = torch.empty((M, n), dtype=torch.float32, device=self.device)
+            dW = torch.empty_like(W)
+            db = torch.empty_like(self.b[i])
+            dX = torch.empty((M, k), dtype=torch.float32, device=self.device) if i > 0 else None
+            act = 1 if i < L - 1 else 0
+            z = zs[i]
+            rc = lib.lrb_mlp_backward(_fp(X), M, k, _fp(W), n, act, _fp(z), _fp(g), _fp(dZ),
+                                      _fp(dW), _fp(db), _fp(dX) if dX is not None else None, stream)
+            B.check(rc, "lrb_mlp_backward")
+            grads[2 * i] = dW
+            grads[2 * i + 1] = db
+            g = dX
+        return grads
+
+
+def _fp(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Adam:
+    def __init__(self, params, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        import torch
+        self.params = params
+        self.m = [torch.zeros_like(p) for p in params]
+        self.v = [torch.zeros_like(p) for p in params]
+        self.lr, self.b1, self.b2, self.eps = lr, b1, b2, eps
+        self.t = 0
+
+    def step(self, grads, lr=None):
+        from . import _bindings as B
+        import torch
+        self.t += 1
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for p, g, m, v in zip(self.params, grads, self.m, self.v):
+            rc = B.lib().lrb_adam(_fp(p), _fp(g), _fp(m), _fp(v), p.numel(),
+                                  self.lr if lr is None else lr, self.b1, self.b2, self.eps,
+                                  self.t, stream)
+            B.check(rc, "lrb_adam")
+
+
+def mse(Y, T, Wt, loss, inv_count=None):
+    """Weighted squared error sum(w (y - t)^2) * inv_count (default 1/numel);
+    returns dY and accumulates the loss into the device scalar ``loss``."""
+    from . import _bindings as B
+    import torch
+    dY = torch.empty_like(Y)
+    inv = 1.0 / Y.numel() if inv_count is None else inv_count
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = B.lib().lrb_mse(_fp(Y), _fp(T), _fp(Wt) if Wt is not None else None, Y.numel(),
+                         inv, _fp(dY), _fp(loss), stream)
+    B.check(rc, "lrb_mse")
+    return dY
+
+
+# -------------------------------------------------------------- the guess
+class LearnedGuess:
+    """Pair model + network + normalisation; ``predict(m)`` gives P0."""
+
+    def __init__(self, model: PairModel, hidden=(256, 256, 256), seed=0, device="cuda"):
+        self.model = model
+        self.hidden = tuple(hidden)
+        self.net = MLP([model.nfeat, *hidden, model.nout], seed=seed, device=device)
+        self.xmu = np.zeros(model.nfeat)
+        self.xsd = np.ones(model.nfeat)
+        self.ymu = np.zeros((model.ntypes, model.nout))
+        self.ysd = np.ones((model.ntypes, model.nout))
+        self.device = device
+
+    def applies(self, m: Molecule) -> bool:
+        return self.model.applies(m)
+
+    # data ------------------------------------------------------------
+    def dataset(self, mols, dens):
+        X, Y, M, T = [], [], [], []
+        for m, P in zip(mols, dens):
+            ps = self.model.pairs(m)
+            y, mk = self.model.to_local(m, P, ps)
+            X.append(ps.X)
+            Y.append(y)
+            M.append(mk)
+            T.append(ps.types)
+        return np.concatenate(X), np.concatenate(Y), np.concatenate(M), np.concatenate(T)
+
+    def fit_normalisation(self, X, Y, M, T):
+        self.xmu = X.mean(0)
+        sd = X.std(0)
+        self.xsd = np.where(sd > 1e-6, sd, 1.0)
+        for t in range(self.model.ntypes):
+            sel = T == t
+            if not sel.any():
+                continue
+            self.ymu[t] = Y[sel].mean(0)
+            sd = Y[sel].std(0)
+            self.ysd[t] = np.where(sd > 1e-8, sd, 1e-8) * M[sel][0]
+
+    def _scaled(self, X, Y, M, T):
+        xs = (X - self.xmu) / self.xsd
+        ysd = self.ysd[T]
+        ys = np.where(ysd > 1e-8, (Y - self.ymu[T]) / np.maximum(ysd, 1e-8), 0.0)
+        w = M * (ysd > 1e-8)
+        return xs, ys, w
+
+    def train(self, X, Y, M, T, epochs=200, batch=2048, lr=1e-3, seed=0, log=None):
+        """Adam on the weighted MSE of the standardised targets, all on the
+        GPU; returns the per-epoch mean loss."""
+        import torch
+        xs, ys, w = self._scaled(X, Y, M, T)
+        dev = self.device
+        Xd = torch.tensor(xs, dtype=torch.float32, device=dev)
+        Yd = torch.tensor(ys, dtype=torch.float32, device=dev)
+        Wd = torch.tensor(w, dtype=torch.float32, device=dev)
+        opt = Adam(self.net.params, lr=lr)
+        n = len(xs)
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        loss = torch.zeros(1, dtype=torch.float32, device=dev)
+        hist = []
+        total = epochs * ((n + batch - 1) // batch)
+        step = 0
+        for ep in range(epochs):
+            perm = torch.randperm(n, generator=g).to(dev)
+            loss.zero_()
+            nb = 0
+            for s in range(0, n, batch):
+                idx = perm[s:s + batch]
+                xb, yb, wb = Xd[idx].contiguous(), Yd[idx].contiguous(), Wd[idx].contiguous()
+                out, acts, zs = self.net.forward(xb, keep=True)
+                dY = mse(out, yb, wb, loss)
+                grads = self.net.backward(acts, zs, dY)
+                cur = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(total, 1)))
+                opt.step(grads, lr=max(cur, lr * 0.02))
+                step += 1
+                nb += 1
+            hist.append(float(loss.item()) / nb)
+            if log and (ep % max(1, epochs // 10) == 0 or ep == epochs - 1):
+                log(f"epoch {ep}: loss {hist[-1]:.4e}")
+        return hist
+
+    def predict_local(self, X, T):
+        import torch
+        xs = (X - self.xmu) / self.xsd
+        out = self.net.forward(torch.tensor(xs, dtype=torch.float32, device=self.device))
+        y = out.double().cpu().numpy()
+        return self.ymu[T] + self.ysd[T] * y
+
+    def predict(self, m: Molecule, S: np.ndarray | None = None, nelec=None):
+        ps = self.model.pairs(m)
+        P = self.model.to_density(m, self.predict_local(ps.X, ps.types), ps)
+        if S is not None:
+            ne = m.nelec if nelec is None else nelec
+            tr = float(np.sum(P * S))
+            if tr > 0:
+                P *= ne / tr
+        return P
+
+    # persistence -----------------------------------------------------
+    def save(self, path):
+        st = self.net.state()
+        lay = {f"layout_{z}": np.array(v, dtype=np.int64) for z, v in self.model.layouts.items()}
+        lay.update({f"prims_{z}": v for z, v in self.model.prims.items()})
+        np.savez_compressed(path, sizes=np.array(self.net.sizes), xmu=self.xmu, xsd=self.xsd,
+                            ymu=self.ymu, ysd=self.ysd, elements=np.array(self.model.elements),
+                            **lay, **st)
+
+    @staticmethod
+    def load(path, device="cuda") -> "LearnedGuess":
+        f = np.load(path)
+        el = [int(v) for v in f["elements"]]
+        model = PairModel(el, {z: tuple(int(v) for v in f[f"layout_{z}"]) for z in el},
+                          {z: f[f"prims_{z}"] for z in el if f"prims_{z}" in f.files})
+        sizes = [int(v) for v in f["sizes"]]
+        g = LearnedGuess(model, hidden=sizes[1:-1], device=device)
+        g.xmu, g.xsd, g.ymu, g.ysd = f["xmu"], f["xsd"], f["ymu"], f["ysd"]
+        g.net.load({k: f[k] for k in f.files if k.startswith("p")})
+        return g

@@ -16,7 +16,8 @@ contraction coefficients are positive and PySCF-normalised
   with H at 1.09 A on edge carbons; C 3s2p1d, H 2s1p, K uniform in 1..6.
 * ``hc_chain``       -- zig-zag C_nH_(2n+2) chain, C-C 1.54 A, C-H 1.09 A,
   +-0.03 A noise, same shells.
-* ``benzene_like``   -- C6H6 ring, bonds +-0.05 A, angles +-3 deg.
+* ``benzene_like``   -- C6H6 ring, bonds +-0.05 A, angles +-3 deg, one shell
+  set per element.
 """
 from __future__ import annotations
 
@@ -132,19 +133,32 @@ C_RANGE = (0.1, 5000.0)
 H_RANGE = (0.1, 50.0)
 
 
-def _add_ch_basis(b: Builder, rng, atoms_z, kmax=6):
+def _draw_shells(rng, z, kmax):
+    shells, (lo, hi) = (C_SHELLS, C_RANGE) if z == 6 else (H_SHELLS, H_RANGE)
+    out = []
+    for l in shells:
+        k = int(rng.integers(1, kmax + 1))
+        out.append((l, _exps(rng, k, lo, hi), _coefs(rng, k)))
+    return out
+
+
+def _add_ch_basis(b: Builder, rng, atoms_z, kmax=6, per_element=False):
+    """Per-atom random shells, or (per_element) one draw per element shared
+    by every atom of that element, like a named basis set."""
+    table = {}
+    if per_element:
+        for z in sorted(set(atoms_z), reverse=True):
+            table[z] = _draw_shells(rng, z, kmax)
     for atom, z in enumerate(atoms_z):
-        shells, (lo, hi) = (C_SHELLS, C_RANGE) if z == 6 else (H_SHELLS, H_RANGE)
-        for l in shells:
-            k = int(rng.integers(1, kmax + 1))
-            b.add_shell(atom, l, _exps(rng, k, lo, hi), _coefs(rng, k))
+        for l, e, c in (table[z] if per_element else _draw_shells(rng, z, kmax)):
+            b.add_shell(atom, l, e, c)
 
 
-def _build_ch(z, xyz_ang, rng, name, **meta):
+def _build_ch(z, xyz_ang, rng, name, per_element=False, **meta):
     b = Builder()
     for zi, r in zip(z, xyz_ang):
         b.add_atom(zi, np.asarray(r) * ANG2BOHR)
-    _add_ch_basis(b, rng, z)
+    _add_ch_basis(b, rng, z, per_element=per_element)
     return b.build(name, **meta)
 
 
@@ -210,8 +224,10 @@ def hc_chain(seed: int = 4, ncarbon: int = 6) -> Molecule:
 
 
 def benzene_like(seed: int = 5, basis_seed: int = 5) -> Molecule:
-    """One C6H6-like ring; geometry from ``seed``, basis from ``basis_seed``
-    (the learned-guess data set keeps one basis across geometries)."""
+    """One C6H6-like ring; geometry from ``seed``, basis from ``basis_seed``,
+    one shell set per element (C 3s2p1d = 15, H 2s1p = 5 cartesian AOs; 120
+    AOs in all).  The learned-guess data set keeps one basis across
+    geometries."""
     rng = np.random.default_rng(seed)
     cc, ch = 1.40, 1.09
     cs, hs = [], []
@@ -223,4 +239,4 @@ def benzene_like(seed: int = 5, basis_seed: int = 5) -> Molecule:
         hs.append([rh * math.cos(t), rh * math.sin(t), 0.0])
     xyz = np.vstack([cs, hs])
     return _build_ch([6] * 6 + [1] * 6, xyz, np.random.default_rng(basis_seed), "benzene_like",
-                     seed=seed, basis_seed=basis_seed)
+                     per_element=True, seed=seed, basis_seed=basis_seed)
