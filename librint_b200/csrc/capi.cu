@@ -138,37 +138,82 @@ int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq
                           (cudaStream_t)stream, nullptr);
 }
 
+// Host buffers in and out.  The quartets run in chunks on two alternating
+// non-blocking streams: chunk c's output copy to the host overlaps chunk
+// c+1's preparation and kernels.  A chunk starts only after the previous
+// chunk's kernels (event), because both share the engine's workspace.
 int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const int *atm,
                     int natm, const int *bas, int nbas, const double *env, long long nenv) {
   if (nq == 0) return LRB_OK;
+  if (!out || !shls || nq < 0) return set_error("bad output or quartet list"), LRB_ERR_INPUT;
   int rc = check_common(atm, natm, bas, nbas, env, nenv);
   if (rc) return rc;
-  const long long len = lrb_int2e_batch_len(coord, shls, nq, bas, nbas);
-  if (len < 0) return set_error("shell index out of range"), LRB_ERR_INPUT;
-  cudaStream_t st = nullptr;
-  DevMol m;
-  rc = m.upload(st, atm, natm, bas, nbas, env, nenv);
-  int *d_shls = nullptr;
-  double *d_out = nullptr;
-  if (!rc) {
-    if (cudaMallocAsync((void **)&d_shls, sizeof(int) * 4 * (size_t)nq, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_out, sizeof(double) * (size_t)std::max(len, 1LL), st) != cudaSuccess) {
-      cudaGetLastError();
-      rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
+  if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
+  for (long long q = 0; q < 4 * nq; ++q)
+    if (shls[q] < 0 || shls[q] >= nbas) return set_error("shell index out of range"), LRB_ERR_INPUT;
+  // chunk boundaries: at most CHUNK_Q quartets and about CHUNK_OUT doubles each
+  constexpr long long CHUNK_Q = 1 << 16, CHUNK_OUT = 1 << 23;
+  std::vector<long long> qb{0}, ob{0};
+  {
+    long long cq = 0, co = 0, tot = 0;
+    for (long long q = 0; q < nq; ++q) {
+      long long b = 1;
+      for (int a = 0; a < 4; ++a) b *= shell_dim(coord, bas, shls[4 * q + a]);
+      if (cq > 0 && (cq == CHUNK_Q || co + b > CHUNK_OUT)) {
+        qb.push_back(q);
+        ob.push_back(tot);
+        cq = co = 0;
+      }
+      ++cq;
+      co += b;
+      tot += b;
     }
+    qb.push_back(nq);
+    ob.push_back(tot);
   }
-  if (!rc && cudaMemcpyAsync(d_shls, shls, sizeof(int) * 4 * (size_t)nq, cudaMemcpyHostToDevice, st) != cudaSuccess)
-    rc = (set_error("copy failed"), LRB_ERR_CUDA);
-  if (!rc)
-    rc = eri_batch_device(engine(), d_out, coord, d_shls, nq, m.atm, natm, m.bas, nbas, m.env,
-                          nenv, st, nullptr);
-  if (!rc && cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    rc = (set_error("copy failed"), LRB_ERR_CUDA);
-  if (d_shls) cudaFreeAsync(d_shls, st);
-  if (d_out) cudaFreeAsync(d_out, st);
-  m.release(st);
-  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) {
-    set_error(cudaGetErrorString(cudaGetLastError()));
+  Engine &eng = engine();
+  for (int i = 0; i < 2; ++i) {
+    if (!eng.pipe[i] && cudaStreamCreateWithFlags(&eng.pipe[i], cudaStreamNonBlocking) != cudaSuccess)
+      return set_error("stream creation failed"), LRB_ERR_CUDA;
+    if (!eng.done[i] && cudaEventCreateWithFlags(&eng.done[i], cudaEventDisableTiming) != cudaSuccess)
+      return set_error("event creation failed"), LRB_ERR_CUDA;
+  }
+  DevMol m;
+  rc = m.upload(eng.pipe[0], atm, natm, bas, nbas, env, nenv);
+  const int nchunk = (int)qb.size() - 1;
+  for (int c = 0; c < nchunk && !rc; ++c) {
+    const int X = c & 1;
+    cudaStream_t st = eng.pipe[X];
+    if (c > 0 && cudaStreamWaitEvent(st, eng.done[1 - X], 0) != cudaSuccess) {
+      rc = (set_error("stream wait failed"), LRB_ERR_CUDA);
+      break;
+    }
+    const long long nqc = qb[c + 1] - qb[c], len = ob[c + 1] - ob[c];
+    int *d_sh = (int *)eng.pipe_in[X].get(st, sizeof(int) * 4 * (size_t)nqc);
+    double *d_o = (double *)eng.pipe_out[X].get(st, sizeof(double) * (size_t)std::max(len, 1LL));
+    if (!d_sh || !d_o) {
+      rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
+      break;
+    }
+    if (cudaMemcpyAsync(d_sh, shls + 4 * qb[c], sizeof(int) * 4 * (size_t)nqc,
+                        cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      rc = (set_error("copy failed"), LRB_ERR_CUDA);
+      break;
+    }
+    rc = eri_batch_device(eng, d_o, coord, d_sh, nqc, m.atm, natm, m.bas, nbas, m.env, nenv, st,
+                          nullptr);
+    if (rc) break;
+    if (cudaEventRecord(eng.done[X], st) != cudaSuccess ||
+        cudaMemcpyAsync(out + ob[c], d_o, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost,
+                        st) != cudaSuccess)
+      rc = (set_error("copy failed"), LRB_ERR_CUDA);
+  }
+  const cudaError_t e0 = cudaStreamSynchronize(eng.pipe[0]);
+  const cudaError_t e1 = cudaStreamSynchronize(eng.pipe[1]);
+  m.release(eng.pipe[0]);
+  const cudaError_t e2 = cudaStreamSynchronize(eng.pipe[0]);
+  if (!rc && (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess)) {
+    set_error(cudaGetErrorString(e0 != cudaSuccess ? e0 : (e1 != cudaSuccess ? e1 : e2)));
     rc = LRB_ERR_CUDA;
   }
   return rc;

@@ -33,7 +33,18 @@ Engine &engine() {
   int dev = 0;
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> g(mu);
-  if (!per_dev[dev]) per_dev[dev] = new Engine();
+  if (!per_dev[dev]) {
+    // keep freed stream-ordered memory in the device's default pool instead
+    // of returning it to the driver at every synchronisation, so repeated
+    // cudaMallocAsync of the same sizes does not remap pages
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    per_dev[dev] = new Engine();
+  }
   return *per_dev[dev];
 }
 

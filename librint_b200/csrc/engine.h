@@ -58,6 +58,12 @@ struct Engine {
   bool profile = false;
   std::vector<ProfRecord> prof;
   long long launches = 0;    // kernels of this library launched so far
+  // host-buffer entry points: two non-blocking streams that alternate over
+  // chunks (copy-out of one chunk overlaps the next chunk's kernels) and
+  // per-stream device buffers that only grow
+  cudaStream_t pipe[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  Arena pipe_out[2], pipe_in[2];
 };
 Engine &engine();          // for the current device
 

@@ -13,11 +13,12 @@ contraction coefficients are positive and PySCF-normalised
   shell has its own centre (uniform in a 10 A cube), K uniform in 1..6 and
   exponents log-uniform in [0.05, 5000].
 * ``hc_cluster``     -- C on a perturbed hexagonal lattice (C-C 1.40 +- 0.05 A)
-  with H at 1.09 A on edge carbons; C 3s2p1d, H 2s1p, K uniform in 1..6.
+  with H at 1.09 A on edge carbons; the even-tempered DZP-like set
+  (``DZP_C``/``DZP_H``: C 3s2p1d, H 2s1p).
 * ``hc_chain``       -- zig-zag C_nH_(2n+2) chain, C-C 1.54 A, C-H 1.09 A,
-  +-0.03 A noise, same shells.
-* ``benzene_like``   -- C6H6 ring, bonds +-0.05 A, angles +-3 deg, one shell
-  set per element.
+  +-0.03 A noise, random C 3s2p1d / H 2s1p shells (K uniform in 1..6).
+* ``benzene_like``   -- C6H6 ring, bonds +-0.05 A, angles +-3 deg, the
+  DZP-like set (or random shells per element from ``basis_seed``).
 """
 from __future__ import annotations
 
@@ -154,20 +155,44 @@ def _add_ch_basis(b: Builder, rng, atoms_z, kmax=6, per_element=False):
             b.add_shell(atom, l, e, c)
 
 
-def _build_ch(z, xyz_ang, rng, name, per_element=False, **meta):
+# Even-tempered split-valence set with polarisation ("DZP-like"): C 3s2p1d,
+# H 2s1p, the same shell counts as the random sets above.  The exponents are
+# round geometric sequences chosen for this library (not a published basis);
+# coefficients are positive and normalised like every other shell here.
+DZP_C = ((0, (3000.0, 450.0, 100.0, 28.0, 9.0, 3.2), (0.002, 0.015, 0.07, 0.24, 0.48, 0.33)),
+         (0, (7.5, 1.8, 0.55), (0.05, 0.3, 0.75)),
+         (0, (0.16,), (1.0,)),
+         (1, (18.0, 4.2, 1.2, 0.38), (0.04, 0.24, 0.5, 0.45)),
+         (1, (0.12,), (1.0,)),
+         (2, (0.8,), (1.0,)))
+DZP_H = ((0, (19.0, 2.9, 0.65), (0.035, 0.23, 0.82)),
+         (0, (0.16,), (1.0,)),
+         (1, (0.75,), (1.0,)))
+
+
+def _add_dzp_basis(b: Builder, atoms_z):
+    for atom, z in enumerate(atoms_z):
+        for l, e, c in (DZP_C if z == 6 else DZP_H):
+            b.add_shell(atom, l, np.array(e), np.array(c))
+
+
+def _build_ch(z, xyz_ang, rng, name, per_element=False, dzp=False, **meta):
     b = Builder()
     for zi, r in zip(z, xyz_ang):
         b.add_atom(zi, np.asarray(r) * ANG2BOHR)
-    _add_ch_basis(b, rng, z, per_element=per_element)
+    if dzp:
+        _add_dzp_basis(b, z)
+    else:
+        _add_ch_basis(b, rng, z, per_element=per_element)
     return b.build(name, **meta)
 
 
-def hc_cluster(seed: int = 3, ncarbon: int = 37, aspect: float = 2.0) -> Molecule:
-    """60-atom C/H flake: the ``ncarbon`` honeycomb sites nearest the origin in
+def hc_cluster(seed: int = 3, ncarbon: int = 34, aspect: float = 2.0) -> Molecule:
+    """54-atom C/H flake: the ``ncarbon`` honeycomb sites nearest the origin in
     the metric sqrt(x^2 + (aspect*y)^2) (an elongated flake, so enough edge
     sites carry H), C-C 1.40 A perturbed by +-0.05 A; one H on each carbon
     with two carbon neighbours, two (tilted out of plane) on each carbon with
-    one.  37 C + 23 H, 670 cartesian AOs."""
+    one.  34 C + 20 H (224 electrons), 610 cartesian AOs, the DZP-like set."""
     rng = np.random.default_rng(seed)
     a = 1.40
     pts = []
@@ -197,7 +222,7 @@ def hc_cluster(seed: int = 3, ncarbon: int = 37, aspect: float = 2.0) -> Molecul
     c3 += rng.uniform(-0.05, 0.05, size=c3.shape) / math.sqrt(3)
     xyz = np.vstack([c3, np.array(hs)])
     z = [6] * len(c3) + [1] * len(hs)
-    return _build_ch(z, xyz, rng, "hc_cluster", seed=seed)
+    return _build_ch(z, xyz, rng, "hc_cluster", dzp=True, seed=seed)
 
 
 def hc_chain(seed: int = 4, ncarbon: int = 6) -> Molecule:
@@ -223,11 +248,11 @@ def hc_chain(seed: int = 4, ncarbon: int = 6) -> Molecule:
     return _build_ch(z, xyz, rng, "hc_chain", seed=seed)
 
 
-def benzene_like(seed: int = 5, basis_seed: int = 5) -> Molecule:
-    """One C6H6-like ring; geometry from ``seed``, basis from ``basis_seed``,
-    one shell set per element (C 3s2p1d = 15, H 2s1p = 5 cartesian AOs; 120
-    AOs in all).  The learned-guess data set keeps one basis across
-    geometries."""
+def benzene_like(seed: int = 5, basis_seed: int | None = None) -> Molecule:
+    """One C6H6-like ring; geometry from ``seed``.  Basis: the even-tempered
+    DZP-like set (``basis_seed=None``) or random shells drawn from
+    ``basis_seed``, one shell set per element either way (C 3s2p1d = 15,
+    H 2s1p = 5 cartesian AOs; 120 AOs in all)."""
     rng = np.random.default_rng(seed)
     cc, ch = 1.40, 1.09
     cs, hs = [], []
@@ -238,5 +263,7 @@ def benzene_like(seed: int = 5, basis_seed: int = 5) -> Molecule:
         rh = r + ch + rng.uniform(-0.05, 0.05)
         hs.append([rh * math.cos(t), rh * math.sin(t), 0.0])
     xyz = np.vstack([cs, hs])
+    if basis_seed is None:
+        return _build_ch([6] * 6 + [1] * 6, xyz, None, "benzene_like", dzp=True, seed=seed)
     return _build_ch([6] * 6 + [1] * 6, xyz, np.random.default_rng(basis_seed), "benzene_like",
                      per_element=True, seed=seed, basis_seed=basis_seed)

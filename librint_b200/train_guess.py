@@ -4,8 +4,8 @@
         --out librint_b200/data/guess_c6h6.npz --summary guess_summary.json
 
 Data: seeded C6H6-like rings (``synthetic.benzene_like``: bonds +-0.05 A,
-angles +-3 deg, one shell set per element, 120 cartesian AOs), geometry
-seeds 10000 + i, basis seed 5.  Each density comes from this library's RHF
+angles +-3 deg, the even-tempered DZP-like C 3s2p1d / H 2s1p set, 120
+cartesian AOs), geometry seeds 10000 + i.  Each density comes from this library's RHF
 (core-Hamiltonian guess, DIIS, FP64, density change <= conv).  After the
 first ``--bootstrap`` geometries a provisional network is trained and used as
 the starting density for the rest, which only shortens data generation (the
@@ -30,8 +30,8 @@ from .scf import MolContext
 SCF_OPTS = dict(guess=1, diis=8, tau=1e-12, max_iter=100)
 
 
-def geometry(i: int, basis_seed: int = 5):
-    return synthetic.benzene_like(seed=10000 + i, basis_seed=basis_seed)
+def geometry(i: int):
+    return synthetic.benzene_like(seed=10000 + i)
 
 
 def run_scf(m, conv, guess=None):
