@@ -123,6 +123,31 @@ __global__ void k_pairs(const QuartetJob *__restrict__ jobs, long long nq,
   pp[t] = o;
 }
 
+// Order every shell pair's primitive pairs by ascending screening key (NaN
+// last, ties by position), so the kernel can visit only the passing prefix.
+// One thread per entry; its rank is counted over its own pair's entries.
+__device__ __forceinline__ double cce_key(double c) { return c != c ? INFINITY : c; }
+__global__ void k_pair_sort(const PrimPair *__restrict__ raw, long long nq,
+                            const int *__restrict__ pair_off, const int *__restrict__ npair,
+                            PrimPair *__restrict__ pp, long long npp_total) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= npp_total) return;
+  long long lo = 0, hi = 2 * nq - 1;
+  while (lo < hi) {
+    const long long mid = (lo + hi + 1) >> 1;
+    if (pair_off[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  const long long s0 = pair_off[lo];
+  const int n = npair[lo];
+  const double c = cce_key(raw[t].cce);
+  int rank = 0;
+  for (int u = 0; u < n; ++u) {
+    const double cu = cce_key(raw[s0 + u].cce);
+    rank += (cu < c) || (cu == c && s0 + u < t);
+  }
+  pp[s0 + rank] = raw[t];
+}
+
 // Shell centres, with the bounds of every index a shell carries checked
 // against natm / nenv so later kernels never read outside the inputs.
 __global__ void k_centers(const int *__restrict__ atm, int natm, const int *__restrict__ bas,
@@ -305,12 +330,15 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   if (herr) return set_error("shell with l > 2, nprim > 31 or nctr != 1"), LRB_ERR_UNSUPPORTED;
   const long long npp = (long long)last_poff + last_np;
   if (npp > 2147483647LL) return set_error("too many primitive pairs in one batch"), LRB_ERR_INPUT;
-  PrimPair *pp = (PrimPair *)w.reserve_pairs(st, (size_t)npp * sizeof(PrimPair));
+  // pairs in natural order go to the second half, sorted ones to the first
+  PrimPair *pp = (PrimPair *)w.reserve_pairs(st, 2 * (size_t)std::max(npp, 1LL) * sizeof(PrimPair));
   if (!pp) return set_error("workspace allocation failed"), LRB_ERR_ALLOC;
   if (npp > 0) {
+    PrimPair *raw = pp + npp;
     k_pairs<<<(unsigned)((npp + T - 1) / T), T, 0, st>>>(jobs, nq, pair_off, d_atm, d_bas, d_env,
-                                                         pp, npp);
-    ++eng.launches;
+                                                         raw, npp);
+    k_pair_sort<<<(unsigned)((npp + T - 1) / T), T, 0, st>>>(raw, nq, pair_off, npair, pp, npp);
+    eng.launches += 2;
   }
   LRB_CK(cudaGetLastError());
   int dev = 0, nsm = 0;

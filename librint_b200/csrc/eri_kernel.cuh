@@ -346,7 +346,25 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
       if (pk.ish == pk.jsh) wdeg *= 0.5;
       if (jb.x == jb.y) wdeg *= 0.5;
     }
-    const int np = job.nij * job.nkl;
+    // Primitive quartets to visit.  Output mode: each shell pair's primitive
+    // pairs are sorted by ascending screening key cce, so for ket pair kl the
+    // bra pairs that pass (bra.cce <= cutoff - ket.cce) are a prefix of
+    // length nb(kl), non-increasing in kl; only those are visited.  Fock mode
+    // (pairs in natural order) visits all and tests each.
+    const double cut = prm.expcutoff;
+    int np = 0;
+    if constexpr (MODE == 0) {
+      int nb = job.nij;
+      for (int k = 0; k < job.nkl; ++k) {
+        const double kc = prm.pp[job.pkl_off + k].cce;
+        if (!(kc <= cut)) break;
+        while (nb > 0 && !(prm.pp[job.pij_off + nb - 1].cce <= cut - kc)) --nb;
+        if (nb == 0) break;
+        np += nb;
+      }
+    } else {
+      np = job.nij * job.nkl;
+    }
     int npmax = np;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) npmax = max(npmax, __shfl_xor_sync(0xffffffffu, npmax, o));
@@ -370,16 +388,34 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
     for (int k = 0; k < (C::NEX > 0 ? C::NEX : 1); ++k) xacc[k] = 0;
 
     int ij = 0, kl = 0;
+    int nbk = job.nij;   // output mode: passing bra prefix of the current ket pair
+    if constexpr (MODE == 0) {
+      if (np > 0) {
+        const double kc = prm.pp[job.pkl_off].cce;
+        while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
+      }
+    }
     for (int p = 0; p < npmax; ++p) {
       bool run = p < np;
       PrimPair bra, ket;
       if (run) {
         ket = prm.pp[job.pkl_off + kl];
         bra = prm.pp[job.pij_off + ij];
-        // screening (reference src/cint2e.rs:367-393)
-        run = !(ket.cce > prm.expcutoff) && !(bra.cce > prm.expcutoff - ket.cce);
+        if constexpr (MODE == 0) {
+          if (++ij == nbk) {
+            ij = 0;
+            ++kl;
+            if (p + 1 < np) {
+              const double kc = prm.pp[job.pkl_off + kl].cce;
+              while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
+            }
+          }
+        } else {
+          // screening (reference src/cint2e.rs:367-393)
+          run = !(ket.cce > cut) && !(bra.cce > cut - ket.cce);
+          if (++ij == job.nij) { ij = 0; ++kl; }
+        }
       }
-      if (++ij == job.nij) { ij = 0; ++kl; }
       double aij = 1.0, akl = 1.0, a0 = 1.0, fac1 = 0.0, x = 0.0;
       double pq[3] = {0, 0, 0};
       if (run) {
