@@ -210,14 +210,24 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU arms
+def _prefix_molecule(atm, bas, env, nshell):
+    """The first nshell shells of a sweep (one atom per shell, env laid out
+    shell after shell), so the host call does not carry the whole class."""
+    from librint_b200.basis import Molecule
+    b = bas.reshape(-1, 8)[:nshell]
+    a = atm.reshape(-1, 6)[:nshell]
+    end = int(max((b[:, 6] + b[:, 2]).max(), (a[:, 1] + 3).max()))
+    return Molecule(np.ascontiguousarray(a.ravel()), np.ascontiguousarray(b.ravel()),
+                    np.ascontiguousarray(env[:end]))
+
+
 def cpu_sample(data, sample, threads):
     """Oracle on the first `sample` quartets of every class; (quartets/s, s)."""
     import oracle
-    from librint_b200.basis import Molecule
     tot_q, tot_t = 0, 0.0
     for cls, atm, bas, env, shls in data:
-        m = Molecule(atm, bas, env)
         sh = np.ascontiguousarray(shls[:sample])
+        m = _prefix_molecule(atm, bas, env, int(sh.max()) + 1)
         t0 = time.perf_counter()
         oracle.int2e_batch(m, sh, 1, nthreads=threads)
         tot_t += time.perf_counter() - t0

@@ -111,7 +111,7 @@ LRB_API double lrb_fp64_peak_probe(int ms) {
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
-  int iters = 1 << 14;
+  int iters = 1 << 14, timed = iters;
   float t = 0.f;
   k_fp64_probe<<<blocks, threads>>>(sink, iters, 0.999999, 1e-9);   // warm-up
   for (int rep = 0; rep < 8; ++rep) {
@@ -120,6 +120,7 @@ LRB_API double lrb_fp64_peak_probe(int ms) {
     cudaEventRecord(b);
     cudaEventSynchronize(b);
     cudaEventElapsedTime(&t, a, b);
+    timed = iters;          // t belongs to this launch's iteration count
     if (t >= ms) break;
     iters *= 2;
   }
@@ -127,7 +128,7 @@ LRB_API double lrb_fp64_peak_probe(int ms) {
   cudaEventDestroy(b);
   cudaFree(sink);
   if (cudaGetLastError() != cudaSuccess || t <= 0.f) return -1.0;
-  const double flops = 2.0 * 8.0 * (double)iters * threads * blocks;
+  const double flops = 2.0 * 8.0 * (double)timed * threads * blocks;
   return flops / (t * 1e-3) / 1e12;
 }
 

@@ -27,7 +27,7 @@ struct ClassEntry {
 
 template <int LI, int LJ, int LK, int LL>
 ClassEntry make_entry() {
-  using C = EriClass<LI, LJ, LK, LL>;
+  using C = EriClass<LI, LJ, LK, LL, true>;
   ClassEntry e;
   e.fn[0] = k_eri<LI, LJ, LK, LL, 0>;
   e.fn[1] = k_eri<LI, LJ, LK, LL, 1>;

@@ -90,6 +90,13 @@ __host__ __device__ constexpr int binom(int n, int k) {
   return r;
 }
 
+// Component ax (0, 1, 2) of a 3-vector held in registers.  Indexing a local
+// array with a runtime axis would place it on the stack (local memory).
+template <typename T>
+__device__ __forceinline__ T pick3(T x, T y, T z, int ax) {
+  return ax == 0 ? x : (ax == 1 ? y : z);
+}
+
 // ------------------------------------------------------------------ data
 // One primitive pair of a shell pair: exponent sum, Gaussian product centre,
 // coefficient product times exp(-mu R^2) (class prefactor folded into the

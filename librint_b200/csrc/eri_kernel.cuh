@@ -26,7 +26,7 @@ namespace lrb {
 constexpr int ERI_WARPS = 4;                 // warps per CTA
 constexpr int ERI_THREADS = 32 * ERI_WARPS;
 
-template <int LI_, int LJ_, int LK_, int LL_>
+template <int LI_, int LJ_, int LK_, int LL_, bool PACK = false>
 struct EriClass {
   static constexpr int LI = LI_, LJ = LJ_, LK = LK_, LL = LL_;
   static constexpr bool IB = LI > LJ;        // bra base is i (else j)
@@ -40,15 +40,47 @@ struct EriClass {
   static constexpr bool ROWKET = NKET <= NBRA;          // rows are ket components
   static constexpr int NROWS = ROWKET ? NKET : NBRA;
   static constexpr int NCOLS = ROWKET ? NBRA : NKET;
-  static constexpr int LANES = NROWS < 32 ? NROWS : 32;   // lanes per slot
+  // Lanes per slot.  Each of the LANES lanes owns one row; rows beyond LANES
+  // are split by columns over the slot's lanes ("extra" elements).  With
+  // PACK the count is chosen by a cost model of one primitive iteration: a
+  // round of (root, axis) units costs ~350 instruction slots, a row column
+  // ~2.75 per root and an extra element twice that; 18-row classes then run
+  // two 16-lane slots per warp instead of one 18-lane slot.
+  static constexpr double lane_rate(int L) {
+    const int ex = NROWS > L ? ((NROWS - L) * NCOLS + L - 1) / L : 0;
+    const int units = (3 * NR + L - 1) / L;
+    return (32 / L) / (units * 350.0 + NR * (NCOLS + 2.0 * ex) * 2.75);
+  }
+  static constexpr int pick_lanes() {
+    if (NROWS >= 32 || !PACK) return NROWS < 32 ? NROWS : 32;
+    int best = NROWS;
+    double rate = lane_rate(NROWS);
+    // at most 5 extra elements per lane (their offsets live in registers)
+    // and at most 88 KB of slot memory per CTA (with the root table, two CTAs per SM)
+    for (int L = 16; L >= 8; L /= 2)
+      if (L < NROWS && ((NROWS - L) * NCOLS + L - 1) / L <= 5 &&
+          ERI_WARPS * (32 / L) * slot_doubles() * 8 <= 88 * 1024 && lane_rate(L) > 1.05 * rate) {
+        best = L;
+        rate = lane_rate(L);
+      }
+    return best;
+  }
+  static constexpr int LANES = pick_lanes();
   static constexpr int SLOTS = 32 / LANES;
-  static constexpr int EXTRA = NROWS > 32 ? (NROWS - 32) * NCOLS : 0;   // split elements
-  static constexpr int NEX = (EXTRA + 31) / 32;                          // per lane
+  static constexpr int EXTRA = NROWS > LANES ? (NROWS - LANES) * NCOLS : 0;   // split elements
+  static constexpr int NEX = (EXTRA + LANES - 1) / LANES;                      // per lane
   // G[a][b][c][d] sizes; row-side indices first, column side contiguous
   static constexpr int BSZ = (LA + 1) * (LB + 1), KSZ = (LC + 1) * (LD + 1);
   static constexpr int GSZ = BSZ * KSZ;
   static constexpr int CW = ROWKET ? BSZ : KSZ;   // column values per axis
-  static constexpr int TSZ = BSZ * (NCD + 1);     // after the bra shift
+  // after the bra shift; not needed when the ket has no shift (LD == 0)
+  static constexpr int TSZ = LD > 0 ? BSZ * (NCD + 1) : 0;
+  // shared-memory doubles of one slot (loop area or output epilogue)
+  static constexpr int slot_doubles() {
+    const int loop = 2 * NR + 3 * NR * GSZ + 3 * NR * TSZ;
+    const int epi = 2 * NBRA * NKET;
+    return loop > epi ? loop : epi;
+  }
 
   // component c of cartesian function n of momentum l
   static constexpr int cc(int l, int n, int axis) {
@@ -127,8 +159,16 @@ __device__ __forceinline__ void vrr_hrr_unit(R *G, R *T, R v00, R cn, R cm, R b1
 #pragma unroll
     for (int a = 0; a <= LA; ++a)
 #pragma unroll
-      for (int b = 0; b <= LB; ++b) T[(a * (LB + 1) + b) * (NCD + 1) + m] = h[a][b];
+      for (int b = 0; b <= LB; ++b) {
+        if constexpr (LD == 0) {   // no ket shift: m is the ket index c
+          const int bi = a * (LB + 1) + b;
+          G[C::ROWKET ? m * C::BSZ + bi : bi * C::KSZ + m] = h[a][b];
+        } else {
+          T[(a * (LB + 1) + b) * (NCD + 1) + m] = h[a][b];
+        }
+      }
   }
+  if constexpr (LD == 0) return;
   // ket shift per (a, b): k[c][d] from T[a][b][c+d']
 #pragma unroll
   for (int a = 0; a <= LA; ++a)
@@ -239,7 +279,7 @@ __device__ __forceinline__ void cart_comp_rt(int l, int n, int &x, int &y, int &
 template <int LI, int LJ, int LK, int LL, int MODE, typename R = double>
 __global__ void __launch_bounds__(ERI_THREADS)
 k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *counter) {
-  using C = EriClass<LI, LJ, LK, LL>;
+  using C = EriClass<LI, LJ, LK, LL, true>;
   using L = EriLayout<C, MODE>;
   static_assert(MODE == 1 || sizeof(R) == 8, "output mode is FP64");
   extern __shared__ double smem[];
@@ -289,10 +329,10 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
   if constexpr (C::NEX > 0) {
 #pragma unroll
     for (int k = 0; k < C::NEX; ++k) {
-      const int e = lane + 32 * k;
-      xrow[k] = e < C::EXTRA ? 32 + e / C::NCOLS : -1;
+      const int e = rho + C::LANES * k;
+      xrow[k] = e < C::EXTRA ? C::LANES + e / C::NCOLS : -1;
       const int col = e < C::EXTRA ? e % C::NCOLS : 0;
-      const int row = e < C::EXTRA ? 32 + e / C::NCOLS : 0;
+      const int row = e < C::EXTRA ? C::LANES + e / C::NCOLS : 0;
       const int p = C::ROWKET ? C::NK : C::NI;
       const int lp = C::ROWKET ? C::LK : C::LI, lq = C::ROWKET ? C::LL : C::LJ;
       const int cp = C::ROWKET ? C::NI : C::NK;
@@ -429,21 +469,24 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
       }
       __syncwarp();
       if (run) {
-        const double pa[3] = {bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2]};
-        const double qc[3] = {ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2]};
         const double s_ab = aij + akl, p_ab = aij * akl;
         for (int u = rho; u < 3 * C::NR; u += C::LANES) {
           const int r = u / 3, ax = u - 3 * r;
+          const double pa = pick3(bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2], ax);
+          const double qc = pick3(ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2], ax);
+          const double pqa = pick3(pq[0], pq[1], pq[2], ax);
+          const double ab = pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
+          const double cd = pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
           const double u2 = a0 * RW[r];
           const double tmp4 = 0.5 / (u2 * s_ab + p_ab);
           const double tmp5 = u2 * tmp4;
           const double b10 = tmp5 + tmp4 * akl;
           const double b01 = tmp5 + tmp4 * aij;
-          const double cn = pa[ax] - 2.0 * tmp5 * akl * pq[ax];
-          const double cm = qc[ax] + 2.0 * tmp5 * aij * pq[ax];
+          const double cn = pa - 2.0 * tmp5 * akl * pqa;
+          const double cm = qc + 2.0 * tmp5 * aij * pqa;
           const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;
           vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, (R)v00, (R)cn, (R)cm,
-                             (R)b10, (R)b01, (R)tmp5, (R)(rA[ax] - rB[ax]), (R)(rC[ax] - rD[ax]));
+                             (R)b10, (R)b01, (R)tmp5, (R)ab, (R)cd);
         }
       }
       __syncwarp();
@@ -482,7 +525,7 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
 #pragma unroll
         for (int k = 0; k < C::NEX; ++k) {
           if (xrow[k] < 0) continue;
-          const int e = lane + 32 * k, col = e % C::NCOLS;
+          const int e = rho + C::LANES * k, col = e % C::NCOLS;
           Bk[C::ROWKET ? col + C::NBRA * xrow[k] : xrow[k] + C::NBRA * col] = xacc[k];
         }
       }

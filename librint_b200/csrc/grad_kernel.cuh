@@ -247,20 +247,23 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
         }
         __syncwarp();
         if (run) {
-          const double pa[3] = {bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2]};
-          const double qc[3] = {ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2]};
           for (int u = rho; u < 3 * C::NR; u += C::LANES) {
             const int r = u / 3, ax = u - 3 * r;
+            const double pa = pick3(bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2], ax);
+            const double qc = pick3(ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2], ax);
+            const double pqa = pick3(pq[0], pq[1], pq[2], ax);
+            const double ab = pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
+            const double cd = pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
             const double u2 = a0 * RW[r];
             const double tmp4 = 0.5 / (u2 * (aij + akl) + aij * akl);
             const double tmp5 = u2 * tmp4;
             const double b10 = tmp5 + tmp4 * akl;
             const double b01 = tmp5 + tmp4 * aij;
-            const double cn = pa[ax] - 2.0 * tmp5 * akl * pq[ax];
-            const double cm = qc[ax] + 2.0 * tmp5 * aij * pq[ax];
+            const double cn = pa - 2.0 * tmp5 * akl * pqa;
+            const double cm = qc + 2.0 * tmp5 * aij * pqa;
             const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;
             vrr_hrr_unit<C, double>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, v00, cn, cm, b10,
-                                    b01, tmp5, rA[ax] - rB[ax], rC[ax] - rD[ax]);
+                                    b01, tmp5, ab, cd);
           }
         }
         __syncwarp();

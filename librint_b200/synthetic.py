@@ -17,6 +17,8 @@ contraction coefficients are positive and PySCF-normalised
   (``DZP_C``/``DZP_H``: C 3s2p1d, H 2s1p).
 * ``hc_chain``       -- zig-zag C_nH_(2n+2) chain, C-C 1.54 A, C-H 1.09 A,
   +-0.03 A noise, random C 3s2p1d / H 2s1p shells (K uniform in 1..6).
+* ``flake_like``     -- hc_cluster construction with 8..20 carbons, for
+  training the learned guess on flake environments.
 * ``benzene_like``   -- C6H6 ring, bonds +-0.05 A, angles +-3 deg, the
   DZP-like set (or random shells per element from ``basis_seed``).
 """
@@ -223,6 +225,22 @@ def hc_cluster(seed: int = 3, ncarbon: int = 34, aspect: float = 2.0) -> Molecul
     xyz = np.vstack([c3, np.array(hs)])
     z = [6] * len(c3) + [1] * len(hs)
     return _build_ch(z, xyz, rng, "hc_cluster", dzp=True, seed=seed)
+
+
+def flake_like(seed: int) -> Molecule:
+    """A small closed-shell C/H flake for training the learned guess: the
+    hc_cluster construction with 8..20 carbons and aspect 1..2.5 drawn from
+    ``seed`` (carbons added until the electron count is even)."""
+    g = np.random.default_rng([seed, 77])
+    nc = int(g.integers(8, 21))
+    aspect = float(g.uniform(1.0, 2.5))
+    while True:
+        m = hc_cluster(seed=seed, ncarbon=nc, aspect=aspect)
+        if m.nelec % 2 == 0:
+            m.name = "flake_like"
+            m.meta = {"seed": seed, "ncarbon": nc, "aspect": aspect}
+            return m
+        nc += 1
 
 
 def hc_chain(seed: int = 4, ncarbon: int = 6) -> Molecule:

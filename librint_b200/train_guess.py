@@ -5,14 +5,17 @@
 
 Data: seeded C6H6-like rings (``synthetic.benzene_like``: bonds +-0.05 A,
 angles +-3 deg, the even-tempered DZP-like C 3s2p1d / H 2s1p set, 120
-cartesian AOs), geometry seeds 10000 + i.  Each density comes from this library's RHF
+cartesian AOs), geometry seeds 10000 + i; optionally (``--flakes``) small
+C/H flakes of the same lattice construction as the 610-AO cluster
+(``synthetic.flake_like``, seeds 20000 + i), so that the network also sees
+interior carbons.  Each density comes from this library's RHF
 (core-Hamiltonian guess, DIIS, FP64, density change <= conv).  After the
-first ``--bootstrap`` geometries a provisional network is trained and used as
-the starting density for the rest, which only shortens data generation (the
-converged densities do not depend on the start).  The final network is
-trained on the GPU with this library's MLP kernels, then judged on held-out
-geometries by SCF: energies against the core-Hamiltonian start, iterations
-and wall time.
+first ``--bootstrap`` ring geometries a provisional network is trained and
+used as the starting density for the rest, which only shortens data
+generation (the converged densities do not depend on the start).  The final
+network is trained on the GPU with this library's MLP kernels, then judged
+on held-out geometries by SCF: energies against the core-Hamiltonian start,
+iterations and wall time.
 """
 from __future__ import annotations
 
@@ -30,8 +33,12 @@ from .scf import MolContext
 SCF_OPTS = dict(guess=1, diis=8, tau=1e-12, max_iter=100)
 
 
-def geometry(i: int):
-    return synthetic.benzene_like(seed=10000 + i)
+def geometry(i: int, family: str = "rings"):
+    if family == "rings":
+        return synthetic.benzene_like(seed=10000 + i)
+    if family == "flakes":
+        return synthetic.flake_like(20000 + i)
+    raise ValueError(family)
 
 
 def run_scf(m, conv, guess=None):
@@ -45,62 +52,78 @@ def run_scf(m, conv, guess=None):
 
 
 def generate(ids, conv, guess=None, log=print):
+    """ids: list of (family, index); returns densities and (iterations, ms, E)."""
     dens, stats = [], []
-    for n, i in enumerate(ids):
-        m = geometry(i)
+    for n, (fam, i) in enumerate(ids):
+        m = geometry(i, fam)
         r, P = run_scf(m, conv, guess)
         dens.append(P)
         stats.append((r.iterations, r.wall_ms, r.energy))
         if log and (n % 100 == 0):
-            log(f"  scf {n}/{len(ids)}: {r.iterations} it, {r.wall_ms:.0f} ms, E={r.energy:.10f}")
+            log(f"  scf {n}/{len(ids)} ({fam} {i}, {m.nao(0)} AOs): {r.iterations} it, "
+                f"{r.wall_ms:.0f} ms, E={r.energy:.10f}")
     return dens, stats
 
 
 def fit(model, ids, dens, hidden, epochs, batch, lr, seed, log=print):
     g = LearnedGuess(model, hidden=hidden, seed=seed)
-    X, Y, M, T = g.dataset([geometry(i) for i in ids], dens)
+    X, Y, M, T = g.dataset([geometry(i, f) for f, i in ids], dens)
     g.fit_normalisation(X, Y, M, T)
     t = time.perf_counter()
     hist = g.train(X, Y, M, T, epochs=epochs, batch=batch, lr=lr, seed=seed, log=log)
     return g, hist, time.perf_counter() - t, len(X)
 
 
+def evaluate_one(g, m, conv, scf_opts=None):
+    """SCF from the core-Hamiltonian start and from the learned start."""
+    opts = dict(SCF_OPTS, **(scf_opts or {}))
+    ctx = MolContext(m)
+    try:
+        S = ctx.int1e(0)
+        t0 = time.perf_counter()
+        P0 = g.predict(m, S=S)
+        t_pred = (time.perf_counter() - t0) * 1e3
+        rb, Pb = ctx.scf(conv=conv, return_density=True, **opts)
+        rl, _ = ctx.scf(conv=conv, P0=P0, return_density=True, **opts)
+    finally:
+        ctx.close()
+    return dict(nao=m.nao(0), e_core=rb.energy, e_learned=rl.energy,
+                it_core=rb.iterations, it_learned=rl.iterations,
+                ms_core=rb.wall_ms, ms_learned=rl.wall_ms + t_pred, ms_predict=t_pred,
+                guess_err=float(np.abs(P0 - Pb).max()))
+
+
+def summarise(rows):
+    de = np.array([abs(r["e_core"] - r["e_learned"]) for r in rows])
+    mean = lambda k: float(np.mean([r[k] for r in rows]))  # noqa: E731
+    return dict(n=len(rows), max_abs_de=float(de.max()), it_core=mean("it_core"),
+                it_learned=mean("it_learned"), ms_core=mean("ms_core"),
+                ms_learned=mean("ms_learned"), ms_predict=mean("ms_predict"),
+                guess_err=mean("guess_err"))
+
+
 def evaluate(g, ids, conv, log=print):
     rows = []
-    for i in ids:
-        m = geometry(i)
-        ctx = MolContext(m)
-        try:
-            S = ctx.int1e(0)
-            t0 = time.perf_counter()
-            P0 = g.predict(m, S=S)
-            t_pred = (time.perf_counter() - t0) * 1e3
-            rb, Pb = ctx.scf(conv=conv, return_density=True, **SCF_OPTS)
-            rl, Pl = ctx.scf(conv=conv, P0=P0, return_density=True, **SCF_OPTS)
-        finally:
-            ctx.close()
-        rows.append(dict(geometry=10000 + i, e_core=rb.energy, e_learned=rl.energy,
-                         it_core=rb.iterations, it_learned=rl.iterations,
-                         ms_core=rb.wall_ms, ms_learned=rl.wall_ms + t_pred, ms_predict=t_pred,
-                         guess_err=float(np.abs(P0 - Pb).max())))
-    de = np.array([abs(r["e_core"] - r["e_learned"]) for r in rows])
-    out = dict(n=len(rows), max_abs_de=float(de.max()),
-               it_core=float(np.mean([r["it_core"] for r in rows])),
-               it_learned=float(np.mean([r["it_learned"] for r in rows])),
-               ms_core=float(np.mean([r["ms_core"] for r in rows])),
-               ms_learned=float(np.mean([r["ms_learned"] for r in rows])),
-               ms_predict=float(np.mean([r["ms_predict"] for r in rows])),
-               guess_err=float(np.mean([r["guess_err"] for r in rows])))
-    if log:
-        log(f"held-out {out['n']}: iterations {out['it_core']:.2f} -> {out['it_learned']:.2f}, "
-            f"wall {out['ms_core']:.1f} -> {out['ms_learned']:.1f} ms, max |dE| {out['max_abs_de']:.2e}")
+    for fam, i in ids:
+        r = evaluate_one(g, geometry(i, fam), conv)
+        r.update(family=fam, index=i)
+        rows.append(r)
+    out = {}
+    for fam in sorted(set(f for f, _ in ids)):
+        out[fam] = summarise([r for r in rows if r["family"] == fam])
+        if log:
+            s = out[fam]
+            log(f"held-out {fam} {s['n']}: iterations {s['it_core']:.2f} -> {s['it_learned']:.2f}, "
+                f"wall {s['ms_core']:.1f} -> {s['ms_learned']:.1f} ms, max |dE| {s['max_abs_de']:.2e}")
     return out, rows
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--train", type=int, default=2000)
-    ap.add_argument("--test", type=int, default=200)
+    ap.add_argument("--train", type=int, default=2000, help="ring geometries for training")
+    ap.add_argument("--test", type=int, default=200, help="held-out ring geometries")
+    ap.add_argument("--flakes", type=int, default=0, help="flake geometries for training")
+    ap.add_argument("--test-flakes", type=int, default=0, help="held-out flake geometries")
     ap.add_argument("--bootstrap", type=int, default=200)
     ap.add_argument("--conv", type=float, default=1e-8)
     ap.add_argument("--hidden", type=int, nargs="+", default=[256, 256, 256])
@@ -114,38 +137,42 @@ def main(argv=None):
     a = ap.parse_args(argv)
 
     model = PairModel.from_molecule(geometry(0))
-    train_ids = list(range(a.train))
-    test_ids = list(range(a.train, a.train + a.test))
+    train_ids = [("rings", i) for i in range(a.train)] + [("flakes", i) for i in range(a.flakes)]
+    test_ids = [("rings", i) for i in range(a.train, a.train + a.test)] + \
+               [("flakes", i) for i in range(a.flakes, a.flakes + a.test_flakes)]
     t0 = time.perf_counter()
     if a.densities and os.path.exists(a.densities):
-        f = np.load(a.densities)
-        dens = list(f["P"][: a.train])
-        stats = [tuple(v) for v in f["stats"][: a.train]]
+        f = np.load(a.densities, allow_pickle=True)
+        dens = list(f["P"])[: len(train_ids)]
+        stats = [tuple(v) for v in f["stats"][: len(train_ids)]]
         print(f"loaded {len(dens)} densities from {a.densities}")
     else:
         nb = min(a.bootstrap, a.train)
         print(f"generating {nb} densities from the core-Hamiltonian start")
         dens, stats = generate(train_ids[:nb], a.conv)
-        if nb < a.train:
-            g0, _, _, _ = fit(model, train_ids[:nb], dens, a.hidden, max(40, a.epochs // 5),
-                              a.batch, a.lr, a.seed, log=None)
-            print(f"generating {a.train - nb} more from the provisional network")
+        if nb < len(train_ids):
+            g0 = fit(model, train_ids[:nb], dens, a.hidden, max(40, a.epochs // 5),
+                     a.batch, a.lr, a.seed, log=None)[0] if nb > 0 else None
+            print(f"generating {len(train_ids) - nb} more from the provisional network")
             d2, s2 = generate(train_ids[nb:], a.conv, guess=g0)
             dens += d2
             stats += s2
         if a.densities:
-            np.savez_compressed(a.densities, P=np.array(dens), stats=np.array(stats))
+            arr = np.empty(len(dens), dtype=object)
+            arr[:] = dens
+            np.savez_compressed(a.densities, P=arr, stats=np.array(stats))
     t_gen = time.perf_counter() - t0
     g, hist, t_train, nsamp = fit(model, train_ids, dens, a.hidden, a.epochs, a.batch, a.lr, a.seed)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
     g.save(a.out)
     ev, rows = evaluate(g, test_ids, a.conv)
     st = np.array(stats)
-    summary = dict(train=a.train, test=a.test, samples=nsamp, hidden=a.hidden, epochs=a.epochs,
-                   batch=a.batch, lr=a.lr, conv=a.conv, scf_options=SCF_OPTS,
-                   gen_seconds=t_gen, gen_iterations_mean=float(st[:, 0].mean()),
+    summary = dict(train=a.train, flakes=a.flakes, test=a.test, test_flakes=a.test_flakes,
+                   samples=nsamp, hidden=a.hidden, epochs=a.epochs, batch=a.batch, lr=a.lr,
+                   conv=a.conv, scf_options=SCF_OPTS, gen_seconds=t_gen,
+                   gen_iterations_mean=float(st[:, 0].mean()), gen_ms_mean=float(st[:, 1].mean()),
                    train_seconds=t_train, loss_first=hist[0], loss_last=hist[-1],
-                   heldout=ev, heldout_rows=rows[:20])
+                   heldout=ev, heldout_rows=rows[:40])
     if a.summary:
         with open(a.summary, "w") as fh:
             json.dump(summary, fh, indent=1)

@@ -7,7 +7,7 @@ import oracle
 from librint_b200 import eri, synthetic
 from librint_b200 import _bindings as B
 from librint_b200.basis import Molecule
-from tests.conftest import assert_eri_close
+from tests.conftest import assert_eri_close, assert_eri_close_or_exact
 
 pytestmark = pytest.mark.gpu
 
@@ -39,7 +39,8 @@ def test_sweep_batch_vs_oracle(coord):
         m, shls = synthetic.eri_sweep(cls, 400, seed=11)
         got = eri.int2e_batch(m, shls, coord)
         ref = oracle.int2e_batch(m, shls, coord)
-        assert_eri_close(got, ref, what=f"class {cls} coord {coord}")
+        assert_eri_close_or_exact(got, ref, m, shls, coord, lambda sh: eri.int2e_batch(m, sh, 0),
+                                  what=f"class {cls} coord {coord}")
 
 
 def test_permuted_shell_orders_vs_oracle():
