@@ -61,6 +61,23 @@ LRB_API int lrb_int2e_batch_device(double *out, int coord, const int *shls, long
                            const int *atm, int natm, const int *bas, int nbas,
                            const double *env, long long nenv, void *stream);
 
+/* lrb_int2e_batch_device for callers that may not allocate device memory
+ * (a framework whose caching allocator already holds the free memory, or a
+ * latency-bound loop that cannot take cudaMalloc's device synchronisation).
+ * No counterpart in the reference.  All scratch comes from one static device
+ * array of LRB_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
+ * until exit.  Batches over LRB_NOALLOC_MAX_QUARTETS quartets, or whose
+ * quartet tables plus primitive pairs (96 bytes per pair, bra and ket) do not
+ * fit, are rejected with LRB_ERR_INPUT and the sizes in lrb_last_error().
+ * Calls share the array: each clears what must start at zero itself, and
+ * calls whose GPU work overlaps race.  The first call on a device sets up
+ * (symbol lookup, kernel table); make it before any stream capture. */
+#define LRB_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define LRB_NOALLOC_MAX_QUARTETS 65536
+LRB_API int lrb_int2e_batch_device_noalloc(double *out, int coord, const int *shls, long long nq,
+                                           const int *atm, int natm, const int *bas, int nbas,
+                                           const double *env, long long nenv, void *stream);
+
 /* Measurement hooks (no reference counterpart).  While enabled, every ERI
  * class kernel is bracketed by CUDA events on its stream; lrb_profile_read
  * adds the milliseconds per class id (canonical order (ss|ss), (ps|ss),

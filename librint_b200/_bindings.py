@@ -94,6 +94,8 @@ def _optional(L):
         "scf_c": (c_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_sz, c_int, c_d)),
         "lrb_grad_len": (c_int, (c_vp,)),
         "lrb_grad": (c_int, (c_vp, P_d, c_d, c_d, c_d, c_d, P_d)),
+        "lrb_int2e_batch_device_noalloc": (c_int, (c_vp, c_int, c_vp, c_ll, c_vp, c_int, c_vp,
+                                                   c_int, c_vp, c_ll, c_vp)),
         "lrb_mlp_forward": (c_int, (c_vp, c_int, c_int, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
                                     c_vp)),
         "lrb_mlp_backward": (c_int, (c_vp, c_int, c_int, c_vp, c_int, c_int, c_vp, c_vp, c_vp,

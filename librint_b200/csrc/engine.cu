@@ -13,6 +13,7 @@ const char *last_error() { return g_err.c_str(); }
 
 char *Arena::get(cudaStream_t st, size_t need) {
   if (need <= size) return ptr;
+  if (fixed) return nullptr;
   if (ptr) cudaFreeAsync(ptr, st);
   size_t sz = need + need / 4 + (1 << 20);
   void *p = nullptr;

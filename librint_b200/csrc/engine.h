@@ -21,6 +21,7 @@ void set_error(const char *msg);
 struct Arena {
   char *ptr = nullptr;
   size_t size = 0;
+  bool fixed = false;   // caller-provided memory: never freed or grown
   char *get(cudaStream_t st, size_t need);
 };
 
