@@ -242,12 +242,17 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def pick_sample(data, threads, budget_s=8.0):
-    """Sample size per class so one oracle pass takes about budget_s."""
-    probe = 16
-    _, t = cpu_sample(data, probe, threads)
-    s = int(probe * budget_s / max(t, 1e-3))
-    return max(16, min(s, data[0][4].shape[0]))
+def pick_sample(data, threads, budget_s=12.0):
+    """Sample size per class so one oracle pass takes about budget_s (two
+    probes: a small one, then one of about a tenth of the budget)."""
+    nmax = data[0][4].shape[0]
+    s = 64
+    for frac in (None, 0.1):
+        if frac is not None:
+            s = max(64, min(int(s * frac), nmax))
+        _, t = cpu_sample(data, s, threads)
+        s = int(s * budget_s / max(t, 1e-4))
+    return max(64, min(s, nmax))
 
 
 # ------------------------------------------------------------ main
@@ -262,6 +267,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--rhf", type=int, default=0,
                     help="also time RHF on the 60-atom C/H cluster (plain FP64 vs mixed)")
+    ap.add_argument("--guess", default=os.path.join(ROOT, "librint_b200", "data", "guess_ch.npz"),
+                    help="learned-guess network for the --rhf runs")
     ap.add_argument("--classes", default="",
                     help="comma list of classes to run, e.g. 2222,2221 (default: all 21)")
     args = ap.parse_args()
@@ -406,7 +413,7 @@ def main():
                          f"workload ({len(CLASSES) * s} quartets, {tcpu:.1f} s), oracle/ C++ restatement, "
                          f"OpenMP over quartets"}
 
-    rhf = run_rhf() if (args.rhf and rank == 0) else None
+    rhf = run_rhf(args.guess) if (args.rhf and rank == 0) else None
 
     if rank == 0:
         line = {
@@ -445,16 +452,17 @@ def main():
         dist.destroy_process_group()
 
 
-def run_rhf():
-    """RHF wall time on the 60-atom C/H cluster (670 cartesian AOs).
+def run_rhf(guess_file=None):
+    """RHF wall time on the C/H flake (hc_cluster: 34 C + 20 H, 610 cartesian
+    AOs, DZP-like basis).
 
-    plain:  FP64 Fock builds, core-H guess, DIIS(8), Schwarz 1e-13;
-    chosen: incremental Fock builds with FP32 quartets (mixed), same guess,
-            DIIS and screening; its energy is evaluated with a full FP64
-            build at its converged density.
-    Both stop at ||dP||/2 < 1e-6; the reference energy is a plain run to
-    1e-9.  Times exclude the one-off pair table / Schwarz set-up (reported).
-    """
+    reference: FP64, core-H guess, DIIS(8), Schwarz 1e-13, ||dP||/2 <= 1e-8;
+    plain:     the same schedule stopped at 1e-5 (the FP64 GPU path);
+    mixed:     incremental Fock builds with FP32 quartets, same stop;
+    learned:   mixed, started from the learned guess when its network applies
+               to this basis (otherwise absent).
+    Energies are compared with the reference run; times exclude the one-off
+    pair table / Schwarz set-up (reported separately)."""
     import torch
     from librint_b200 import scf as S
     mol = synthetic.hc_cluster()
@@ -462,17 +470,38 @@ def run_rhf():
     ctx = S.MolContext(mol)
     torch.cuda.synchronize()
     setup = time.perf_counter() - t0
-    ref = ctx.scf(conv=1e-9, guess=1, diis=8, tau=1e-13, max_iter=200)
-    out = {"system": "hc_cluster seed 3: 37 C + 23 H, %d cartesian AOs, %d shells" % (ctx.nao, mol.nbas),
-           "setup_s": setup, "E_ref": ref.energy, "ref_iterations": ref.iterations}
-    for name, kw in (("plain", dict(mixed=0)), ("chosen", dict(mixed=1))):
+    base = dict(guess=1, diis=8, tau=1e-13, max_iter=300, check=False)
+
+    def run(name, conv, P0=None, extra_ms=0.0, **kw):
         t0 = time.perf_counter()
-        r = ctx.scf(conv=1e-6, guess=1, diis=8, tau=1e-13, max_iter=200, **kw)
-        dt = time.perf_counter() - t0
-        out[name] = {"wall_s": dt, "energy": r.energy, "dE_vs_ref": r.energy - ref.energy,
-                     "iterations": r.iterations, "fock_ms": r.fock_ms, "quartets": r.quartets,
-                     "fp32_quartets": r.fp32_quartets}
-    out["speedup_chosen_vs_plain"] = out["plain"]["wall_s"] / out["chosen"]["wall_s"]
+        r = ctx.scf(conv=conv, P0=P0, **dict(base, **kw))
+        dt = time.perf_counter() - t0 + extra_ms / 1e3
+        return {"wall_s": dt, "energy": r.energy, "iterations": r.iterations,
+                "converged": bool(r.converged), "delta": r.delta, "fock_ms": r.fock_ms,
+                "quartets": r.quartets, "fp32_quartets": r.fp32_quartets}
+
+    out = {"system": "hc_cluster seed 3: %d cartesian AOs, %d shells, %d electrons"
+                     % (ctx.nao, mol.nbas, mol.nelec), "setup_s": setup}
+    out["reference"] = run("reference", 1e-8)
+    out["plain"] = run("plain", 1e-5)
+    out["mixed"] = run("mixed", 1e-5, mixed=1)
+    if guess_file and os.path.exists(guess_file):
+        from librint_b200.guess import LearnedGuess
+        g = LearnedGuess.load(guess_file)
+        if g.applies(mol):
+            S_ov = ctx.int1e(0)
+            tp = time.perf_counter()
+            P0 = g.predict(mol, S=S_ov)
+            t_pred = (time.perf_counter() - tp) * 1e3
+            out["learned_fp64"] = run("learned_fp64", 1e-5, P0=P0, extra_ms=t_pred)
+            out["learned_mixed"] = run("learned_mixed", 1e-5, P0=P0, extra_ms=t_pred, mixed=1)
+            out["predict_ms"] = t_pred
+    e_ref = out["reference"]["energy"]
+    for k in ("plain", "mixed", "learned_fp64", "learned_mixed"):
+        if k in out:
+            out[k]["dE_vs_reference"] = out[k]["energy"] - e_ref
+            out[k]["speedup_vs_plain"] = out["plain"]["wall_s"] / out[k]["wall_s"]
+    ctx.close()
     return out
 
 

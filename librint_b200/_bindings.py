@@ -24,6 +24,11 @@ class LibrintError(RuntimeError):
     pass
 
 
+# status codes (include/librint_b200.h)
+LRB_OK, LRB_ERR_INPUT, LRB_ERR_UNSUPPORTED, LRB_ERR_ALLOC = 0, -1, -2, -3
+LRB_ERR_CUDA, LRB_ERR_SCF, LRB_ERR_TIMEOUT = -4, -5, -6
+
+
 def lib():
     global _lib
     if _lib is not None:

@@ -152,7 +152,7 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
   for (long long q = 0; q < 4 * nq; ++q)
     if (shls[q] < 0 || shls[q] >= nbas) return set_error("shell index out of range"), LRB_ERR_INPUT;
   // chunk boundaries: at most CHUNK_Q quartets and about CHUNK_OUT doubles each
-  constexpr long long CHUNK_Q = 1 << 16, CHUNK_OUT = 1 << 23;
+  constexpr long long CHUNK_Q = 1 << 17, CHUNK_OUT = 1 << 25;
   std::vector<long long> qb{0}, ob{0};
   {
     long long cq = 0, co = 0, tot = 0;
@@ -180,6 +180,13 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
   }
   DevMol m;
   rc = m.upload(eng.pipe[0], atm, natm, bas, nbas, env, nenv);
+  // shell centres once per call (chunk 0's kernels, and through its event
+  // every later chunk, are ordered after them on stream 0)
+  double *cen = (double *)eng.pipe_centers.get(eng.pipe[0], sizeof(double) * 3 * (size_t)nbas + 256);
+  if (!rc && !cen) rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
+  if (!rc)
+    rc = eri_centers(m.atm, natm, m.bas, nbas, m.env, nenv, cen,
+                     reinterpret_cast<int *>(cen + 3 * (size_t)nbas), eng.pipe[0]);
   const int nchunk = (int)qb.size() - 1;
   for (int c = 0; c < nchunk && !rc; ++c) {
     const int X = c & 1;
@@ -201,7 +208,7 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
       break;
     }
     rc = eri_batch_device(eng, d_o, coord, d_sh, nqc, m.atm, natm, m.bas, nbas, m.env, nenv, st,
-                          nullptr);
+                          nullptr, cen);
     if (rc) break;
     if (cudaEventRecord(eng.done[X], st) != cudaSuccess ||
         cudaMemcpyAsync(out + ob[c], d_o, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost,

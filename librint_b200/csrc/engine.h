@@ -64,7 +64,7 @@ struct Engine {
   // per-stream device buffers that only grow
   cudaStream_t pipe[2] = {nullptr, nullptr};
   cudaEvent_t done[2] = {nullptr, nullptr};
-  Arena pipe_out[2], pipe_in[2];
+  Arena pipe_out[2], pipe_in[2], pipe_centers;
 };
 Engine &engine();          // for the current device
 
@@ -72,9 +72,16 @@ struct EriBatchStats {
   long long nq = 0, out_len = 0, prim_pairs = 0;
 };
 
+// centers_ready: shell centres already computed (and the molecule's indices
+// checked) by eri_centers for this molecule; NULL computes them per call.
 int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, long long nq,
                      const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
-                     long long nenv, cudaStream_t st, EriBatchStats *stats);
+                     long long nenv, cudaStream_t st, EriBatchStats *stats,
+                     const double *centers_ready = nullptr);
+// Shell centres (3 doubles per shell) with every atm/bas/env index checked;
+// d_err is one device int; synchronises st to read it.
+int eri_centers(const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
+                long long nenv, double *centers, int *d_err, cudaStream_t st);
 long long eri_batch_out_len(int coord, const int *shls, long long nq, const int *bas);
 
 }  // namespace lrb

@@ -262,9 +262,24 @@ const double *rys_table_device() {
     }                                                    \
   } while (0)
 
+int eri_centers(const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
+                long long nenv, double *centers, int *d_err, cudaStream_t st) {
+  const int T = 256;
+  int herr = 0;
+  LRB_CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+  k_centers<<<(nbas + T - 1) / T, T, 0, st>>>(d_atm, natm, d_bas, nbas, d_env, nenv, centers, d_err);
+  LRB_CK(cudaGetLastError());
+  ++engine().launches;
+  LRB_CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LRB_CK(cudaStreamSynchronize(st));
+  if (herr) return set_error("atm/bas/env index out of range"), LRB_ERR_INPUT;
+  return LRB_OK;
+}
+
 int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, long long nq,
                      const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
-                     long long nenv, cudaStream_t st, EriBatchStats *stats) {
+                     long long nenv, cudaStream_t st, EriBatchStats *stats,
+                     const double *centers_ready) {
   if (nq <= 0) return LRB_OK;
   if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
   const ClassEntry *tab = class_table();
@@ -288,15 +303,16 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   LRB_CK(cudaMemsetAsync(counters, 0, sizeof(int) * (NCLASS * 2 + 2), st));
 
   const int T = 256;
-  k_centers<<<(nbas + T - 1) / T, T, 0, st>>>(d_atm, natm, d_bas, nbas, d_env, nenv, centers, err);
-  LRB_CK(cudaGetLastError());
-  // a bad shell must not reach the classifier: it reads bas[] of every shell
-  {
+  if (!centers_ready) {
+    k_centers<<<(nbas + T - 1) / T, T, 0, st>>>(d_atm, natm, d_bas, nbas, d_env, nenv, centers, err);
+    LRB_CK(cudaGetLastError());
+    // a bad shell must not reach the classifier: it reads bas[] of every shell
     int herr0 = 0;
     LRB_CK(cudaMemcpyAsync(&herr0, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     LRB_CK(cudaStreamSynchronize(st));
     if (herr0) return set_error("atm/bas/env index out of range"), LRB_ERR_INPUT;
   }
+  const double *cen = centers_ready ? centers_ready : centers;
   k_classify<<<(unsigned)((nq + T - 1) / T), T, 0, st>>>(d_shls, nq, d_bas, nbas, coord, jobs, keys,
                                                          idx, blk, npair, err);
   LRB_CK(cudaGetLastError());
@@ -312,7 +328,7 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   LRB_CK(cub::DeviceScan::ExclusiveSum(tmp, tmp2, npair, pair_off, (int)(2 * nq), st));
   LRB_CK(cub::DeviceRadixSort::SortPairs(tmp, tmp3, keys, keys2, idx, idx2, (int)nq, 0, 32, st));
   k_offsets<<<(unsigned)((nq + T - 1) / T), T, 0, st>>>(jobs, nq, out_off, pair_off);
-  eng.launches += 3;   // k_centers, k_classify, k_offsets
+  eng.launches += centers_ready ? 2 : 3;   // k_centers, k_classify, k_offsets
   // totals and class boundaries back to the host (small copies)
   long long last_blk = 0, last_off = 0;
   int last_np = 0, last_poff = 0, herr = 0;
@@ -348,7 +364,7 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   EriParams prm;
   prm.jobs = jobs;
   prm.pp = pp;
-  prm.centers = centers;
+  prm.centers = cen;
   prm.out = out;
   prm.expcutoff = eng.expcutoff;
   prm.sph = coord;

@@ -430,8 +430,33 @@ def mse(Y, T, Wt, loss, inv_count=None):
 
 
 # -------------------------------------------------------------- the guess
+def lowdin(S):
+    """S^(1/2) and S^(-1/2) of a positive definite overlap matrix."""
+    w, U = np.linalg.eigh(S)
+    return (U * np.sqrt(w)) @ U.T, (U / np.sqrt(w)) @ U.T
+
+
+def density_from_lowdin(Pt, S, nocc):
+    """Closed-shell AO density from an approximate Loewdin density: the N/2
+    largest eigenvectors C of sym(Pt) give S^(-1/2) (2 C C^T) S^(-1/2), which
+    is idempotent in the S metric (P S P = 2 P) with tr(P S) = 2 nocc."""
+    w, V = np.linalg.eigh(0.5 * (Pt + Pt.T))
+    C = V[:, len(w) - nocc:]
+    _, Sih = lowdin(S)
+    return Sih @ (2.0 * C @ C.T) @ Sih
+
+
 class LearnedGuess:
-    """Pair model + network + normalisation; ``predict(m)`` gives P0."""
+    """Pair model + network + normalisation; ``predict(m, S)`` gives P0.
+
+    The network learns blocks of the Loewdin-transformed density
+    P~ = S^(1/2) P S^(1/2) (eigenvalues 0 and 2).  In the raw AO basis the
+    density has large, nearly unobservable components along near-null
+    overlap directions (diffuse shells on neighbouring atoms) that change a
+    lot between nearby geometries; P~ varies about four times less and is
+    what a Fock build actually responds to.  The prediction is projected on
+    the N/2 largest eigenvectors of P~ (an idempotent density with the right
+    electron count) and transformed back with S^(-1/2)."""
 
     def __init__(self, model: PairModel, hidden=(256, 256, 256), seed=0, device="cuda"):
         self.model = model
@@ -448,6 +473,7 @@ class LearnedGuess:
 
     # data ------------------------------------------------------------
     def dataset(self, mols, dens):
+        """Training arrays from molecules and their Loewdin densities P~."""
         X, Y, M, T = [], [], [], []
         for m, P in zip(mols, dens):
             ps = self.model.pairs(m)
@@ -519,15 +545,11 @@ class LearnedGuess:
         y = out.double().cpu().numpy()
         return self.ymu[T] + self.ysd[T] * y
 
-    def predict(self, m: Molecule, S: np.ndarray | None = None, nelec=None):
+    def predict(self, m: Molecule, S: np.ndarray, nelec=None):
+        """P0 in the AO basis from the overlap matrix S of ``m``."""
         ps = self.model.pairs(m)
-        P = self.model.to_density(m, self.predict_local(ps.X, ps.types), ps)
-        if S is not None:
-            ne = m.nelec if nelec is None else nelec
-            tr = float(np.sum(P * S))
-            if tr > 0:
-                P *= ne / tr
-        return P
+        Pt = self.model.to_density(m, self.predict_local(ps.X, ps.types), ps)
+        return density_from_lowdin(Pt, S, (m.nelec if nelec is None else nelec) // 2)
 
     # persistence -----------------------------------------------------
     def save(self, path):

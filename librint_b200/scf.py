@@ -59,11 +59,14 @@ class MolContext:
         return out
 
     def scf(self, nelec=None, max_iter=100, conv=1e-10, guess=0, diis=0, tau=0.0, P0=None,
-            return_density=False, mixed=0, fp32_until=1e-3, tau32=1e-7, rebuild_every=6):
+            return_density=False, mixed=0, fp32_until=1e-3, tau32=1e-7, rebuild_every=6,
+            check=True):
         """RHF.  Defaults are the reference's algorithm (P0 = I, plain
         Roothaan, FP64, no screening); guess=1 / diis / tau / mixed select
         the faster schedules, which change iterations and time, not the
-        converged energy (mixed: within the tolerance stated in the tests)."""
+        converged energy (mixed: within the tolerance stated in the tests).
+        check=False returns a non-converged result (``r.converged`` 0)
+        instead of raising."""
         nelec = self.m.nelec if nelec is None else nelec
         o = B.ScfOptions(max_iter, conv, guess, diis, tau, mixed, fp32_until, tau32, rebuild_every)
         r = B.ScfResult()
@@ -71,7 +74,8 @@ class MolContext:
         p0 = None if P0 is None else np.ascontiguousarray(P0, dtype=np.float64).ctypes.data_as(B.P_d)
         rc = B.lib().lrb_scf(self.h, nelec, ctypes.byref(o), ctypes.byref(r),
                              P.ctypes.data_as(B.P_d), p0)
-        B.check(rc, "lrb_scf")
+        if check or rc != B.LRB_ERR_SCF:
+            B.check(rc, f"lrb_scf ({r.iterations} iterations, delta {r.delta:.3e})")
         return (r, P) if return_density else r
 
     def energy(self, P, tau: float = 0.0):

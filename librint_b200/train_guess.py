@@ -27,7 +27,7 @@ import time
 import numpy as np
 
 from . import synthetic
-from .guess import LearnedGuess, PairModel
+from .guess import LearnedGuess, PairModel, lowdin
 from .scf import MolContext
 
 SCF_OPTS = dict(guess=1, diis=8, tau=1e-12, max_iter=100)
@@ -42,17 +42,21 @@ def geometry(i: int, family: str = "rings"):
 
 
 def run_scf(m, conv, guess=None):
+    """Converged density and its Loewdin transform S^(1/2) P S^(1/2)."""
     ctx = MolContext(m)
     try:
-        P0 = guess.predict(m, S=ctx.int1e(0)) if guess is not None else None
+        S = ctx.int1e(0)
+        P0 = guess.predict(m, S=S) if guess is not None else None
         r, P = ctx.scf(conv=conv, P0=P0, return_density=True, **SCF_OPTS)
     finally:
         ctx.close()
-    return r, P
+    Sh, _ = lowdin(S)
+    return r, Sh @ P @ Sh
 
 
 def generate(ids, conv, guess=None, log=print):
-    """ids: list of (family, index); returns densities and (iterations, ms, E)."""
+    """ids: list of (family, index); returns Loewdin densities and
+    (iterations, ms, E) per geometry."""
     dens, stats = [], []
     for n, (fam, i) in enumerate(ids):
         m = geometry(i, fam)
@@ -87,10 +91,12 @@ def evaluate_one(g, m, conv, scf_opts=None):
         rl, _ = ctx.scf(conv=conv, P0=P0, return_density=True, **opts)
     finally:
         ctx.close()
+    Sh, _ = lowdin(S)
+    # guess error in the Loewdin metric, max |S^1/2 (P0 - P) S^1/2|
     return dict(nao=m.nao(0), e_core=rb.energy, e_learned=rl.energy,
                 it_core=rb.iterations, it_learned=rl.iterations,
                 ms_core=rb.wall_ms, ms_learned=rl.wall_ms + t_pred, ms_predict=t_pred,
-                guess_err=float(np.abs(P0 - Pb).max()))
+                guess_err=float(np.abs(Sh @ (P0 - Pb) @ Sh).max()))
 
 
 def summarise(rows):
@@ -143,7 +149,7 @@ def main(argv=None):
     t0 = time.perf_counter()
     if a.densities and os.path.exists(a.densities):
         f = np.load(a.densities, allow_pickle=True)
-        dens = list(f["P"])[: len(train_ids)]
+        dens = list(f["Pt"])[: len(train_ids)]
         stats = [tuple(v) for v in f["stats"][: len(train_ids)]]
         print(f"loaded {len(dens)} densities from {a.densities}")
     else:
@@ -160,7 +166,7 @@ def main(argv=None):
         if a.densities:
             arr = np.empty(len(dens), dtype=object)
             arr[:] = dens
-            np.savez_compressed(a.densities, P=arr, stats=np.array(stats))
+            np.savez_compressed(a.densities, Pt=arr, stats=np.array(stats))
     t_gen = time.perf_counter() - t0
     g, hist, t_train, nsamp = fit(model, train_ids, dens, a.hidden, a.epochs, a.batch, a.lr, a.seed)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)

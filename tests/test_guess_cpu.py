@@ -128,3 +128,20 @@ def test_adam_oracle_first_step_is_sign_step():
     g = np.array([0.5, -0.1, 0.0])
     q, m, v = mlp_ref.adam_step(p, g, np.zeros(3), np.zeros(3), 0.01, 0.9, 0.999, 1e-8, 1)
     np.testing.assert_allclose(q, p - 0.01 * np.array([1.0, -1.0, 0.0]), atol=1e-6)
+
+
+def test_lowdin_density_round_trip():
+    """A converged density survives S^1/2 P S^1/2 and the projection back,
+    and a perturbed one comes back idempotent with the right trace."""
+    m = synthetic.water_like()
+    P = oracle.density(m, conv=1e-11)[0]
+    S = oracle.int1e(m, 0)
+    Sh, Sih = G.lowdin(S)
+    np.testing.assert_allclose(Sh @ Sih, np.eye(len(S)), atol=1e-12)
+    Pt = Sh @ P @ Sh
+    np.testing.assert_allclose(G.density_from_lowdin(Pt, S, m.nelec // 2), P, atol=1e-9)
+    rng = np.random.default_rng(1)
+    noise = rng.normal(scale=0.05, size=Pt.shape)
+    P0 = G.density_from_lowdin(Pt + noise + noise.T, S, m.nelec // 2)
+    assert abs(np.sum(P0 * S) - m.nelec) < 1e-10
+    np.testing.assert_allclose(P0 @ S @ P0, 2 * P0, atol=1e-10)
