@@ -32,7 +32,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from librint_b200 import synthetic  # noqa: E402
+from librint_b200 import shard, synthetic  # noqa: E402
 
 CLASSES = synthetic.canonical_classes(2)
 METRIC = "ERI shell quartets/s (FP64 Rys sweep, (ss|ss)..(dd|dd), K=1..6, spherical)"
@@ -276,16 +276,14 @@ def main():
     if args.classes:
         CLASSES = [tuple(int(ch) for ch in c.strip()) for c in args.classes.split(",")]
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = shard.world_info()
     threads = host_threads()
 
     if args.impl == "reference":
         return run_reference(args, rank, world, threads)
 
     # inputs generated on the host before any CUDA call (spawn pool)
-    data = generate(args.nq, 2 + 1000 * rank, procs=max(1, threads // max(world, 1)))
+    data = generate(args.nq, shard.shard_seed(2, rank), procs=max(1, threads // max(world, 1)))
 
     import torch
     import torch.distributed as dist
@@ -345,11 +343,7 @@ def main():
     launches = L.lrb_launch_count() - n0
     ms_arr = (__import__("ctypes").c_double * 64)()
     L.lrb_profile_read(ms_arr, 64)
-    elapsed = ev0.elapsed_time(ev1) / 1e3
-    if world > 1:
-        tt = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
+    elapsed = shard.max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dev)
     nq_total = world * len(CLASSES) * args.nq * args.steps
     value = nq_total / elapsed
 
@@ -394,11 +388,7 @@ def main():
         for _ in range(args.e2e_steps):
             e2e_step()
         torch.cuda.synchronize()
-        te = time.perf_counter() - t0
-        if world > 1:
-            tt = torch.tensor([te], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = shard.max_over_ranks(time.perf_counter() - t0, dev)
         e2e = {"value": world * len(CLASSES) * args.nq * args.e2e_steps / te, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "note": "lrb_int2e_batch with pinned host buffers; all %d classes per step"

@@ -134,6 +134,13 @@ LRB_API int lrb_mol_nao(const LrbMol *m);
  * (tau = 0 keeps every quartet the reference keeps).  Host or device. */
 LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long long *quartets);
 LRB_API int lrb_fock_G_device(LrbMol *m, const double *P, double *G, double tau, void *stream);
+/* The same G(P) with the mixed-precision kernels (no reference counterpart):
+ * prec 0 all FP64, 1 all FP32, 2 FP32 only for quartets whose Schwarz x
+ * density bound is below tau32.  FP32 quartets run the recurrences and the
+ * digestion in FP32 (roots and weights FP64) and add into FP64 J/K.  Host
+ * buffers; quartets / fp32_quartets (may be NULL) receive the counts. */
+LRB_API int lrb_fock_G_prec(LrbMol *m, const double *P, double *G, double tau, int prec,
+                            double tau32, long long *quartets, long long *fp32_quartets);
 
 typedef struct {
   int max_iter;       /* reference imax */
@@ -183,6 +190,15 @@ LRB_API double scf_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double 
 LRB_API int lrb_grad_len(const LrbMol *m);
 LRB_API int lrb_grad(LrbMol *m, const double *P, double cH, double cR, double cS, double tau,
                      double *out);
+
+/* RHF gradient with respect to the nuclear coordinates, out[3*atom + axis]
+ * (natm*3 doubles, Hartree/Bohr), at a converged density P (n*n host):
+ *   dE/dR = sum P dH/dR + dR/dR - 1/2 sum (P F P) dS/dR + dE_nuc/dR,
+ * with the nuclear-attraction Hellmann-Feynman term and the ERI centre
+ * derivatives contracted in-kernel (2 a x^(a+1) - a_d x^(a-1) per primitive).
+ * The reference differentiates only exponents and coefficients
+ * (src/utils.rs:152-175); the coordinates are this library's extension. */
+LRB_API int lrb_grad_nuc(LrbMol *m, const double *P, double tau, double *out);
 
 /* src/p2c.rs:240, 267, 294, 321, 348, 376: buffers of lrb_grad_len doubles,
  * release with free_c; NULL on failure. */

@@ -89,6 +89,8 @@ def _optional(L):
         "lrb_mol_nao": (c_int, (c_vp,)),
         "lrb_fock_G": (c_int, (c_vp, P_d, P_d, c_d, ctypes.POINTER(c_ll))),
         "lrb_fock_G_device": (c_int, (c_vp, c_vp, c_vp, c_d, c_vp)),
+        "lrb_fock_G_prec": (c_int, (c_vp, P_d, P_d, c_d, c_int, c_d, ctypes.POINTER(c_ll),
+                                    ctypes.POINTER(c_ll))),
         "lrb_scf": (c_int, (c_vp, c_ll, ctypes.POINTER(ScfOptions), ctypes.POINTER(ScfResult),
                             P_d, P_d)),
         "lrb_energy": (c_int, (c_vp, P_d, c_d, P_d)),
@@ -99,6 +101,7 @@ def _optional(L):
         "scf_c": (c_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, c_sz, c_int, c_d)),
         "lrb_grad_len": (c_int, (c_vp,)),
         "lrb_grad": (c_int, (c_vp, P_d, c_d, c_d, c_d, c_d, P_d)),
+        "lrb_grad_nuc": (c_int, (c_vp, P_d, c_d, P_d)),
         "lrb_int2e_batch_device_noalloc": (c_int, (c_vp, c_int, c_vp, c_ll, c_vp, c_int, c_vp,
                                                    c_int, c_vp, c_ll, c_vp)),
         "lrb_mlp_forward": (c_int, (c_vp, c_int, c_int, c_vp, c_vp, c_int, c_int, c_vp, c_vp,

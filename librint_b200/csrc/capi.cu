@@ -451,6 +451,28 @@ LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long l
   return rc;
 }
 
+LRB_API int lrb_fock_G_prec(LrbMol *m, const double *P, double *G, double tau, int prec,
+                            double tau32, long long *quartets, long long *fp32_quartets) {
+  if (!m || !P || !G) return set_error("NULL argument"), LRB_ERR_INPUT;
+  if (prec < 0 || prec > 2) return set_error("prec must be 0, 1 or 2"), LRB_ERR_INPUT;
+  const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
+  cudaStream_t st = nullptr;
+  double *dP = nullptr, *dG = nullptr;
+  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
+      cudaMallocAsync((void **)&dG, nn * 8, st) != cudaSuccess)
+    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
+  FockStats fs;
+  int rc = fock_build(m->ctx, dP, dG, tau, st, &fs, prec, tau32, false);
+  if (!rc) cudaMemcpyAsync(G, dG, nn * 8, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dP, st);
+  cudaFreeAsync(dG, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
+  if (quartets) *quartets = fs.quartets;
+  if (fp32_quartets) *fp32_quartets = fs.fp32_quartets;
+  return rc;
+}
+
 LRB_API int lrb_scf(LrbMol *m, long long nelec, const LrbScfOptions *opt, LrbScfResult *res,
                     double *P_out, const double *P0) {
   if (!m) return set_error("NULL molecule"), LRB_ERR_INPUT;
@@ -591,6 +613,25 @@ LRB_API int lrb_grad(LrbMol *m, const double *P, double cH, double cR, double cS
   cudaMemsetAsync(dg, 0, glen * 8, st);
   int rc = grad_run(c, dP, cH, cR, cS, tau, dg, s1, st);
   if (!rc) cudaMemcpyAsync(out, dg, sizeof(double) * (size_t)(s2 - s1), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dP, st);
+  cudaFreeAsync(dg, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
+  return rc;
+}
+
+LRB_API int lrb_grad_nuc(LrbMol *m, const double *P, double tau, double *out) {
+  if (!m || !P || !out) return set_error("NULL argument"), LRB_ERR_INPUT;
+  MolCtx &c = m->ctx;
+  const size_t nn = (size_t)c.nao * c.nao, ng = 3 * (size_t)c.natm;
+  cudaStream_t st = nullptr;
+  double *dP = nullptr, *dg = nullptr;
+  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
+      cudaMallocAsync((void **)&dg, ng * 8, st) != cudaSuccess)
+    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(dg, 0, ng * 8, st);
+  int rc = grad_nuc_run(c, dP, tau, dg, st);
+  if (!rc) cudaMemcpyAsync(out, dg, ng * 8, cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(dP, st);
   cudaFreeAsync(dg, st);
   if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);

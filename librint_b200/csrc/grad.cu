@@ -31,18 +31,24 @@ int scf_dense_fock(MolCtx &m, const double *P, double *F, cudaStream_t st);
     }                                             \
   } while (0)
 
-GradEntry g_grad_classes[NGRADCLS][2];
+GradEntry g_grad_classes[NGRADCLS][NGRADMODE];
 
 static void grad_table_init() {
   static bool init = false;
   if (init) return;
-  grad_register_x0(&g_grad_classes[0][0]);
-  grad_register_x1(&g_grad_classes[0][0]);
-  grad_register_x2(&g_grad_classes[0][0]);
+  GradEntry *t = &g_grad_classes[0][0];
+  for (int i = 0; i < NGRADCLS * NGRADMODE; ++i) t[i] = GradEntry{nullptr, 0, 1, 1};
+  grad_register_x0(t);
+  grad_register_x1(t);
+  grad_register_x2(t);
+  grad_register_n0(t);
+  grad_register_n1(t);
+  grad_register_n2(t);
   for (int c = 0; c < NGRADCLS; ++c)
-    for (int r = 0; r < 2; ++r)
-      cudaFuncSetAttribute(g_grad_classes[c][r].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)g_grad_classes[c][r].smem);
+    for (int r = 0; r < NGRADMODE; ++r)
+      if (g_grad_classes[c][r].fn)
+        cudaFuncSetAttribute(g_grad_classes[c][r].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)g_grad_classes[c][r].smem);
   init = true;
 }
 
@@ -131,7 +137,7 @@ __device__ double os1(int ti, int tj, double xpa, double xpb, double oo2p) {
 // contraction coefficients; same conventions as int1e.cu.
 __device__ double prim1e(int op, const int ia[3], const int jb[3], double ai, double bj,
                          const double *A, const double *B, int li, int lj, const int *atm,
-                         int natm, const double *env, const double *rys) {
+                         int natm, const double *env, const double *rys, int cnuc = -1) {
   const double p = ai + bj;
   const double rab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) +
                       (A[2] - B[2]) * (A[2] - B[2]);
@@ -160,7 +166,8 @@ __device__ double prim1e(int op, const int ia[3], const int jb[3], double ai, do
   const int tot = ia[0] + ia[1] + ia[2] + jb[0] + jb[1] + jb[2];
   const int nr = tot / 2 + 1;
   double acc = 0.0;
-  for (int c = 0; c < natm; ++c) {
+  // all nuclei, or only nucleus cnuc
+  for (int c = cnuc < 0 ? 0 : cnuc; c < (cnuc < 0 ? natm : cnuc + 1); ++c) {
     const double *C = env + atm[6 * c + 1];
     const double z = -fabs((double)atm[6 * c]);
     const double x = p * ((P[0] - C[0]) * (P[0] - C[0]) + (P[1] - C[1]) * (P[1] - C[1]) +
@@ -243,7 +250,152 @@ __global__ void k_grad1e(int op, double scale, int n, const int *__restrict__ ao
   }
 }
 
+// Nuclear-coordinate derivative of sum W[mu nu] O[mu nu], one thread per
+// ordered AO pair: the bra function's centre derivative
+//   d/dA_d (x^a e^{-p r^2}) = 2 p x^(a+e_d) e^.. - a_d x^(a-e_d) e^..
+// times 2 (the ket side is the same by symmetry of W and O), added to the
+// bra's atom.  For the nuclear attraction (op 2) each nucleus C also takes
+// the Hellmann-Feynman term, which by translational invariance of the
+// C-term is minus the sum of both basis-centre derivatives.
+__global__ void k_grad1e_nuc(int op, double scale, int n, const int *__restrict__ ao_shell,
+                             const int *__restrict__ ao_comp, const int *__restrict__ atm,
+                             int natm, const int *__restrict__ bas, const double *__restrict__ env,
+                             const double *__restrict__ W, const double *__restrict__ rys,
+                             double *gatom) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int mu = (int)(t / n), nu = (int)(t % n);
+  const double wmn = W[t] * 2.0 * scale;
+  if (wmn == 0.0) return;
+  const int si = ao_shell[mu], sj = ao_shell[nu];
+  const int *bi = bas + 8 * si, *bj = bas + 8 * sj;
+  const int li = bi[1], lj = bj[1];
+  int ia[3], jb[3];
+  cart_of(li, ao_comp[mu], ia[0], ia[1], ia[2]);
+  cart_of(lj, ao_comp[nu], jb[0], jb[1], jb[2]);
+  const double *A = env + atm[6 * bi[0] + 1], *B = env + atm[6 * bj[0] + 1];
+  const int na = op == 2 ? natm : 1;
+  for (int c = 0; c < na; ++c) {
+    const int cn = op == 2 ? c : -1;
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int ip = 0; ip < bi[2]; ++ip) {
+      const double ai = env[bi[5] + ip], cip = env[bi[6] + ip];
+      for (int jp = 0; jp < bj[2]; ++jp) {
+        const double bjx = env[bj[5] + jp], cc = cip * env[bj[6] + jp];
+        for (int d = 0; d < 3; ++d) {
+          int ib[3] = {ia[0], ia[1], ia[2]};
+          ib[d] += 1;
+          double v = 2.0 * ai * prim1e(op, ib, jb, ai, bjx, A, B, li, lj, atm, natm, env, rys, cn);
+          if (ia[d] > 0) {
+            ib[d] -= 2;
+            v -= ia[d] * prim1e(op, ib, jb, ai, bjx, A, B, li, lj, atm, natm, env, rys, cn);
+          }
+          g[d] += cc * v;
+        }
+      }
+    }
+    for (int d = 0; d < 3; ++d) {
+      atomicAdd(&gatom[3 * bi[0] + d], wmn * g[d]);
+      if (op == 2) atomicAdd(&gatom[3 * c + d], -wmn * g[d]);
+    }
+  }
+}
+
+// d/dR of the nuclear repulsion, one thread per atom.
+__global__ void k_grad_nn(const int *__restrict__ atm, int natm, const double *__restrict__ env,
+                          double *gatom) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natm) return;
+  const double *Ra = env + atm[6 * a + 1];
+  const double za = (double)atm[6 * a];
+  double g[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < natm; ++b) {
+    if (b == a) continue;
+    const double *Rb = env + atm[6 * b + 1];
+    const double d[3] = {Ra[0] - Rb[0], Ra[1] - Rb[1], Ra[2] - Rb[2]};
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double f = -za * (double)atm[6 * b] / (r2 * sqrt(r2));
+    for (int k = 0; k < 3; ++k) g[k] += f * d[k];
+  }
+  for (int k = 0; k < 3; ++k) gatom[3 * a + k] += g[k];
+}
+
 }  // namespace
+
+// Adjoint ERI pass over all canonical quartets that survive Schwarz x density
+// screening (density Ps, already scaled), launching mode slots
+// [slot0, slot0 + nslot) of the class table with the parameters in gp.
+static int grad_eri_pass(MolCtx &m, const double *Ps, double tau, int slot0, int nslot,
+                         GradParams gp, cudaStream_t st) {
+  Engine &eng = engine();
+  const int nbas = m.nbas;
+  const double *rys = rys_table_device();
+  const long long ncand = (long long)m.npairs * (m.npairs + 1) / 2;
+  const size_t cap = (size_t)ncand * 4;
+  GradJob *jobs = nullptr;
+  unsigned *keys = nullptr, *keys2 = nullptr;
+  int *idx = nullptr, *idx2 = nullptr, *counters = nullptr;
+  unsigned long long *count = nullptr;
+  long long *starts = nullptr;
+  GR_CK(cudaMallocAsync((void **)&jobs, sizeof(GradJob) * cap, st));
+  GR_CK(cudaMallocAsync((void **)&keys, sizeof(unsigned) * cap, st));
+  GR_CK(cudaMallocAsync((void **)&keys2, sizeof(unsigned) * cap, st));
+  GR_CK(cudaMallocAsync((void **)&idx, sizeof(int) * cap, st));
+  GR_CK(cudaMallocAsync((void **)&idx2, sizeof(int) * cap, st));
+  GR_CK(cudaMallocAsync((void **)&counters, sizeof(int) * NGRADMODE * NGRADCLS, st));
+  GR_CK(cudaMallocAsync((void **)&count, sizeof(unsigned long long), st));
+  GR_CK(cudaMallocAsync((void **)&starts, sizeof(long long) * (NGRADCLS + 1), st));
+  GR_CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
+  GR_CK(cudaMemsetAsync(counters, 0, sizeof(int) * NGRADMODE * NGRADCLS, st));
+  dens_max_device(m, Ps, st);
+  k_grad_jobs<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(m.pairs, m.Q, m.Dsh, m.bas, nbas, ncand,
+                                                               tau, jobs, keys, idx, count, cap);
+  eng.launches += 2;
+  unsigned long long nj = 0;
+  GR_CK(cudaMemcpyAsync(&nj, count, sizeof(nj), cudaMemcpyDeviceToHost, st));
+  GR_CK(cudaStreamSynchronize(st));
+  if (nj > cap) nj = cap;
+  void *tmp = nullptr;
+  if (nj > 0) {
+    size_t tmpb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st);
+    GR_CK(cudaMallocAsync(&tmp, tmpb + 16, st));
+    GR_CK(cub::DeviceRadixSort::SortPairs(tmp, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st));
+    k_grad_starts<<<1, 64, 0, st>>>(keys2, (long long)nj, starts);
+    eng.launches++;
+    long long cb[NGRADCLS + 1];
+    GR_CK(cudaMemcpyAsync(cb, starts, sizeof(cb), cudaMemcpyDeviceToHost, st));
+    GR_CK(cudaStreamSynchronize(st));
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    gp.jobs = jobs;
+    for (int c = 0; c < NGRADCLS; ++c) {
+      if (cb[c + 1] <= cb[c]) continue;
+      gp.order = idx2 + cb[c];
+      gp.njobs = (int)(cb[c + 1] - cb[c]);
+      for (int r = slot0; r < slot0 + nslot; ++r) {
+        const GradEntry &ge = g_grad_classes[c][r];
+        if (!ge.fn) continue;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ge.fn, GRAD_THREADS, ge.smem);
+        if (per_sm < 1) per_sm = 1;
+        const long long tasks = (gp.njobs + ge.slots - 1) / ge.slots;
+        long long grid = (long long)nsm * per_sm;
+        const long long needg = (tasks + GRAD_WARPS - 1) / GRAD_WARPS;
+        if (grid > needg) grid = needg;
+        ge.fn<<<(unsigned)grid, GRAD_THREADS, ge.smem, st>>>(gp, rys + RYS_TAB_OFFSET[ge.nr],
+                                                             counters + NGRADMODE * c + r);
+        GR_CK(cudaGetLastError());
+        eng.launches++;
+      }
+    }
+  }
+  for (void *p : {(void *)jobs, (void *)keys, (void *)keys2, (void *)idx, (void *)idx2,
+                  (void *)counters, (void *)count, (void *)starts, tmp})
+    if (p) cudaFreeAsync(p, st);
+  return LRB_OK;
+}
 
 int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, double tau,
              double *d_grad, int s1, cudaStream_t st) {
@@ -298,83 +450,71 @@ int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, doub
     cublasHandle_t h = grad_blas();
     cublasSetStream(h, st);
     cublasDscal(h, (int)nn, &sc, Ps, 1);
-    const long long ncand = (long long)m.npairs * (m.npairs + 1) / 2;
-    const size_t cap = (size_t)ncand * 4;
-    GradJob *jobs = nullptr;
-    unsigned *keys = nullptr, *keys2 = nullptr;
-    int *idx = nullptr, *idx2 = nullptr, *counters = nullptr;
-    unsigned long long *count = nullptr;
-    long long *starts = nullptr;
-    double *gR = nullptr;
-    GR_CK(cudaMallocAsync((void **)&jobs, sizeof(GradJob) * cap, st));
-    GR_CK(cudaMallocAsync((void **)&keys, sizeof(unsigned) * cap, st));
-    GR_CK(cudaMallocAsync((void **)&keys2, sizeof(unsigned) * cap, st));
-    GR_CK(cudaMallocAsync((void **)&idx, sizeof(int) * cap, st));
-    GR_CK(cudaMallocAsync((void **)&idx2, sizeof(int) * cap, st));
-    GR_CK(cudaMallocAsync((void **)&counters, sizeof(int) * 2 * NGRADCLS, st));
-    GR_CK(cudaMallocAsync((void **)&count, sizeof(unsigned long long), st));
-    GR_CK(cudaMallocAsync((void **)&starts, sizeof(long long) * (NGRADCLS + 1), st));
     const size_t glen = (size_t)(m.nenv - s1);
+    double *gR = nullptr;
     GR_CK(cudaMallocAsync((void **)&gR, sizeof(double) * glen, st));
     GR_CK(cudaMemsetAsync(gR, 0, sizeof(double) * glen, st));
-    GR_CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
-    GR_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 2 * NGRADCLS, st));
-    // density maxima of P for screening
-    dens_max_device(m, Ps, st);
-    k_grad_jobs<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(m.pairs, m.Q, m.Dsh, m.bas, nbas, ncand,
-                                                                 tau, jobs, keys, idx, count, cap);
-    eng.launches += 2;
-    unsigned long long nj = 0;
-    GR_CK(cudaMemcpyAsync(&nj, count, sizeof(nj), cudaMemcpyDeviceToHost, st));
-    GR_CK(cudaStreamSynchronize(st));
-    if (nj > cap) nj = cap;
-    if (nj > 0) {
-      size_t tmpb = 0;
-      cub::DeviceRadixSort::SortPairs(nullptr, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st);
-      void *tmp = nullptr;
-      GR_CK(cudaMallocAsync(&tmp, tmpb + 16, st));
-      GR_CK(cub::DeviceRadixSort::SortPairs(tmp, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st));
-      k_grad_starts<<<1, 64, 0, st>>>(keys2, (long long)nj, starts);
-      eng.launches++;
-      long long cb[NGRADCLS + 1];
-      GR_CK(cudaMemcpyAsync(cb, starts, sizeof(cb), cudaMemcpyDeviceToHost, st));
-      GR_CK(cudaStreamSynchronize(st));
-      int dev = 0, nsm = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      GradParams gp;
-      gp.jobs = jobs; gp.pairs = m.pairs; gp.pp = m.pp; gp.centers = m.centers;
-      gp.bas = m.bas; gp.aooff = m.aooff; gp.env = m.env; gp.P = Ps; gp.n = n;
-      gp.expcutoff = eng.expcutoff; gp.grad = gR; gp.s1 = s1;
-      for (int c = 0; c < NGRADCLS; ++c) {
-        if (cb[c + 1] <= cb[c]) continue;
-        gp.order = idx2 + cb[c];
-        gp.njobs = (int)(cb[c + 1] - cb[c]);
-        for (int r = 0; r < 2; ++r) {
-          const GradEntry &ge = g_grad_classes[c][r];
-          int per_sm = 0;
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ge.fn, GRAD_THREADS, ge.smem);
-          if (per_sm < 1) per_sm = 1;
-          const long long tasks = (gp.njobs + ge.slots - 1) / ge.slots;
-          long long grid = (long long)nsm * per_sm;
-          const long long needg = (tasks + GRAD_WARPS - 1) / GRAD_WARPS;
-          if (grid > needg) grid = needg;
-          ge.fn<<<(unsigned)grid, GRAD_THREADS, ge.smem, st>>>(gp, rys + RYS_TAB_OFFSET[ge.nr],
-                                                               counters + 2 * c + r);
-          GR_CK(cudaGetLastError());
-          eng.launches++;
-        }
-      }
-      cudaFreeAsync(tmp, st);
-    }
+    GradParams gp{};
+    gp.pairs = m.pairs; gp.pp = m.pp; gp.centers = m.centers;
+    gp.bas = m.bas; gp.aooff = m.aooff; gp.env = m.env; gp.P = Ps; gp.n = n;
+    gp.expcutoff = eng.expcutoff; gp.grad = gR; gp.s1 = s1; gp.gatom = nullptr;
+    int rc = grad_eri_pass(m, Ps, tau, 0, 2, gp, st);
+    if (rc) return rc;
     // d_grad += sign(cR) * gR
     const double sg = cR < 0 ? -1.0 : 1.0;
     cublasDaxpy(h, (int)glen, &sg, gR, 1, d_grad, 1);
-    for (void *p : {(void *)jobs, (void *)keys, (void *)keys2, (void *)idx, (void *)idx2,
-                    (void *)counters, (void *)count, (void *)starts, (void *)gR, (void *)Ps})
-      cudaFreeAsync(p, st);
+    cudaFreeAsync(gR, st);
+    cudaFreeAsync(Ps, st);
   }
   cudaFreeAsync(d_map, st);
+  GR_CK(cudaStreamSynchronize(st));
+  GR_CK(cudaGetLastError());
+  return LRB_OK;
+}
+
+int grad_nuc_run(MolCtx &m, const double *d_P, double tau, double *d_gatom, cudaStream_t st) {
+  grad_table_init();
+  Engine &eng = engine();
+  const int n = m.nao, nbas = m.nbas;
+  const long long nn = (long long)n * n;
+  const double *rys = rys_table_device();
+  std::vector<int> ao_shell, ao_comp;
+  for (int s = 0; s < nbas; ++s)
+    for (int c = 0; c < ncart(m.h_bas[8 * s + 1]); ++c) { ao_shell.push_back(s); ao_comp.push_back(c); }
+  int *d_map = nullptr;
+  double *F = nullptr, *Qm = nullptr, *Wk = nullptr;
+  GR_CK(cudaMallocAsync((void **)&d_map, sizeof(int) * 2 * n, st));
+  GR_CK(cudaMemcpyAsync(d_map, ao_shell.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  GR_CK(cudaMemcpyAsync(d_map + n, ao_comp.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  const unsigned gb = (unsigned)((nn + 127) / 128);
+  // dH: kinetic and nuclear attraction (with the Hellmann-Feynman term)
+  k_grad1e_nuc<<<gb, 128, 0, st>>>(1, 1.0, n, d_map, d_map + n, m.atm, m.natm, m.bas, m.env, d_P,
+                                   rys, d_gatom);
+  k_grad1e_nuc<<<gb, 128, 0, st>>>(2, 1.0, n, d_map, d_map + n, m.atm, m.natm, m.bas, m.env, d_P,
+                                   rys, d_gatom);
+  // -1/2 sum (P F P) dS
+  GR_CK(cudaMallocAsync((void **)&F, sizeof(double) * nn, st));
+  GR_CK(cudaMallocAsync((void **)&Qm, sizeof(double) * nn, st));
+  GR_CK(cudaMallocAsync((void **)&Wk, sizeof(double) * nn, st));
+  int rc = scf_dense_fock(m, d_P, F, st);
+  if (rc) return rc;
+  cublasHandle_t h = grad_blas();
+  cublasSetStream(h, st);
+  const double one = 1.0, zero = 0.0;
+  cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, d_P, n, F, n, &zero, Wk, n);
+  cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Wk, n, d_P, n, &zero, Qm, n);
+  k_grad1e_nuc<<<gb, 128, 0, st>>>(0, -0.5, n, d_map, d_map + n, m.atm, m.natm, m.bas, m.env, Qm,
+                                   rys, d_gatom);
+  k_grad_nn<<<(m.natm + 127) / 128, 128, 0, st>>>(m.atm, m.natm, m.env, d_gatom);
+  eng.launches += 4;
+  // dR: centre derivatives of the ERIs contracted with Gamma
+  GradParams gp{};
+  gp.pairs = m.pairs; gp.pp = m.pp; gp.centers = m.centers;
+  gp.bas = m.bas; gp.aooff = m.aooff; gp.env = m.env; gp.P = d_P; gp.n = n;
+  gp.expcutoff = eng.expcutoff; gp.grad = nullptr; gp.s1 = 0; gp.gatom = d_gatom;
+  rc = grad_eri_pass(m, d_P, tau, 2, 2, gp, st);
+  if (rc) return rc;
+  for (void *p : {(void *)F, (void *)Qm, (void *)Wk, (void *)d_map}) cudaFreeAsync(p, st);
   GR_CK(cudaStreamSynchronize(st));
   GR_CK(cudaGetLastError());
   return LRB_OK;

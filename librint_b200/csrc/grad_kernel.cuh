@@ -10,7 +10,12 @@
 // X first, (X Y | Z W), so the derivative always acts on position i:
 //   d/dc_p : primitive p of X only, divided by c_p   (RAISE = 0)
 //   d/da_p : d/da (c x^a e^{-a r^2}) = -c r^2 x^a e^{-a r^2}, i.e. the class
-//            with l_X + 2 contracted with -sum_axis Gamma(a' - 2e_axis) (RAISE = 2).
+//            with l_X + 2 contracted with -sum_axis Gamma(a' - 2e_axis) (MODE 2).
+//   d/dX_d : d/dX_d (x^a e^{-a r^2}) = 2 a_p x^(a+e_d) e^.. - a_d x^(a-e_d) e^..,
+//            the class with l_X + 1 contracted per axis with Gamma(a' - e_d)
+//            and weighted by 2 a_p (MODE 1), and the class with l_X - 1
+//            contracted with -(a'_d + 1) Gamma(a' + e_d) (MODE 3); the three
+//            axis sums go to the atom of X (nuclear-coordinate gradient).
 // Primitives of X are the outer loop, so every primitive gets one reduced
 // scalar; the recurrences and the root handling are those of the energy
 // kernel (vrr_hrr_unit, rys_function).
@@ -41,29 +46,39 @@ struct GradParams {
   const double *P;
   int n;
   double expcutoff;
-  double *grad;     // d/d env[s1 + t]
+  double *grad;     // d/d env[s1 + t] (modes 0, 2)
   int s1;
+  double *gatom;    // d/d atom coordinates, 3 per atom (modes 1, 3)
 };
 
-template <class C>
+// modes: 0 coefficient, 2 exponent, 1 and 3 the raised and lowered parts of
+// the centre derivative; dl is the momentum change of X, nc the axis sums
+__host__ __device__ constexpr int grad_dl(int mode) { return mode == 3 ? -1 : mode; }
+__host__ __device__ constexpr int grad_nc(int mode) { return (mode == 1 || mode == 3) ? 3 : 1; }
+
+template <class C, int NC = 1>
 struct GradLayout {
   static constexpr int LOOP = 2 * C::NR + C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ;
-  static constexpr int GAM = C::NBRA * C::NKET;
-  static constexpr int RED = 32;
+  static constexpr int GAM1 = C::NBRA * C::NKET;   // one Gamma table
+  static constexpr int GAM = NC * GAM1;
+  static constexpr int RED = 32 * NC;
   static constexpr int SLOT = LOOP + GAM + RED;
   static constexpr int WARP = C::SLOTS * SLOT;
   static constexpr int TAB = (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR]);
   static constexpr size_t SMEM = sizeof(double) * (size_t)(TAB + GRAD_WARPS * WARP);
 };
 
-// S += sum_k gam[k] x[col_x(k)] y[col_y(k)] z[col_z(k)]
-template <class C, int K>
-__device__ __forceinline__ void gout_gamma(double &S, const double *gam, const double (&x)[C::CW],
-                                           const double (&y)[C::CW], const double (&z)[C::CW]) {
+// S[c] += sum_k gam[c * stride + k] x[col_x(k)] y[col_y(k)] z[col_z(k)]
+template <class C, int NC, int STRIDE, int K>
+__device__ __forceinline__ void gout_gamma(double (&S)[NC], const double *gam,
+                                           const double (&x)[C::CW], const double (&y)[C::CW],
+                                           const double (&z)[C::CW]) {
   if constexpr (K < C::NCOLS) {
     constexpr int X = C::col_off(K, 0), Y = C::col_off(K, 1), Z = C::col_off(K, 2);
-    S = fma(gam[K], x[X] * y[Y] * z[Z], S);
-    gout_gamma<C, K + 1>(S, gam, x, y, z);
+    const double t = x[X] * y[Y] * z[Z];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) S[c] = fma(gam[c * STRIDE + K], t, S[c]);
+    gout_gamma<C, NC, STRIDE, K + 1>(S, gam, x, y, z);
   }
 }
 
@@ -71,11 +86,12 @@ __device__ __forceinline__ int cart_pos(int x, int y, int z) {
   return (y + z) * (y + z + 1) / 2 + z;
 }
 
-template <int LX, int LY, int LZ, int LW, int RAISE>
+template <int LX, int LY, int LZ, int LW, int MODE>
 __global__ void __launch_bounds__(GRAD_THREADS)
 k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
-  using C = EriClass<LX + RAISE, LY, LZ, LW>;
-  using L = GradLayout<C>;
+  constexpr int NC = grad_nc(MODE);
+  using C = EriClass<LX + grad_dl(MODE), LY, LZ, LW>;
+  using L = GradLayout<C, NC>;
   extern __shared__ double smem[];
   double *tab = smem;
   for (int i = threadIdx.x; i < L::TAB; i += blockDim.x) tab[i] = rys_tab_n[i];
@@ -190,18 +206,25 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
                  P[(long long)a * n + c] * P[(long long)b * n + d] -
                  P[(long long)a * n + d] * P[(long long)b * n + c];
         };
-        double v;
-        if (RAISE == 0) {
-          v = w * gam(ox + ic);
-        } else {
-          v = 0.0;
+        const int bra = ic + C::NI * jc, ket = kc + C::NK * lc;
+        double *g0 = Gam + (C::ROWKET ? ket * C::NBRA + bra : bra * C::NKET + ket);
+        if constexpr (MODE == 0) {
+          g0[0] = w * gam(ox + ic);
+        } else if constexpr (MODE == 2) {
+          double v = 0.0;
           if (ax_ >= 2) v -= gam(ox + cart_pos(ax_ - 2, ay_, az_));
           if (ay_ >= 2) v -= gam(ox + cart_pos(ax_, ay_ - 2, az_));
           if (az_ >= 2) v -= gam(ox + cart_pos(ax_, ay_, az_ - 2));
-          v *= w;
+          g0[0] = w * v;
+        } else if constexpr (MODE == 1) {   // raised: Gamma(a' - e_d)
+          g0[0] = ax_ >= 1 ? w * gam(ox + cart_pos(ax_ - 1, ay_, az_)) : 0.0;
+          g0[L::GAM1] = ay_ >= 1 ? w * gam(ox + cart_pos(ax_, ay_ - 1, az_)) : 0.0;
+          g0[2 * L::GAM1] = az_ >= 1 ? w * gam(ox + cart_pos(ax_, ay_, az_ - 1)) : 0.0;
+        } else {                            // lowered: -(a'_d + 1) Gamma(a' + e_d)
+          g0[0] = -w * (ax_ + 1) * gam(ox + cart_pos(ax_ + 1, ay_, az_));
+          g0[L::GAM1] = -w * (ay_ + 1) * gam(ox + cart_pos(ax_, ay_ + 1, az_));
+          g0[2 * L::GAM1] = -w * (az_ + 1) * gam(ox + cart_pos(ax_, ay_, az_ + 1));
         }
-        const int bra = ic + C::NI * jc, ket = kc + C::NK * lc;
-        Gam[C::ROWKET ? ket * C::NBRA + bra : bra * C::NKET + ket] = v;
       }
     }
     int kxmax = KX;
@@ -223,7 +246,9 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
     __syncwarp();
     const double *gamrow = Gam + (C::ROWKET ? rho * C::NBRA : rho * C::NKET);
     for (int px = 0; px < kxmax; ++px) {
-      double S = 0.0;
+      double S[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) S[c] = 0.0;
       for (int q = 0; q < innermax; ++q) {
         bool run = have && px < KX && q < inner;
         PrimPair bra, ket;
@@ -278,14 +303,16 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
               for (int m = 0; m < C::CW; ++m) {
                 vx[m] = gx[roff[0] + m]; vy[m] = gy[roff[1] + m]; vz[m] = gz[roff[2] + m];
               }
-              gout_gamma<C, 0>(S, gamrow, vx, vy, vz);
+              gout_gamma<C, NC, L::GAM1, 0>(S, gamrow, vx, vy, vz);
             }
             if constexpr (C::NEX > 0) {
 #pragma unroll
               for (int k = 0; k < C::NEX; ++k)
                 if (xrow[k] >= 0) {
-                  const double g = Gam[C::ROWKET ? xrow[k] * C::NBRA + xcol[k] : xrow[k] * C::NKET + xcol[k]];
-                  S = fma(g, gx[xoff[k][0]] * gy[xoff[k][1]] * gz[xoff[k][2]], S);
+                  const double *g = Gam + (C::ROWKET ? xrow[k] * C::NBRA + xcol[k] : xrow[k] * C::NKET + xcol[k]);
+                  const double prod = gx[xoff[k][0]] * gy[xoff[k][1]] * gz[xoff[k][2]];
+#pragma unroll
+                  for (int c = 0; c < NC; ++c) S[c] = fma(g[c * L::GAM1], prod, S[c]);
                 }
             }
           }
@@ -293,28 +320,45 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
         __syncwarp();
       }
       // reduce over the slot's lanes (extra elements live on all 32 lanes)
-      red[rho] = 0.0;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) red[32 * c + rho] = 0.0;
       __syncwarp();
+      double tot[NC];
       if (C::NEX > 0) {
         // one slot per warp when rows exceed 32: plain warp reduction
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) S += __shfl_xor_sync(0xffffffffu, S, o);
-        if (lane == 0 && have && px < KX) {
-          const double c = gp.env[gp.bas[8 * X + 6] + px];
-          const int idx = RAISE ? gp.bas[8 * X + 5] + px : gp.bas[8 * X + 6] + px;
-          const double val = RAISE ? S : (c != 0.0 ? S / c : 0.0);
-          atomicAdd(&gp.grad[idx - gp.s1], val);
+        for (int c = 0; c < NC; ++c) {
+          double v = S[c];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          tot[c] = v;
         }
       } else {
-        if (lane_live) red[rho] = S;
+        if (lane_live) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) red[32 * c + rho] = S[c];
+        }
         __syncwarp();
-        if (have && rho == 0 && px < KX) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
           double t = 0.0;
-          for (int k = 0; k < C::LANES; ++k) t += red[k];
+          for (int k = 0; k < C::LANES; ++k) t += red[32 * c + k];
+          tot[c] = t;
+        }
+      }
+      const bool writer = C::NEX > 0 ? lane == 0 : rho == 0;
+      if (writer && have && px < KX) {
+        if constexpr (MODE == 0 || MODE == 2) {
           const double c = gp.env[gp.bas[8 * X + 6] + px];
-          const int idx = RAISE ? gp.bas[8 * X + 5] + px : gp.bas[8 * X + 6] + px;
-          const double val = RAISE ? t : (c != 0.0 ? t / c : 0.0);
+          const int idx = MODE == 2 ? gp.bas[8 * X + 5] + px : gp.bas[8 * X + 6] + px;
+          const double val = MODE == 2 ? tot[0] : (c != 0.0 ? tot[0] / c : 0.0);
           atomicAdd(&gp.grad[idx - gp.s1], val);
+        } else {
+          // raised part carries 2 a_p of this primitive; lowered part none
+          const double f = MODE == 1 ? 2.0 * gp.env[gp.bas[8 * X + 5] + px] : 1.0;
+          double *g = gp.gatom + 3 * gp.bas[8 * X];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) atomicAdd(&g[c], f * tot[c]);
         }
       }
       __syncwarp();

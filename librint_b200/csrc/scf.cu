@@ -259,7 +259,14 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
   double *Pb = o.mixed ? dv.alloc<double>(nn) : nullptr;
   double *dPm = o.mixed ? dv.alloc<double>(nn) : nullptr;
   if (!dv.ok) return set_error("scf: device allocation failed"), LRB_ERR_ALLOC;
-  int since_full = 1 << 30, phase = -1;   // phase 1: all FP32, 2: split
+  // mixed schedule: phase 1 all FP32 while the density moves by more than
+  // fp32_until (left for good when it stops shrinking), phase 2 FP32 only
+  // for quartets with bound < tau32, phase 0 all FP64 once ||dP||/2 is within
+  // 10 x conv, so the last iterations and the fixed point are those of the
+  // FP64 operator.  A phase change forces a full build and restarts DIIS.
+  int since_full = 1 << 30, phase = -1;
+  bool fp32_done = false, fp64_final = false;
+  double hist[3] = {1e300, 1e300, 1e300};   // delta of the last iterations
   while (delta > o.conv && it < o.max_iter) {
     cudaMemcpyAsync(Pold, P, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
     const auto tf = std::chrono::steady_clock::now();
@@ -267,8 +274,12 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
     if (!o.mixed) {
       if ((rc = fock_build(m, P, G, o.tau, st, &fs))) return rc;
     } else {
-      const int want = delta > o.fp32_until && it > 0 ? 1 : (it == 0 ? 1 : 2);
+      if (it >= 3 && delta > 0.5 * hist[2]) fp32_done = true;   // no progress in two steps
+      if (it > 0 && delta <= o.fp32_until) fp32_done = true;
+      if (fp32_done && delta <= 10.0 * o.conv) fp64_final = true;
+      const int want = !fp32_done ? 1 : (fp64_final ? 0 : 2);
       const bool full = want != phase || since_full >= o.rebuild_every;
+      if (want != phase && phase >= 0) nd = 0;   // DIIS restarts with the new operator
       if (full) {
         if ((rc = fock_build(m, P, Gc, o.tau, st, &fs, want, o.tau32, false))) return rc;
         since_full = 0;
@@ -320,6 +331,9 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
     if ((rc = density_from_fock(Fuse))) return rc;
     k_axpby<<<gb, 256, 0, st>>>(P, Pold, W1, 1.0, -1.0, nn);
     delta = std::sqrt(dot(W1, W1, nn, st, scr)) / 2.0;
+    hist[2] = hist[1];
+    hist[1] = hist[0];
+    hist[0] = delta;
     ++it;
   }
   if (res) {

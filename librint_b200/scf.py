@@ -52,6 +52,18 @@ class MolContext:
         B.check(rc, "lrb_fock_G")
         return G
 
+    def fock_G_prec(self, P, prec: int, tau: float = 0.0, tau32: float = 0.0):
+        """G(P) with the mixed-precision kernels (0 FP64, 1 FP32, 2 FP32 for
+        quartets with Schwarz x density bound below tau32); returns
+        (G, quartets, fp32 quartets)."""
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        G = np.empty_like(P)
+        nq, n32 = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        rc = B.lib().lrb_fock_G_prec(self.h, P.ctypes.data_as(B.P_d), G.ctypes.data_as(B.P_d), tau,
+                                     prec, tau32, ctypes.byref(nq), ctypes.byref(n32))
+        B.check(rc, "lrb_fock_G_prec")
+        return G, nq.value, n32.value
+
     def int1e(self, typec: int, coord: int = 0):
         n = self.m.nao(coord)
         out = np.empty((n, n))

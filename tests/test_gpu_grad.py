@@ -60,3 +60,48 @@ def test_analytical_gradient_vs_scf_differences():
                 conv=1e-11, guess=1, diis=8).energy)
         fd = (es[0] - es[1]) / (2 * h)
         assert abs(fd - g[t - s1]) < 2e-6 * max(1.0, abs(fd)), (t, fd, g[t - s1])
+
+
+def _nuc_case(golden, name):
+    if name == "water_like":
+        return synthetic.water_like()
+    k = f"mol/{name}"
+    atm = golden[f"{k}/atm"]
+    return Molecule(atm, golden[f"{k}/bas"], golden[f"{k}/env"],
+                    int(atm.reshape(-1, 6)[:, 0].sum()))
+
+
+@pytest.mark.parametrize("name", ["water_like", "h2o/def2svp"])
+def test_nuclear_gradient_vs_scf_differences(golden, name):
+    """dE/dR from lrb_grad_nuc against central differences of converged SCF
+    energies (h = 1e-4 Bohr), plus translational invariance."""
+    m = _nuc_case(golden, name)
+    kw = dict(conv=1e-11)
+    _, P = dscf._energy_and_density(m, kw)
+    g = dscf.nuclear_gradient(m, P)
+    assert np.abs(g.sum(axis=0)).max() < 1e-9          # sum over atoms vanishes
+    xyz = dscf.coordinates(m)
+    h = 1e-4
+    for a in range(m.natm):
+        for d in range(3):
+            es = []
+            for sgn in (1.0, -1.0):
+                x2 = xyz.copy()
+                x2[a, d] += sgn * h
+                es.append(dscf._energy_and_density(dscf.with_coordinates(m, x2), kw)[0])
+            fd = (es[0] - es[1]) / (2 * h)
+            assert abs(fd - g[a, d]) < 2e-7, (a, d, fd, g[a, d])
+
+
+def test_rhf_energy_autograd_matches_kernels():
+    """The torch.autograd.Function returns the kernel gradients."""
+    torch = pytest.importorskip("torch")
+    m = synthetic.water_like()
+    xyz = torch.tensor(dscf.coordinates(m), requires_grad=True)
+    s1, s2 = dscf.split(m.bas)
+    theta = torch.tensor(m.env[s1:s2].copy(), requires_grad=True)
+    e = dscf.rhf_energy(m, xyz, theta, dict(conv=1e-11))
+    e.backward()
+    _, P = dscf._energy_and_density(m, dict(conv=1e-11))
+    np.testing.assert_allclose(xyz.grad.numpy(), dscf.nuclear_gradient(m, P), atol=1e-9)
+    np.testing.assert_allclose(theta.grad.numpy(), dscf.danalyticalf(m, P), atol=1e-9)

@@ -104,3 +104,43 @@ def test_scf_failures_in_band(golden):
         *scf._p2c(m)[0], m.nelec, 2, 1e-14))
     with pytest.raises(Exception):
         scf.scf(m, nelec=11)
+
+
+def _ring():
+    return synthetic.benzene_like(seed=10007)
+
+
+@pytest.mark.parametrize("which", ["ring", "h2o/def2svp"])
+def test_fp32_fock_build_error(golden, which):
+    """Mixed-precision G(P) against the FP64 build at a converged density:
+    all-FP32 quartets stay within 2e-6 (absolute, per element) and the split
+    build (FP32 only below the bound tau32) within 1e-8."""
+    m = _ring() if which == "ring" else Molecule(
+        golden["mol/h2o/def2svp/atm"], golden["mol/h2o/def2svp/bas"],
+        golden["mol/h2o/def2svp/env"], 10)
+    ctx = scf.MolContext(m)
+    _, P = ctx.scf(conv=1e-8, guess=1, diis=8, return_density=True)
+    G64, n64, z64 = ctx.fock_G_prec(P, 0)
+    G32, n32, f32 = ctx.fock_G_prec(P, 1)
+    G2, n2, f2 = ctx.fock_G_prec(P, 2, tau32=1e-7)
+    ctx.close()
+    assert z64 == 0 and f32 == n32 and 0 < f2 < n2
+    e32 = np.abs(G32 - G64).max()
+    e2 = np.abs(G2 - G64).max()
+    print(f"{which}: FP32 {e32:.3e}, split {e2:.3e} ({f2} of {n2} quartets FP32)")
+    assert e32 < 2e-6 and e2 < 1e-8
+
+
+@pytest.mark.parametrize("which", ["ring", "h2o/def2svp"])
+def test_mixed_scf_matches_fp64(golden, which):
+    """The mixed schedule ends with FP64 builds, so it converges to the FP64
+    energy (1e-9 Eh) at the same density threshold."""
+    m = _ring() if which == "ring" else Molecule(
+        golden["mol/h2o/def2svp/atm"], golden["mol/h2o/def2svp/bas"],
+        golden["mol/h2o/def2svp/env"], 10)
+    ctx = scf.MolContext(m)
+    r64 = ctx.scf(conv=1e-8, guess=1, diis=8, tau=1e-13)
+    rmx = ctx.scf(conv=1e-8, guess=1, diis=8, tau=1e-13, mixed=1)
+    ctx.close()
+    assert rmx.converged and rmx.fp32_quartets > 0
+    assert abs(rmx.energy - r64.energy) < 1e-9, (rmx.energy, r64.energy)
