@@ -1,7 +1,7 @@
 """Train the learned initial guess on densities the GPU SCF generates.
 
-    python -m librint_b200.train_guess --train 2000 --test 200 \
-        --out librint_b200/data/guess_c6h6.npz --summary guess_summary.json
+    python -m librint_b200.train_guess --train 2000 --test 200 --flakes 100 \
+        --test-flakes 10 --out librint_b200/data/guess_ch.npz --summary summary.json
 
 Data: seeded C6H6-like rings (``synthetic.benzene_like``: bonds +-0.05 A,
 angles +-3 deg, the even-tempered DZP-like C 3s2p1d / H 2s1p set, 120
@@ -137,7 +137,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=2048)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "data", "guess_c6h6.npz"))
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "data", "guess_ch.npz"))
     ap.add_argument("--summary", default=None)
     ap.add_argument("--densities", default=None, help="cache file for the training densities")
     a = ap.parse_args(argv)

@@ -10,7 +10,7 @@ from oracle import mlp_ref
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-GUESS_FILE = os.path.join(os.path.dirname(__file__), "..", "librint_b200", "data", "guess_c6h6.npz")
+GUESS_FILE = os.path.join(os.path.dirname(__file__), "..", "librint_b200", "data", "guess_ch.npz")
 
 
 def _net(sizes, seed=1):
