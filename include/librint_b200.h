@@ -200,6 +200,12 @@ LRB_API int lrb_grad(LrbMol *m, const double *P, double cH, double cR, double cS
  * (src/utils.rs:152-175); the coordinates are this library's extension. */
 LRB_API int lrb_grad_nuc(LrbMol *m, const double *P, double tau, double *out);
 
+/* src/p2c.rs:131 dS_u: overlap Jacobian with respect to env[s1:s2]
+ * (src/dscf.rs:96-151); element (nu * n + mu) * L + l = d S[mu nu] /
+ * d env[s1 + l], n*n*L doubles (n cartesian AOs, L = s2 - s1); free_c. */
+LRB_API double *dS_u(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
+                     size_t env_l);
+
 /* src/p2c.rs:240, 267, 294, 321, 348, 376: buffers of lrb_grad_len doubles,
  * release with free_c; NULL on failure. */
 LRB_API double *grad_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,

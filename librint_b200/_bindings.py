@@ -112,6 +112,7 @@ def _optional(L):
         "lrb_adam": (c_int, (c_vp, c_vp, c_vp, c_vp, c_ll, ctypes.c_float, ctypes.c_float,
                              ctypes.c_float, ctypes.c_float, c_int, c_vp)),
     }
+    sigs["dS_u"] = (P_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz))
     for name in ("grad_c", "dS_c", "dHcore_c", "dR_c", "danalytical_c", "denergy_c"):
         sigs[name] = (P_d, (P_i, c_sz, P_i, c_sz, P_d, c_sz, P_d, c_sz))
     for name, (res, args) in list(sigs.items()):

@@ -657,6 +657,33 @@ static double *grad_p2c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, doub
   return out;
 }
 
+// src/p2c.rs:131 dS_u: overlap Jacobian with respect to env[s1:s2], element
+// (nu * n + mu) * (s2 - s1) + l (src/dscf.rs:96-151); n*n*(s2-s1) doubles.
+double *dS_u(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, size_t env_l) {
+  LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
+  if (!m) return nullptr;
+  int s1, s2;
+  env_split(m->ctx.h_bas.data(), m->ctx.nbas, s1, s2);
+  const size_t len = (size_t)m->ctx.nao * m->ctx.nao * (size_t)(s2 - s1);
+  double *out = (double *)std::malloc(sizeof(double) * std::max<size_t>(len, 1));
+  double *d = nullptr;
+  cudaStream_t st = nullptr;
+  int rc = out ? LRB_OK : (set_error("allocation failed"), LRB_ERR_ALLOC);
+  if (!rc && cudaMallocAsync((void **)&d, sizeof(double) * std::max<size_t>(len, 1), st) != cudaSuccess)
+    rc = (set_error("allocation failed"), LRB_ERR_ALLOC);
+  if (!rc) rc = dS_u_run(m->ctx, s1, s2 - s1, d, st);
+  if (!rc && cudaMemcpyAsync(out, d, sizeof(double) * len, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    rc = (set_error("copy failed"), LRB_ERR_CUDA);
+  if (d) cudaFreeAsync(d, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
+  lrb_mol_destroy(m);
+  if (rc) {
+    std::free(out);
+    return nullptr;
+  }
+  return out;
+}
+
 // src/p2c.rs:240 grad_c = dHcore + dR (src/dscf.rs:547-557)
 double *grad_c(int *a, size_t al, int *b, size_t bl, double *e, size_t el, double *P, size_t Pl) {
   return grad_p2c(a, al, b, bl, e, el, P, Pl, 1.0, 1.0, 0.0);

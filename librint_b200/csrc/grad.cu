@@ -301,6 +301,49 @@ __global__ void k_grad1e_nuc(int op, double scale, int n, const int *__restrict_
   }
 }
 
+// Overlap Jacobian with respect to env[s1:s1+L] (the reference's dS_u,
+// src/dscf.rs:96-151): one thread per AO pair (mu, nu) owns the row
+// out[(nu * n + mu) * L + l] = d S[mu, nu] / d env[s1 + l].  Bra-side
+// parameters are those of mu's shell, ket-side those of nu's (the two add
+// when shells share parameters); coefficients c_p and exponents a_p as in
+// k_grad1e.
+__global__ void k_dS_u(int n, int L, int s1, const int *__restrict__ ao_shell,
+                       const int *__restrict__ ao_comp, const int *__restrict__ atm, int natm,
+                       const int *__restrict__ bas, const double *__restrict__ env,
+                       const double *__restrict__ rys, double *out) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int mu = (int)(t / n), nu = (int)(t % n);
+  double *row = out + ((long long)nu * n + mu) * L;
+  for (int side = 0; side < 2; ++side) {
+    const int a = side == 0 ? mu : nu, b = side == 0 ? nu : mu;   // a carries the parameters
+    const int sa = ao_shell[a], sb = ao_shell[b];
+    const int *ba = bas + 8 * sa, *bb = bas + 8 * sb;
+    int ia[3], jb[3];
+    cart_of(ba[1], ao_comp[a], ia[0], ia[1], ia[2]);
+    cart_of(bb[1], ao_comp[b], jb[0], jb[1], jb[2]);
+    const double *A = env + atm[6 * ba[0] + 1], *B = env + atm[6 * bb[0] + 1];
+    for (int ip = 0; ip < ba[2]; ++ip) {
+      const double ai = env[ba[5] + ip], cip = env[ba[6] + ip];
+      double dcoef = 0.0, dexp = 0.0;
+      for (int jp = 0; jp < bb[2]; ++jp) {
+        const double bj = env[bb[5] + jp], cj = env[bb[6] + jp];
+        dcoef += cj * prim1e(0, ia, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys);
+        double r = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          int ib[3] = {ia[0], ia[1], ia[2]};
+          ib[d] += 2;
+          r += prim1e(0, ib, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys);
+        }
+        dexp -= cip * cj * r;
+      }
+      const int kc = ba[6] + ip - s1, ke = ba[5] + ip - s1;
+      if (kc >= 0 && kc < L) row[kc] += dcoef;
+      if (ke >= 0 && ke < L) row[ke] += dexp;
+    }
+  }
+}
+
 // d/dR of the nuclear repulsion, one thread per atom.
 __global__ void k_grad_nn(const int *__restrict__ atm, int natm, const double *__restrict__ env,
                           double *gatom) {
@@ -468,6 +511,25 @@ int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, doub
   }
   cudaFreeAsync(d_map, st);
   GR_CK(cudaStreamSynchronize(st));
+  GR_CK(cudaGetLastError());
+  return LRB_OK;
+}
+
+int dS_u_run(MolCtx &m, int s1, int L, double *d_out, cudaStream_t st) {
+  const int n = m.nao, nbas = m.nbas;
+  const long long nn = (long long)n * n;
+  std::vector<int> ao_shell, ao_comp;
+  for (int s = 0; s < nbas; ++s)
+    for (int c = 0; c < ncart(m.h_bas[8 * s + 1]); ++c) { ao_shell.push_back(s); ao_comp.push_back(c); }
+  int *d_map = nullptr;
+  GR_CK(cudaMallocAsync((void **)&d_map, sizeof(int) * 2 * n, st));
+  GR_CK(cudaMemcpyAsync(d_map, ao_shell.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  GR_CK(cudaMemcpyAsync(d_map + n, ao_comp.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  GR_CK(cudaMemsetAsync(d_out, 0, sizeof(double) * (size_t)nn * L, st));
+  k_dS_u<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, L, s1, d_map, d_map + n, m.atm, m.natm,
+                                                       m.bas, m.env, rys_table_device(), d_out);
+  engine().launches++;
+  cudaFreeAsync(d_map, st);
   GR_CK(cudaGetLastError());
   return LRB_OK;
 }

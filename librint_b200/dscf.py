@@ -46,6 +46,17 @@ def _call(fname, m: Molecule, P):
     return _take(ptr, s2 - s1)
 
 
+def dSu(m: Molecule) -> np.ndarray:
+    """Overlap Jacobian (s2 - s1, n, n): [l, nu, mu] = d S[mu nu] / d env[s1 + l]
+    (src/p2c.rs:131; the reference's python/librint/dscf.py dSu layout)."""
+    _require_grad_domain(m)
+    from .scf import _p2c, _take
+    args, _keep = _p2c(m)
+    s1, s2 = split(m.bas)
+    n = m.nao(0)
+    return _take(B.lib().dS_u(*args), n * n * (s2 - s1)).reshape(n, n, s2 - s1).transpose(2, 0, 1)
+
+
 def grad(m, P):          # src/p2c.rs:240 -> dH + dR
     return _call("grad_c", m, P)
 

@@ -105,3 +105,17 @@ def test_rhf_energy_autograd_matches_kernels():
     _, P = dscf._energy_and_density(m, dict(conv=1e-11))
     np.testing.assert_allclose(xyz.grad.numpy(), dscf.nuclear_gradient(m, P), atol=1e-9)
     np.testing.assert_allclose(theta.grad.numpy(), dscf.danalyticalf(m, P), atol=1e-9)
+
+
+@pytest.mark.parametrize("key", ["h2", "h2o", "water_like"])
+def test_dsu_vs_reference(key):
+    """dS_u (overlap Jacobian w.r.t. exponents and coefficients) against the
+    reference's shipped dS_u."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_dsu.npz"))
+    m = Molecule(g[f"dsu/{key}/atm"], g[f"dsu/{key}/bas"], g[f"dsu/{key}/env"])
+    n = m.nao(0)
+    s1, s2 = dscf.split(m.bas)
+    want = g[f"dsu/{key}/dS_u"].reshape(n, n, s2 - s1).transpose(2, 0, 1)
+    got = dscf.dSu(m)
+    np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-12 * np.abs(want).max())

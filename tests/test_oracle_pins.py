@@ -123,3 +123,25 @@ def test_rys_tables_vs_exact():
             we = np.array([float(v) for v in we])
             np.testing.assert_allclose(u, ue, rtol=4e-15, err_msg=f"n={n} x={x}")
             np.testing.assert_allclose(w, we, rtol=4e-15, err_msg=f"n={n} x={x}")
+
+
+def test_dsu_golden_layout_vs_oracle_differences():
+    """The reference's dS_u fixture is d S[mu, nu] / d env[s1 + l] at element
+    (nu * n + mu) * L + l: central differences of the oracle's overlap."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_dsu.npz"))
+    for key in ("h2o", "water_like"):
+        m = Molecule(g[f"dsu/{key}/atm"], g[f"dsu/{key}/bas"], g[f"dsu/{key}/env"])
+        b = m.bas.reshape(-1, 8)
+        s1 = int(b[:, 5].min())
+        s2 = int((b[:, 6] + b[:, 2]).max())
+        n, L = m.nao(0), s2 - s1
+        J = g[f"dsu/{key}/dS_u"].reshape(n, n, L)          # [nu, mu, l]
+        h = 1e-6
+        for l in range(0, L, max(1, L // 8)):
+            ep, em = m.env.copy(), m.env.copy()
+            ep[s1 + l] += h
+            em[s1 + l] -= h
+            fd = (oracle.int1e(Molecule(m.atm, m.bas, ep), 0) -
+                  oracle.int1e(Molecule(m.atm, m.bas, em), 0)) / (2 * h)
+            np.testing.assert_allclose(J[:, :, l].T, fd, atol=2e-7 * max(1.0, np.abs(fd).max()))
