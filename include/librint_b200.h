@@ -67,7 +67,7 @@ LRB_API int lrb_int2e_batch_device(double *out, int coord, const int *shls, long
  * No counterpart in the reference.  All scratch comes from one static device
  * array of LRB_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
  * until exit.  Batches over LRB_NOALLOC_MAX_QUARTETS quartets, or whose
- * quartet tables plus primitive pairs (96 bytes per pair, bra and ket) do not
+ * quartet tables plus primitive pairs (128 bytes per pair, bra and ket) do not
  * fit, are rejected with LRB_ERR_INPUT and the sizes in lrb_last_error().
  * Calls share the array: each clears what must start at zero itself, and
  * calls whose GPU work overlaps race.  The first call on a device sets up

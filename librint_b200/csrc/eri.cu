@@ -119,6 +119,8 @@ __global__ void k_pairs(const QuartetJob *__restrict__ jobs, long long nq,
   // 2 pi^3 / sqrt(pi) = 2 pi^2.5 (reference src/g2e.rs:74-82), on the ket side
   if (ket) fac *= 34.986836655249725;
   o.fac = fac;
+  o.ia = inv;
+  o.facia = fac * inv;
   o.cce = eij - log_rr - log(fabs(ci)) - log(fabs(cj));
   pp[t] = o;
 }

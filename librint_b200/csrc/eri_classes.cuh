@@ -34,7 +34,7 @@ ClassEntry make_entry() {
   e.fn[2] = k_eri<LI, LJ, LK, LL, 1, float>;
   e.smem[0] = EriLayout<C, 0>::SMEM;
   e.smem[1] = EriLayout<C, 1>::SMEM;
-  e.smem[2] = EriLayout<C, 1>::SMEM;
+  e.smem[2] = EriLayout<C, 1, float>::SMEM;
   e.slots = C::SLOTS;
   e.nr = C::NR;
   return e;

@@ -103,8 +103,11 @@ __device__ __forceinline__ T pick3(T x, T y, T z, int ax) {
 // ket side by the caller), and libcint's screening key
 // cce = mu R^2 - log_rr - log|c_i| - log|c_j| (reference
 // src/optimizer.rs:732-808).
+// ia = 1/a and facia = fac/a let the kernels form the prefactor
+// sqrt(a0/(a_ij a_kl)^3) fac_ij fac_kl = sqrt(1/(a_ij+a_kl)) facia_ij facia_kl
+// and the recurrence coefficients without divisions.
 struct __align__(16) PrimPair {
-  double a, px, py, pz, fac, cce;
+  double a, ia, px, py, pz, fac, facia, cce;
 };
 
 // One shell quartet of a class launch, canonical order.

@@ -77,7 +77,7 @@ struct EriClass {
   static constexpr int TSZ = LD > 0 ? BSZ * (NCD + 1) : 0;
   // shared-memory doubles of one slot (loop area or output epilogue)
   static constexpr int slot_doubles() {
-    const int loop = 2 * NR + 3 * NR * GSZ + 3 * NR * TSZ;
+    const int loop = 3 * NR + 3 * NR * GSZ + 3 * NR * TSZ;
     const int epi = 2 * NBRA * NKET;
     return loop > epi ? loop : epi;
   }
@@ -101,14 +101,16 @@ struct EriClass {
   }
 };
 
-template <class C, int MODE = 0>
+template <class C, int MODE = 0, typename R = double>
 struct EriLayout {
   static constexpr int NKO_MAX = C::NKET;   // cartesian >= spherical
-  // per-slot doubles: roots (2 NR), G (NR*3*GSZ) and per-unit bra-shift
-  // scratch (3*NR*TSZ) in the loop; block (NBRA*NKET) + ket-transformed
-  // block (NBRA*NKO) in the epilogue
-  static constexpr int LOOP = 2 * C::NR + C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ;
-  static constexpr int EPI = C::NBRA * C::NKET + (MODE == 0 ? C::NBRA * NKO_MAX : 0);
+  // per-slot sizes in doubles: roots, weights, 1/(1+u) (3 NR, FP64), then G
+  // (NR*3*GSZ) and per-unit bra-shift scratch (3*NR*TSZ) in the arithmetic
+  // type R in the loop; block (NBRA*NKET, R) + ket-transformed block
+  // (NBRA*NKO, output mode only) in the epilogue.  FP32 halves the R parts.
+  static constexpr int RD(int n) { return (int)((n * sizeof(R) + 7) / 8); }
+  static constexpr int LOOP = 3 * C::NR + RD(C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ);
+  static constexpr int EPI = RD(C::NBRA * C::NKET) + (MODE == 0 ? C::NBRA * NKO_MAX : 0);
   static constexpr int SLOT = LOOP > EPI ? LOOP : EPI;
   static constexpr int WARP = C::SLOTS * SLOT;
   static constexpr int TAB = (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR]);
@@ -280,7 +282,7 @@ template <int LI, int LJ, int LK, int LL, int MODE, typename R = double>
 __global__ void __launch_bounds__(ERI_THREADS)
 k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *counter) {
   using C = EriClass<LI, LJ, LK, LL, true>;
-  using L = EriLayout<C, MODE>;
+  using L = EriLayout<C, MODE, R>;
   static_assert(MODE == 1 || sizeof(R) == 8, "output mode is FP64");
   extern __shared__ double smem[];
   double *tab = smem;
@@ -299,8 +301,8 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
   const bool lane_live = slot < C::SLOTS;
   const int myslot = lane_live ? slot : C::SLOTS - 1;
   double *sb = wbuf + myslot * L::SLOT;        // this slot's area
-  double *RW = sb;                             // [2*NR] FP64 roots and weights
-  R *G = reinterpret_cast<R *>(sb + 2 * C::NR);            // [NR][3][GSZ]
+  double *RW = sb;                             // [3*NR] FP64 roots, weights, 1/(1+u)
+  R *G = reinterpret_cast<R *>(sb + 3 * C::NR);            // [NR][3][GSZ]
   R *Tsc = G + C::NR * 3 * C::GSZ;                         // [3*NR][TSZ]
 
   // row offsets of this lane (row side indices, per axis)
@@ -456,32 +458,41 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
           if (++ij == job.nij) { ij = 0; ++kl; }
         }
       }
-      double aij = 1.0, akl = 1.0, a0 = 1.0, fac1 = 0.0, x = 0.0;
+      double aij = 1.0, akl = 1.0, inv = 1.0, fac1 = 0.0, x = 0.0;
       double pq[3] = {0, 0, 0};
       if (run) {
         aij = bra.a; akl = ket.a;
-        const double a1 = aij * akl;
-        a0 = a1 / (aij + akl);
-        fac1 = sqrt(a0 / (a1 * a1 * a1)) * bra.fac * ket.fac;
+        inv = 1.0 / (aij + akl);
+        fac1 = sqrt(inv) * bra.facia * ket.facia;
         pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
-        x = a0 * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
-        for (int f = rho; f < 2 * C::NR; f += C::LANES) RW[f] = rys_function<C::NR>(tab, x, f);
+        x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
+        for (int f = rho; f < 2 * C::NR; f += C::LANES) {
+          const double v = rys_function<C::NR>(tab, x, f);
+          RW[f] = v;
+          if (f < C::NR) RW[2 * C::NR + f] = 1.0 / (1.0 + v);   // t^2 complement 1/(1+u)
+        }
       }
       __syncwarp();
       if (run) {
-        const double s_ab = aij + akl, p_ab = aij * akl;
-        for (int u = rho; u < 3 * C::NR; u += C::LANES) {
+        // rounds of (root, axis) units per lane, unrolled so that a lane's
+        // independent units can interleave
+        constexpr int UR = (3 * C::NR + C::LANES - 1) / C::LANES;
+#pragma unroll
+        for (int k = 0; k < UR; ++k) {
+          const int u = rho + k * C::LANES;
+          if (u >= 3 * C::NR) break;
           const int r = u / 3, ax = u - 3 * r;
           const double pa = pick3(bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2], ax);
           const double qc = pick3(ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2], ax);
           const double pqa = pick3(pq[0], pq[1], pq[2], ax);
           const double ab = pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
           const double cd = pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
-          const double u2 = a0 * RW[r];
-          const double tmp4 = 0.5 / (u2 * s_ab + p_ab);
-          const double tmp5 = u2 * tmp4;
-          const double b10 = tmp5 + tmp4 * akl;
-          const double b01 = tmp5 + tmp4 * aij;
+          // with d = 1/(1+u): B00 = u d / (2 (aij+akl)), B10 = B00 + d / (2 aij),
+          // B01 = B00 + d / (2 akl) (u2 (aij+akl) + aij akl = aij akl (1+u))
+          const double d = RW[2 * C::NR + r];
+          const double tmp5 = 0.5 * inv * RW[r] * d;
+          const double b10 = tmp5 + 0.5 * bra.ia * d;
+          const double b01 = tmp5 + 0.5 * ket.ia * d;
           const double cn = pa - 2.0 * tmp5 * akl * pqa;
           const double cm = qc + 2.0 * tmp5 * aij * pqa;
           const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;

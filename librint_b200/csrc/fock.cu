@@ -73,6 +73,8 @@ __global__ void k_mol_pairs(const PairInfo *__restrict__ pairs, int npairs,
   o.py = ri[1] + wj * (rj[1] - ri[1]);
   o.pz = ri[2] + wj * (rj[2] - ri[2]);
   o.fac = ci * cj * exp(-eij) * fac_sp_d(bi[1]) * fac_sp_d(bj[1]) * 5.9149671727956129;
+  o.ia = 1.0 / aij;
+  o.facia = o.fac * o.ia;
   o.cce = eij - log_rr - log(fabs(ci)) - log(fabs(cj));
   pp[t] = o;
 }

@@ -58,7 +58,7 @@ __host__ __device__ constexpr int grad_nc(int mode) { return (mode == 1 || mode 
 
 template <class C, int NC = 1>
 struct GradLayout {
-  static constexpr int LOOP = 2 * C::NR + C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ;
+  static constexpr int LOOP = 3 * C::NR + C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ;
   static constexpr int GAM1 = C::NBRA * C::NKET;   // one Gamma table
   static constexpr int GAM = NC * GAM1;
   static constexpr int RED = 32 * NC;
@@ -104,7 +104,7 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
   const int myslot = lane_live ? slot : C::SLOTS - 1;
   double *sb = wbuf + myslot * L::SLOT;
   double *RW = sb;
-  double *G = sb + 2 * C::NR;
+  double *G = sb + 3 * C::NR;
   double *Tsc = G + C::NR * 3 * C::GSZ;
   double *Gam = sb + L::LOOP;              // [rows][cols]
   double *red = Gam + L::GAM;              // per-lane partial sums
@@ -259,16 +259,19 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
           bra = gp.pp[pbo + ij];
           run = !(ket.cce > gp.expcutoff) && !(bra.cce > gp.expcutoff - ket.cce);
         }
-        double aij = 1.0, akl = 1.0, a0 = 1.0, fac1 = 0.0, x = 0.0;
+        double aij = 1.0, akl = 1.0, inv = 1.0, fac1 = 0.0, x = 0.0;
         double pq[3] = {0, 0, 0};
         if (run) {
           aij = bra.a; akl = ket.a;
-          const double a1 = aij * akl;
-          a0 = a1 / (aij + akl);
-          fac1 = sqrt(a0 / (a1 * a1 * a1)) * bra.fac * ket.fac;
+          inv = 1.0 / (aij + akl);
+          fac1 = sqrt(inv) * bra.facia * ket.facia;
           pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
-          x = a0 * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
-          for (int f = rho; f < 2 * C::NR; f += C::LANES) RW[f] = rys_function<C::NR>(tab, x, f);
+          x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
+          for (int f = rho; f < 2 * C::NR; f += C::LANES) {
+            const double v = rys_function<C::NR>(tab, x, f);
+            RW[f] = v;
+            if (f < C::NR) RW[2 * C::NR + f] = 1.0 / (1.0 + v);   // t^2 complement 1/(1+u)
+          }
         }
         __syncwarp();
         if (run) {
@@ -279,11 +282,10 @@ k_eri_grad(GradParams gp, const double *__restrict__ rys_tab_n, int *counter) {
             const double pqa = pick3(pq[0], pq[1], pq[2], ax);
             const double ab = pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
             const double cd = pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
-            const double u2 = a0 * RW[r];
-            const double tmp4 = 0.5 / (u2 * (aij + akl) + aij * akl);
-            const double tmp5 = u2 * tmp4;
-            const double b10 = tmp5 + tmp4 * akl;
-            const double b01 = tmp5 + tmp4 * aij;
+            const double d = RW[2 * C::NR + r];
+            const double tmp5 = 0.5 * inv * RW[r] * d;
+            const double b10 = tmp5 + 0.5 * bra.ia * d;
+            const double b01 = tmp5 + 0.5 * ket.ia * d;
             const double cn = pa - 2.0 * tmp5 * akl * pqa;
             const double cm = qc + 2.0 * tmp5 * aij * pqa;
             const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;

@@ -42,12 +42,18 @@ def geometry(i: int, family: str = "rings"):
 
 
 def run_scf(m, conv, guess=None):
-    """Converged density and its Loewdin transform S^(1/2) P S^(1/2)."""
+    """Converged density and its Loewdin transform S^(1/2) P S^(1/2).  A
+    start from ``guess`` that does not converge is redone from the
+    core-Hamiltonian start (the data must not depend on the start)."""
     ctx = MolContext(m)
     try:
         S = ctx.int1e(0)
-        P0 = guess.predict(m, S=S) if guess is not None else None
-        r, P = ctx.scf(conv=conv, P0=P0, return_density=True, **SCF_OPTS)
+        r = None
+        if guess is not None:
+            r, P = ctx.scf(conv=conv, P0=guess.predict(m, S=S), return_density=True, check=False,
+                           **SCF_OPTS)
+        if r is None or not r.converged:
+            r, P = ctx.scf(conv=conv, return_density=True, **dict(SCF_OPTS, max_iter=300))
     finally:
         ctx.close()
     Sh, _ = lowdin(S)
@@ -60,7 +66,8 @@ def generate(ids, conv, guess=None, log=print):
     dens, stats = [], []
     for n, (fam, i) in enumerate(ids):
         m = geometry(i, fam)
-        r, P = run_scf(m, conv, guess)
+        # the provisional network has seen rings only
+        r, P = run_scf(m, conv, guess if fam == "rings" else None)
         dens.append(P)
         stats.append((r.iterations, r.wall_ms, r.energy))
         if log and (n % 100 == 0):
@@ -88,21 +95,23 @@ def evaluate_one(g, m, conv, scf_opts=None):
         P0 = g.predict(m, S=S)
         t_pred = (time.perf_counter() - t0) * 1e3
         rb, Pb = ctx.scf(conv=conv, return_density=True, **opts)
-        rl, _ = ctx.scf(conv=conv, P0=P0, return_density=True, **opts)
+        rl, _ = ctx.scf(conv=conv, P0=P0, return_density=True, check=False, **opts)
     finally:
         ctx.close()
     Sh, _ = lowdin(S)
     # guess error in the Loewdin metric, max |S^1/2 (P0 - P) S^1/2|
     return dict(nao=m.nao(0), e_core=rb.energy, e_learned=rl.energy,
+                learned_converged=bool(rl.converged),
                 it_core=rb.iterations, it_learned=rl.iterations,
                 ms_core=rb.wall_ms, ms_learned=rl.wall_ms + t_pred, ms_predict=t_pred,
                 guess_err=float(np.abs(Sh @ (P0 - Pb) @ Sh).max()))
 
 
 def summarise(rows):
-    de = np.array([abs(r["e_core"] - r["e_learned"]) for r in rows])
+    de = np.array([abs(r["e_core"] - r["e_learned"]) for r in rows if r["learned_converged"]])
     mean = lambda k: float(np.mean([r[k] for r in rows]))  # noqa: E731
-    return dict(n=len(rows), max_abs_de=float(de.max()), it_core=mean("it_core"),
+    return dict(n=len(rows), learned_not_converged=sum(not r["learned_converged"] for r in rows),
+                max_abs_de=float(de.max()) if de.size else None, it_core=mean("it_core"),
                 it_learned=mean("it_learned"), ms_core=mean("ms_core"),
                 ms_learned=mean("ms_learned"), ms_predict=mean("ms_predict"),
                 guess_err=mean("guess_err"))
