@@ -200,6 +200,14 @@ LRB_API int lrb_grad(LrbMol *m, const double *P, double cH, double cR, double cS
  * (src/utils.rs:152-175); the coordinates are this library's extension. */
 LRB_API int lrb_grad_nuc(LrbMol *m, const double *P, double tau, double *out);
 
+/* Full Jacobian of a one-electron matrix (typec 0 S, 1 T, 2 V) with respect
+ * to every env entry -- coordinates (including, for V, the nuclei of the
+ * operator), exponents and coefficients: out[(nu*n + mu)*nenv + l] =
+ * d O[mu nu] / d env[l], n*n*nenv doubles (host).  The reference computes the
+ * same Jacobians with Enzyme in its checks (checks/overlap.rs:96-175,
+ * kinetic.rs, nuclear.rs); there is no reference ABI counterpart. */
+LRB_API int lrb_int1e_jacobian(LrbMol *m, int typec, double *out);
+
 /* src/p2c.rs:131 dS_u: overlap Jacobian with respect to env[s1:s2]
  * (src/dscf.rs:96-151); element (nu * n + mu) * L + l = d S[mu nu] /
  * d env[s1 + l], n*n*L doubles (n cartesian AOs, L = s2 - s1); free_c. */

@@ -102,6 +102,7 @@ def _optional(L):
         "lrb_grad_len": (c_int, (c_vp,)),
         "lrb_grad": (c_int, (c_vp, P_d, c_d, c_d, c_d, c_d, P_d)),
         "lrb_grad_nuc": (c_int, (c_vp, P_d, c_d, P_d)),
+        "lrb_int1e_jacobian": (c_int, (c_vp, c_int, P_d)),
         "lrb_int2e_batch_device_noalloc": (c_int, (c_vp, c_int, c_vp, c_ll, c_vp, c_int, c_vp,
                                                    c_int, c_vp, c_ll, c_vp)),
         "lrb_mlp_forward": (c_int, (c_vp, c_int, c_int, c_vp, c_vp, c_int, c_int, c_vp, c_vp,

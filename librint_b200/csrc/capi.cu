@@ -638,6 +638,22 @@ LRB_API int lrb_grad_nuc(LrbMol *m, const double *P, double tau, double *out) {
   return rc;
 }
 
+LRB_API int lrb_int1e_jacobian(LrbMol *m, int typec, double *out) {
+  if (!m || !out) return set_error("NULL argument"), LRB_ERR_INPUT;
+  if (typec < 0 || typec > 2) return set_error("typec must be 0, 1 or 2"), LRB_ERR_INPUT;
+  MolCtx &c = m->ctx;
+  const size_t len = (size_t)c.nao * c.nao * (size_t)c.nenv;
+  cudaStream_t st = nullptr;
+  double *d = nullptr;
+  if (cudaMallocAsync((void **)&d, sizeof(double) * std::max<size_t>(len, 1), st) != cudaSuccess)
+    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  int rc = d1e_env_run(c, typec, d, st);
+  if (!rc) cudaMemcpyAsync(out, d, sizeof(double) * len, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(d, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
+  return rc;
+}
+
 static double *grad_p2c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p,
                         size_t env_l, double *P_p, size_t P_l, double cH, double cR, double cS) {
   LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);

@@ -109,23 +109,65 @@ __global__ void k_dens_max(const double *__restrict__ P, int n, const int *__res
 
 __device__ inline int pair_cls_of(int li, int lj) { return li * (li + 1) / 2 + lj; }
 
-// Screen canonical pair pairs (b >= k) and append survivors.
-// prec: 0 all FP64, 1 all FP32, 2 FP32 when the bound is below tau32.
-// FP32 quartets get class ids offset by NCLASS.
-__global__ void k_screen(const PairInfo *__restrict__ pairs, const int *__restrict__ pcls,
-                         const double *__restrict__ Q, const double *__restrict__ Dsh, int nbas,
-                         long long ncand, int npairs, double tau, int prec, double tau32,
-                         int2 *jobs, unsigned *keys, int *idx, unsigned long long *count,
-                         unsigned long long cap) {
+// Quartet test: Schwarz factors times the largest density element that the
+// quartet's J and K contributions touch.  prec: 0 all FP64, 1 all FP32, 2 FP32
+// when the bound is below tau32; FP32 quartets get class ids offset by NCLASS.
+
+// Largest shell-block density maximum (one block).
+__global__ void k_max_reduce(const double *__restrict__ v, int n, double *out) {
+  __shared__ double sm[1024];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, v[i]);
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sm[0];
+}
+
+// Candidate count per sorted bra position i: ket positions j <= i whose
+// Q_i Q_j 2 Dmax reaches tau (a prefix, as Qs is descending).  2 Dmax bounds
+// the density factor of every quartet, so nothing the full test keeps is lost.
+__global__ void k_cand_count(const double *__restrict__ Qs, int npairs,
+                             const double *__restrict__ dmax, double tau, int *cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npairs) return;
+  const double f = Qs[i] * 2.0 * dmax[0];
+  int c = 0;
+  if (f > 0.0) {
+    const double thr = tau / f;
+    int lo = 0, hi = i + 1;   // first j in [0, i] with Qs[j] < thr
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (Qs[mid] >= thr) lo = mid + 1; else hi = mid;
+    }
+    c = lo;
+  }
+  cnt[i] = c;
+}
+
+// Screen the candidates (sorted positions i >= j) and append survivors; the
+// per-quartet test, precision choice and sort key are those of k_screen.
+__global__ void k_screen_sorted(const PairInfo *__restrict__ pairs, const int *__restrict__ pcls,
+                                const double *__restrict__ Q, const int *__restrict__ qorder,
+                                const long long *__restrict__ qoff, int npairs,
+                                const double *__restrict__ Dsh, int nbas, long long ncand,
+                                double tau, int prec, double tau32, int2 *jobs, unsigned *keys,
+                                int *idx, unsigned long long *count, unsigned long long cap) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   bool keep = false;
   int b = 0, k = 0;
   unsigned key = 0;
   if (t < ncand) {
-    b = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((long long)b * (b + 1) / 2 > t) --b;
-    while ((long long)(b + 1) * (b + 2) / 2 <= t) ++b;
-    k = (int)(t - (long long)b * (b + 1) / 2);
+    int lo = 0, hi = npairs - 1;   // last position i with qoff[i] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (qoff[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    b = qorder[lo];
+    k = qorder[(int)(t - qoff[lo])];
     const PairInfo pb = pairs[b], pk = pairs[k];
     const int I = pb.ish, J = pb.jsh, K = pk.ish, L = pk.jsh;
     const double d = fmax(fmax(2.0 * Dsh[I * nbas + J], 2.0 * Dsh[K * nbas + L]),
@@ -136,7 +178,7 @@ __global__ void k_screen(const PairInfo *__restrict__ pairs, const int *__restri
     if (keep) {
       const bool f32 = prec == 1 || (prec == 2 && bound < tau32);
       int cb = pcls[b], ck = pcls[k];
-      if (cb < ck) {   // bra class must not be below the ket class
+      if (cb < ck) {
         const int tmp = b; b = k; k = tmp;
         const int tc = cb; cb = ck; ck = tc;
       }
@@ -145,7 +187,6 @@ __global__ void k_screen(const PairInfo *__restrict__ pairs, const int *__restri
       key = ((unsigned)cid << 20) | (unsigned)(0xfffff - kprod);
     }
   }
-  // warp-aggregated append
   const unsigned mask = __ballot_sync(0xffffffffu, keep);
   if (!mask) return;
   const int lane = threadIdx.x & 31;
@@ -292,12 +333,30 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
   cudaFreeAsync(d_boff, st);
   cudaFreeAsync(d_blk, st);
   FK_CK(cudaStreamSynchronize(st));
+  // pairs by descending Schwarz factor, for the candidate enumeration
+  {
+    std::vector<double> q(m.npairs);
+    FK_CK(cudaMemcpy(q.data(), m.Q, sizeof(double) * m.npairs, cudaMemcpyDeviceToHost));
+    std::vector<int> ord(m.npairs);
+    for (int p = 0; p < m.npairs; ++p) ord[p] = p;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return q[a] > q[b]; });
+    std::vector<double> qs(m.npairs);
+    for (int p = 0; p < m.npairs; ++p) qs[p] = q[ord[p]];
+    if (!al((void **)&m.qorder, sizeof(int) * m.npairs) || !al((void **)&m.Qs, sizeof(double) * m.npairs) ||
+        !al((void **)&m.qcnt, sizeof(int) * m.npairs) ||
+        !al((void **)&m.qoff, sizeof(long long) * (m.npairs + 1)) || !al((void **)&m.dmax, sizeof(double)))
+      return set_error("molecule: device allocation failed"), LRB_ERR_ALLOC;
+    FK_CK(cudaMemcpyAsync(m.qorder, ord.data(), sizeof(int) * m.npairs, cudaMemcpyHostToDevice, st));
+    FK_CK(cudaMemcpyAsync(m.Qs, qs.data(), sizeof(double) * m.npairs, cudaMemcpyHostToDevice, st));
+    FK_CK(cudaStreamSynchronize(st));
+  }
   return LRB_OK;
 }
 
 void mol_destroy(MolCtx &m, cudaStream_t st) {
   for (void *p : {(void *)m.atm, (void *)m.bas, (void *)m.env, (void *)m.aooff, (void *)m.pairs,
-                  (void *)m.pcls, (void *)m.pp, (void *)m.Q, (void *)m.Dsh, (void *)m.centers})
+                  (void *)m.pcls, (void *)m.pp, (void *)m.Q, (void *)m.Dsh, (void *)m.centers,
+                  (void *)m.qorder, (void *)m.Qs, (void *)m.qcnt, (void *)m.qoff, (void *)m.dmax})
     if (p) cudaFreeAsync(p, st);
   cudaStreamSynchronize(st);
 }
@@ -308,9 +367,31 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
   Engine &eng = engine();
   const ClassEntry *tab = class_table();
   const int n = m.nao, nbas = m.nbas;
-  const long long ncand = (long long)m.npairs * (m.npairs + 1) / 2;
-  // job capacity: all candidates (worst case, no screening)
-  const size_t cap = (size_t)ncand;
+  // candidates: sorted positions i >= j with Q_i Q_j 2 max|D| >= tau
+  k_dens_max<<<(nbas * nbas + 255) / 256, 256, 0, st>>>(dP, n, m.aooff, nbas, m.Dsh);
+  k_max_reduce<<<1, 1024, 0, st>>>(m.Dsh, nbas * nbas, m.dmax);
+  k_cand_count<<<(m.npairs + 255) / 256, 256, 0, st>>>(m.Qs, m.npairs, m.dmax, tau, m.qcnt);
+  eng.launches += 3;
+  {
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, m.qcnt, m.qoff, m.npairs + 1, st);
+    void *tmp = eng.ws.reserve_aux(st, tb + 64);
+    if (!tmp) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
+    // qcnt has npairs entries; the scan of npairs + 1 reads one past it, so
+    // run it on npairs and add the last count on the host
+    FK_CK(cub::DeviceScan::ExclusiveSum(tmp, tb, m.qcnt, m.qoff, m.npairs, st));
+  }
+  long long ncand = 0;
+  {
+    long long lastoff = 0;
+    int lastcnt = 0;
+    FK_CK(cudaMemcpyAsync(&lastoff, m.qoff + m.npairs - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    FK_CK(cudaMemcpyAsync(&lastcnt, m.qcnt + m.npairs - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FK_CK(cudaStreamSynchronize(st));
+    ncand = lastoff + lastcnt;
+  }
+  // job capacity: all candidates (worst case, nothing screened further)
+  const size_t cap = (size_t)std::max(ncand, 1LL);
   const size_t need = carve_size(sizeof(int2) * cap) + 2 * carve_size(sizeof(unsigned) * cap) +
                       2 * carve_size(sizeof(int) * cap) + 2 * carve_size(sizeof(double) * (size_t)n * n) +
                       carve_size(sizeof(long long) * 64) + carve_size(sizeof(unsigned long long)) +
@@ -329,11 +410,12 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
   FK_CK(cudaMemsetAsync(K, 0, sizeof(double) * (size_t)n * n, st));
   FK_CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
   FK_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 64, st));
-  k_dens_max<<<(nbas * nbas + 255) / 256, 256, 0, st>>>(dP, n, m.aooff, nbas, m.Dsh);
-  k_screen<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(m.pairs, m.pcls, m.Q, m.Dsh, nbas, ncand,
-                                                            m.npairs, tau, prec, tau32, jobs, keys,
-                                                            idx, count, cap);
-  eng.launches += 2;
+  if (ncand > 0) {
+    k_screen_sorted<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(
+        m.pairs, m.pcls, m.Q, m.qorder, m.qoff, m.npairs, m.Dsh, nbas, ncand, tau, prec, tau32,
+        jobs, keys, idx, count, cap);
+    ++eng.launches;
+  }
   FK_CK(cudaGetLastError());
   unsigned long long nj = 0;
   long long n32 = 0;

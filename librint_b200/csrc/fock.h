@@ -18,6 +18,11 @@ struct MolCtx {
   double *centers = nullptr;   // 3 doubles per shell
   PairInfo *pairs = nullptr;
   PrimPair *pp = nullptr;
+  // pairs by descending Schwarz factor: qorder[position] = pair, Qs = Q sorted;
+  // per-position candidate counts / offsets and the density maximum of a build
+  int *qorder = nullptr, *qcnt = nullptr;
+  double *Qs = nullptr, *dmax = nullptr;
+  long long *qoff = nullptr;
 };
 
 struct FockStats {

@@ -344,6 +344,81 @@ __global__ void k_dS_u(int n, int L, int s1, const int *__restrict__ ao_shell,
   }
 }
 
+// Full Jacobian of a one-electron matrix (op 0 S, 1 T, 2 V) with respect to
+// every env entry: row (nu * n + mu) holds d O[mu, nu] / d env[l] for all l
+// (the layout of the reference's Enzyme checks, checks/overlap.rs:96-175).
+// Columns: exponents and coefficients of the two shells, the coordinates of
+// the two atoms (centre derivatives 2 a x^(a+e_d) - a_d x^(a-e_d)) and, for
+// V, every nucleus position (Hellmann-Feynman term, minus the two centre
+// derivatives of that nucleus's term).  One thread per AO pair.
+__global__ void k_d1e_env(int op, int n, long long nenv, const int *__restrict__ ao_shell,
+                          const int *__restrict__ ao_comp, const int *__restrict__ atm, int natm,
+                          const int *__restrict__ bas, const double *__restrict__ env,
+                          const double *__restrict__ rys, double *out) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int mu = (int)(t / n), nu = (int)(t % n);
+  double *row = out + ((long long)nu * n + mu) * nenv;
+  for (int side = 0; side < 2; ++side) {
+    const int a = side == 0 ? mu : nu, b = side == 0 ? nu : mu;   // a is differentiated
+    const int sa = ao_shell[a], sb = ao_shell[b];
+    const int *ba = bas + 8 * sa, *bb = bas + 8 * sb;
+    int ia[3], jb[3];
+    cart_of(ba[1], ao_comp[a], ia[0], ia[1], ia[2]);
+    cart_of(bb[1], ao_comp[b], jb[0], jb[1], jb[2]);
+    const double *A = env + atm[6 * ba[0] + 1], *B = env + atm[6 * bb[0] + 1];
+    const int pa = atm[6 * ba[0] + 1];
+    for (int ip = 0; ip < ba[2]; ++ip) {
+      const double ai = env[ba[5] + ip], cip = env[ba[6] + ip];
+      double dcoef = 0.0, dexp = 0.0, dc[3] = {0.0, 0.0, 0.0};
+      for (int jp = 0; jp < bb[2]; ++jp) {
+        const double bj = env[bb[5] + jp], cj = env[bb[6] + jp];
+        dcoef += cj * prim1e(op, ia, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys);
+        double r = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          int ib[3] = {ia[0], ia[1], ia[2]};
+          ib[d] += 2;
+          r += prim1e(op, ib, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys);
+          ib[d] -= 1;
+          double v = 2.0 * ai * prim1e(op, ib, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys);
+          if (ia[d] > 0) {
+            ib[d] -= 2;
+            v -= ia[d] * prim1e(op, ib, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys);
+          }
+          dc[d] += cip * cj * v;
+        }
+        dexp -= cip * cj * r;
+      }
+      row[ba[6] + ip] += dcoef;
+      row[ba[5] + ip] += dexp;
+      for (int d = 0; d < 3; ++d) row[pa + d] += dc[d];
+    }
+    if (op == 2) {
+      for (int c = 0; c < natm; ++c) {
+        double g[3] = {0.0, 0.0, 0.0};
+        for (int ip = 0; ip < ba[2]; ++ip) {
+          const double ai = env[ba[5] + ip], cip = env[ba[6] + ip];
+          for (int jp = 0; jp < bb[2]; ++jp) {
+            const double bj = env[bb[5] + jp], cc = cip * env[bb[6] + jp];
+            for (int d = 0; d < 3; ++d) {
+              int ib[3] = {ia[0], ia[1], ia[2]};
+              ib[d] += 1;
+              double v = 2.0 * ai * prim1e(op, ib, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys, c);
+              if (ia[d] > 0) {
+                ib[d] -= 2;
+                v -= ia[d] * prim1e(op, ib, jb, ai, bj, A, B, ba[1], bb[1], atm, natm, env, rys, c);
+              }
+              g[d] += cc * v;
+            }
+          }
+        }
+        const int pc = atm[6 * c + 1];
+        for (int d = 0; d < 3; ++d) row[pc + d] -= g[d];
+      }
+    }
+  }
+}
+
 // d/dR of the nuclear repulsion, one thread per atom.
 __global__ void k_grad_nn(const int *__restrict__ atm, int natm, const double *__restrict__ env,
                           double *gatom) {
@@ -528,6 +603,26 @@ int dS_u_run(MolCtx &m, int s1, int L, double *d_out, cudaStream_t st) {
   GR_CK(cudaMemsetAsync(d_out, 0, sizeof(double) * (size_t)nn * L, st));
   k_dS_u<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, L, s1, d_map, d_map + n, m.atm, m.natm,
                                                        m.bas, m.env, rys_table_device(), d_out);
+  engine().launches++;
+  cudaFreeAsync(d_map, st);
+  GR_CK(cudaGetLastError());
+  return LRB_OK;
+}
+
+int d1e_env_run(MolCtx &m, int op, double *d_out, cudaStream_t st) {
+  const int n = m.nao, nbas = m.nbas;
+  const long long nn = (long long)n * n;
+  std::vector<int> ao_shell, ao_comp;
+  for (int s = 0; s < nbas; ++s)
+    for (int c = 0; c < ncart(m.h_bas[8 * s + 1]); ++c) { ao_shell.push_back(s); ao_comp.push_back(c); }
+  int *d_map = nullptr;
+  GR_CK(cudaMallocAsync((void **)&d_map, sizeof(int) * 2 * n, st));
+  GR_CK(cudaMemcpyAsync(d_map, ao_shell.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  GR_CK(cudaMemcpyAsync(d_map + n, ao_comp.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  GR_CK(cudaMemsetAsync(d_out, 0, sizeof(double) * (size_t)nn * m.nenv, st));
+  k_d1e_env<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(op, n, m.nenv, d_map, d_map + n, m.atm,
+                                                          m.natm, m.bas, m.env, rys_table_device(),
+                                                          d_out);
   engine().launches++;
   cudaFreeAsync(d_map, st);
   GR_CK(cudaGetLastError());

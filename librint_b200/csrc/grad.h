@@ -48,6 +48,8 @@ int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, doub
 // d_gatom[3 * atom + axis] += d/dR of the RHF energy at the converged
 // density d_P: dH + dR - (1/2) sum (P F P) dS + d E_nuc (all on the device).
 int grad_nuc_run(MolCtx &m, const double *d_P, double tau, double *d_gatom, cudaStream_t st);
+// Full env Jacobian of S (op 0), T (1) or V (2): d_out[(nu n + mu) nenv + l].
+int d1e_env_run(MolCtx &m, int op, double *d_out, cudaStream_t st);
 // Overlap Jacobian d S[mu nu] / d env[s1 + l] into d_out[(nu n + mu) L + l].
 int dS_u_run(MolCtx &m, int s1, int L, double *d_out, cudaStream_t st);
 

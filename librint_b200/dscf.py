@@ -101,6 +101,21 @@ def nuclear_gradient(m: Molecule, P, tau: float = 0.0) -> np.ndarray:
     return out.reshape(m.natm, 3)
 
 
+def int1e_jacobian(m: Molecule, typec: int) -> np.ndarray:
+    """(n*n, nenv) Jacobian of S (0), T (1) or V (2) with respect to all of
+    env; row nu*n + mu, the layout of the reference's Enzyme checks."""
+    from .scf import MolContext
+    ctx = MolContext(m)
+    try:
+        n = ctx.nao
+        out = np.empty(n * n * m.env.size)
+        B.check(B.lib().lrb_int1e_jacobian(ctx.h, typec, out.ctypes.data_as(B.P_d)),
+                "lrb_int1e_jacobian")
+    finally:
+        ctx.close()
+    return out.reshape(n * n, m.env.size)
+
+
 def with_coordinates(m: Molecule, xyz) -> Molecule:
     """Copy of m with the atoms at xyz (natm, 3) Bohr."""
     env = np.array(m.env, dtype=np.float64)

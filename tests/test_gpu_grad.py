@@ -119,3 +119,16 @@ def test_dsu_vs_reference(key):
     want = g[f"dsu/{key}/dS_u"].reshape(n, n, s2 - s1).transpose(2, 0, 1)
     got = dscf.dSu(m)
     np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("key", ["h2", "h2o"])
+@pytest.mark.parametrize("op,typec", [("dS", 0), ("dT", 1), ("dV", 2)])
+def test_int1e_jacobian_vs_reference_truth(key, op, typec):
+    """d{S,T,V}/d env over every entry (coordinates, nuclear positions,
+    exponents, coefficients) against the reference's Enzyme truths, with
+    the reference checks' own absolute tolerance 1e-12."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_truth.npz"))
+    m = Molecule(g[f"truth/{key}/atm"], g[f"truth/{key}/bas"], g[f"truth/{key}/env"])
+    got = dscf.int1e_jacobian(m, typec)
+    np.testing.assert_allclose(got, g[f"truth/{key}/{op}"], rtol=0, atol=1e-12)

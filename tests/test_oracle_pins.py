@@ -145,3 +145,23 @@ def test_dsu_golden_layout_vs_oracle_differences():
             fd = (oracle.int1e(Molecule(m.atm, m.bas, ep), 0) -
                   oracle.int1e(Molecule(m.atm, m.bas, em), 0)) / (2 * h)
             np.testing.assert_allclose(J[:, :, l].T, fd, atol=2e-7 * max(1.0, np.abs(fd).max()))
+
+
+@pytest.mark.parametrize("op,typec", [("dS", 0), ("dT", 1), ("dV", 2)])
+def test_truth_jacobians_vs_oracle_differences(op, typec):
+    """The reference's Enzyme truths d{S,T,V}/d env (coordinates, exponents,
+    coefficients) against central differences of the oracle's matrices."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_truth.npz"))
+    m = Molecule(g["truth/h2o/atm"], g["truth/h2o/bas"], g["truth/h2o/env"])
+    J = g[f"truth/h2o/{op}"]                               # (n*n, len(env)), row nu*n + mu
+    h = 1e-6
+    cols = [l for l in range(m.env.size) if np.abs(J[:, l]).max() > 0]
+    for l in cols[:: max(1, len(cols) // 10)]:
+        ep, em = m.env.copy(), m.env.copy()
+        ep[l] += h
+        em[l] -= h
+        fd = (oracle.int1e(Molecule(m.atm, m.bas, ep), typec) -
+              oracle.int1e(Molecule(m.atm, m.bas, em), typec)) / (2 * h)
+        np.testing.assert_allclose(J[:, l].reshape(fd.shape).T, fd,
+                                   atol=1e-7 * max(1.0, np.abs(fd).max()))
