@@ -77,25 +77,13 @@ __device__ inline double common_fac_sp(int l) {
   return l == 0 ? 0.28209479177387814 : (l == 1 ? 0.48860251190291992 : 1.0);  // 1/sqrt(4pi), sqrt(3/(4pi))
 }
 
-// One thread per primitive pair.  pair 2q is the bra (i,j), 2q+1 the ket.
-// Screening key as CINTset_pairdata (reference src/optimizer.rs:732-808).
-__global__ void k_pairs(const QuartetJob *__restrict__ jobs, long long nq,
-                        const int *__restrict__ pair_off, const int *__restrict__ atm,
-                        const int *__restrict__ bas, const double *__restrict__ env,
-                        PrimPair *pp, long long npp_total) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= npp_total) return;
-  // find the pair owning entry t: binary search over pair_off (2*nq entries)
-  long long lo = 0, hi = 2 * nq - 1;
-  while (lo < hi) {
-    const long long mid = (lo + hi + 1) >> 1;
-    if (pair_off[mid] <= t) lo = mid; else hi = mid - 1;
-  }
-  const long long pr = lo;
-  const QuartetJob j = jobs[pr >> 1];
-  const bool ket = pr & 1;
-  const int si = ket ? j.ksh : j.ish, sj = ket ? j.lsh : j.jsh;
-  const int e = (int)(t - pair_off[pr]);
+// Primitive pair e (ip fastest) of shells (si, sj); ket pairs carry the
+// class prefactor.  Screening key as CINTset_pairdata (reference
+// src/optimizer.rs:732-808).
+__device__ __forceinline__ PrimPair make_pair(int si, int sj, bool ket, int e,
+                                              const int *__restrict__ atm,
+                                              const int *__restrict__ bas,
+                                              const double *__restrict__ env) {
   const int *bi = bas + 8 * si, *bj = bas + 8 * sj;
   const int ki = bi[2], kj = bj[2];
   const int ip = e % ki, jp = e / ki;
@@ -122,32 +110,55 @@ __global__ void k_pairs(const QuartetJob *__restrict__ jobs, long long nq,
   o.ia = inv;
   o.facia = fac * inv;
   o.cce = eij - log_rr - log(fabs(ci)) - log(fabs(cj));
-  pp[t] = o;
+  return o;
 }
 
-// Order every shell pair's primitive pairs by ascending screening key (NaN
-// last, ties by position), so the kernel can visit only the passing prefix.
-// One thread per entry; its rank is counted over its own pair's entries.
 __device__ __forceinline__ double cce_key(double c) { return c != c ? INFINITY : c; }
-__global__ void k_pair_sort(const PrimPair *__restrict__ raw, long long nq,
-                            const int *__restrict__ pair_off, const int *__restrict__ npair,
-                            PrimPair *__restrict__ pp, long long npp_total) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= npp_total) return;
-  long long lo = 0, hi = 2 * nq - 1;
-  while (lo < hi) {
-    const long long mid = (lo + hi + 1) >> 1;
-    if (pair_off[mid] <= t) lo = mid; else hi = mid - 1;
+
+// One warp per shell pair (pair 2q is the bra (i,j) of quartet q, 2q+1 the
+// ket): builds its primitive pairs and writes them ordered by ascending
+// screening key (NaN last, ties by position), so the ERI kernel can visit
+// only the passing prefix.  Pairs of up to 64 entries are ranked in
+// registers with shuffles; larger ones (K_i K_j > 64) go through `raw`.
+__global__ void k_pairs_sorted(const QuartetJob *__restrict__ jobs, long long nq,
+                               const int *__restrict__ pair_off, const int *__restrict__ atm,
+                               const int *__restrict__ bas, const double *__restrict__ env,
+                               PrimPair *__restrict__ pp, PrimPair *__restrict__ raw) {
+  const long long pr = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (pr >= 2 * nq) return;   // whole warps exit together
+  const QuartetJob j = jobs[pr >> 1];
+  const bool ket = pr & 1;
+  const int si = ket ? j.ksh : j.ish, sj = ket ? j.lsh : j.jsh;
+  const int n = ket ? j.nkl : j.nij;
+  const long long off = pair_off[pr];
+  if (n <= 64) {
+    const bool h0 = lane < n, h1 = lane + 32 < n;
+    PrimPair o0, o1;
+    double k0 = INFINITY, k1 = INFINITY;
+    if (h0) { o0 = make_pair(si, sj, ket, lane, atm, bas, env); k0 = cce_key(o0.cce); }
+    if (h1) { o1 = make_pair(si, sj, ket, lane + 32, atm, bas, env); k1 = cce_key(o1.cce); }
+    int r0 = 0, r1 = 0;
+    for (int u = 0; u < n; ++u) {
+      const double ku = __shfl_sync(0xffffffffu, u < 32 ? k0 : k1, u & 31);
+      r0 += (ku < k0) || (ku == k0 && u < lane);
+      r1 += (ku < k1) || (ku == k1 && u < lane + 32);
+    }
+    if (h0) pp[off + r0] = o0;
+    if (h1) pp[off + r1] = o1;
+  } else {
+    for (int e = lane; e < n; e += 32) raw[off + e] = make_pair(si, sj, ket, e, atm, bas, env);
+    __syncwarp();
+    for (int e = lane; e < n; e += 32) {
+      const double c = cce_key(raw[off + e].cce);
+      int rank = 0;
+      for (int u = 0; u < n; ++u) {
+        const double cu = cce_key(raw[off + u].cce);
+        rank += (cu < c) || (cu == c && u < e);
+      }
+      pp[off + rank] = raw[off + e];
+    }
   }
-  const long long s0 = pair_off[lo];
-  const int n = npair[lo];
-  const double c = cce_key(raw[t].cce);
-  int rank = 0;
-  for (int u = 0; u < n; ++u) {
-    const double cu = cce_key(raw[s0 + u].cce);
-    rank += (cu < c) || (cu == c && s0 + u < t);
-  }
-  pp[s0 + rank] = raw[t];
 }
 
 // Shell centres, with the bounds of every index a shell carries checked
@@ -352,11 +363,10 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   PrimPair *pp = (PrimPair *)w.reserve_pairs(st, 2 * (size_t)std::max(npp, 1LL) * sizeof(PrimPair));
   if (!pp) return set_error("workspace allocation failed"), LRB_ERR_ALLOC;
   if (npp > 0) {
-    PrimPair *raw = pp + npp;
-    k_pairs<<<(unsigned)((npp + T - 1) / T), T, 0, st>>>(jobs, nq, pair_off, d_atm, d_bas, d_env,
-                                                         raw, npp);
-    k_pair_sort<<<(unsigned)((npp + T - 1) / T), T, 0, st>>>(raw, nq, pair_off, npair, pp, npp);
-    eng.launches += 2;
+    const long long warps = 2 * nq;
+    k_pairs_sorted<<<(unsigned)((warps * 32 + T - 1) / T), T, 0, st>>>(jobs, nq, pair_off, d_atm,
+                                                                      d_bas, d_env, pp, pp + npp);
+    ++eng.launches;
   }
   LRB_CK(cudaGetLastError());
   int dev = 0, nsm = 0;

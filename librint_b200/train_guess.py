@@ -53,27 +53,35 @@ def run_scf(m, conv, guess=None):
             r, P = ctx.scf(conv=conv, P0=guess.predict(m, S=S), return_density=True, check=False,
                            **SCF_OPTS)
         if r is None or not r.converged:
-            r, P = ctx.scf(conv=conv, return_density=True, **dict(SCF_OPTS, max_iter=300))
+            r, P = ctx.scf(conv=conv, return_density=True, check=False,
+                           **dict(SCF_OPTS, max_iter=300))
     finally:
         ctx.close()
+    if not r.converged:          # no usable target (e.g. a near-degenerate flake)
+        return r, None
     Sh, _ = lowdin(S)
     return r, Sh @ P @ Sh
 
 
 def generate(ids, conv, guess=None, log=print):
-    """ids: list of (family, index); returns Loewdin densities and
-    (iterations, ms, E) per geometry."""
-    dens, stats = [], []
+    """ids: list of (family, index); returns the ids that converged, their
+    Loewdin densities and (iterations, ms, E) per geometry."""
+    kept, dens, stats = [], [], []
     for n, (fam, i) in enumerate(ids):
         m = geometry(i, fam)
         # the provisional network has seen rings only
         r, P = run_scf(m, conv, guess if fam == "rings" else None)
+        if P is None:
+            if log:
+                log(f"  {fam} {i}: SCF did not converge from the core-Hamiltonian start; skipped")
+            continue
+        kept.append((fam, i))
         dens.append(P)
         stats.append((r.iterations, r.wall_ms, r.energy))
         if log and (n % 100 == 0):
             log(f"  scf {n}/{len(ids)} ({fam} {i}, {m.nao(0)} AOs): {r.iterations} it, "
                 f"{r.wall_ms:.0f} ms, E={r.energy:.10f}")
-    return dens, stats
+    return kept, dens, stats
 
 
 def fit(model, ids, dens, hidden, epochs, batch, lr, seed, log=print):
@@ -94,7 +102,9 @@ def evaluate_one(g, m, conv, scf_opts=None):
         t0 = time.perf_counter()
         P0 = g.predict(m, S=S)
         t_pred = (time.perf_counter() - t0) * 1e3
-        rb, Pb = ctx.scf(conv=conv, return_density=True, **opts)
+        rb, Pb = ctx.scf(conv=conv, return_density=True, check=False, **opts)
+        if not rb.converged:
+            return None
         rl, _ = ctx.scf(conv=conv, P0=P0, return_density=True, check=False, **opts)
     finally:
         ctx.close()
@@ -121,6 +131,8 @@ def evaluate(g, ids, conv, log=print):
     rows = []
     for fam, i in ids:
         r = evaluate_one(g, geometry(i, fam), conv)
+        if r is None:      # no converged reference for this geometry
+            continue
         r.update(family=fam, index=i)
         rows.append(r)
     out = {}
@@ -158,24 +170,30 @@ def main(argv=None):
     t0 = time.perf_counter()
     if a.densities and os.path.exists(a.densities):
         f = np.load(a.densities, allow_pickle=True)
-        dens = list(f["Pt"])[: len(train_ids)]
-        stats = [tuple(v) for v in f["stats"][: len(train_ids)]]
+        train_ids = [(str(fam), int(i)) for fam, i in f["ids"]]
+        dens = list(f["Pt"])
+        stats = [tuple(v) for v in f["stats"]]
         print(f"loaded {len(dens)} densities from {a.densities}")
     else:
         nb = min(a.bootstrap, a.train)
         print(f"generating {nb} densities from the core-Hamiltonian start")
-        dens, stats = generate(train_ids[:nb], a.conv)
+        kept, dens, stats = generate(train_ids[:nb], a.conv)
         if nb < len(train_ids):
-            g0 = fit(model, train_ids[:nb], dens, a.hidden, max(40, a.epochs // 5),
-                     a.batch, a.lr, a.seed, log=None)[0] if nb > 0 else None
+            g0 = fit(model, kept, dens, a.hidden, max(40, a.epochs // 5),
+                     a.batch, a.lr, a.seed, log=None)[0] if kept else None
             print(f"generating {len(train_ids) - nb} more from the provisional network")
-            d2, s2 = generate(train_ids[nb:], a.conv, guess=g0)
+            k2, d2, s2 = generate(train_ids[nb:], a.conv, guess=g0)
+            kept += k2
             dens += d2
             stats += s2
+        print(f"{len(kept)} of {len(train_ids)} training geometries converged")
+        train_ids = kept
         if a.densities:
             arr = np.empty(len(dens), dtype=object)
             arr[:] = dens
-            np.savez_compressed(a.densities, Pt=arr, stats=np.array(stats))
+            ids = np.empty(len(train_ids), dtype=object)
+            ids[:] = train_ids
+            np.savez_compressed(a.densities, Pt=arr, stats=np.array(stats), ids=ids)
     t_gen = time.perf_counter() - t0
     g, hist, t_train, nsamp = fit(model, train_ids, dens, a.hidden, a.epochs, a.batch, a.lr, a.seed)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
@@ -183,6 +201,7 @@ def main(argv=None):
     ev, rows = evaluate(g, test_ids, a.conv)
     st = np.array(stats)
     summary = dict(train=a.train, flakes=a.flakes, test=a.test, test_flakes=a.test_flakes,
+                   train_converged=len(train_ids),
                    samples=nsamp, hidden=a.hidden, epochs=a.epochs, batch=a.batch, lr=a.lr,
                    conv=a.conv, scf_options=SCF_OPTS, gen_seconds=t_gen,
                    gen_iterations_mean=float(st[:, 0].mean()), gen_ms_mean=float(st[:, 1].mean()),
