@@ -129,6 +129,37 @@ def atom_rotation(ls, Q):
     return A
 
 
+def cart_rotation_batch(l: int, Q: np.ndarray) -> np.ndarray:
+    """cart_rotation for a stack of matrices Q (m, 3, 3), l <= 2."""
+    m = Q.shape[0]
+    if l == 0:
+        return np.ones((m, 1, 1))
+    if l == 1:
+        return np.ascontiguousarray(np.transpose(Q, (0, 2, 1)))
+    if l == 2:
+        A = np.empty((m, 6, 6))
+        for mu, (i, j) in enumerate(_D_PAIRS):
+            for nu, (k, q) in enumerate(_D_PAIRS):
+                v = Q[:, k, i] * Q[:, q, j]
+                if k != q:
+                    v = v + Q[:, q, i] * Q[:, k, j]
+                A[:, mu, nu] = v
+        return A
+    return np.stack([cart_rotation(l, q) for q in Q])
+
+
+def atom_rotation_batch(ls, Q):
+    """atom_rotation for a stack of matrices Q (m, 3, 3)."""
+    n = sum(ncart(l) for l in ls)
+    A = np.zeros((Q.shape[0], n, n))
+    o = 0
+    for l in ls:
+        k = ncart(l)
+        A[:, o:o + k, o:o + k] = cart_rotation_batch(l, Q)
+        o += k
+    return A
+
+
 # ------------------------------------------------------------------ features
 def molecule_geometry(m: Molecule):
     atm = np.asarray(m.atm).reshape(-1, 6)
@@ -136,6 +167,37 @@ def molecule_geometry(m: Molecule):
     z = atm[:, 0].astype(int)
     xyz = np.stack([env[p:p + 3] for p in atm[:, 1]])
     return z, xyz
+
+
+def _frames(xyz, z, A, B):
+    """Origins (m, 3) and frames (m, 3, 3) of the pairs (A[i], B[i]) -- the
+    rules of _frame, for all pairs at once."""
+    m = len(A)
+    idx = np.arange(m)
+    diag = A == B
+    O = np.where(diag[:, None], xyz[A], 0.5 * (xyz[A] + xyz[B]))
+    D = np.linalg.norm(xyz[None, :, :] - xyz[:, None, :], axis=2)
+    np.fill_diagonal(D, np.inf)
+    other = np.where(z[None, :] != z[:, None], D, np.inf)
+    near = np.where(np.isfinite(other).any(1), np.argmin(other, 1), np.argmin(D, 1))
+    e1 = np.where(diag[:, None], xyz[near[A]] - xyz[A], xyz[B] - xyz[A])
+    e1 = e1 / np.linalg.norm(e1, axis=1)[:, None]
+    T = xyz[None, :, :] - O[:, None, :]                          # (m, n, 3)
+    perp = T - np.einsum("mnk,mk->mn", T, e1)[..., None] * e1[:, None, :]
+    pn = np.linalg.norm(perp, axis=2)
+    key = np.where(pn > 0.1, np.linalg.norm(T, axis=2), np.inf)
+    key[idx, A] = np.inf
+    key[idx, B] = np.inf
+    j2 = np.argmin(key, axis=1)                                   # first among ties
+    has = np.isfinite(key[idx, j2])
+    e2 = perp[idx, j2] / np.where(has, pn[idx, j2], 1.0)[:, None]
+    if not has.all():                                             # linear: any perpendicular
+        t = np.where((np.abs(e1[:, 0]) < 0.9)[:, None], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0])
+        t = t - np.sum(t * e1, axis=1)[:, None] * e1
+        t = t / np.linalg.norm(t, axis=1)[:, None]
+        e2 = np.where(has[:, None], e2, t)
+    e3 = np.cross(e1, e2)
+    return O, np.stack([e1, e2, e3], axis=1)
 
 
 def _frame(xyz, z, a, b):
@@ -233,46 +295,57 @@ class PairModel:
         return True
 
     def pairs(self, m: Molecule) -> PairSet:
+        """All unordered atom pairs (heavier element first, diagonal
+        included) with their frames and features."""
         z, xyz = molecule_geometry(m)
         n = len(z)
-        pl, tl, fl, xl = [], [], [], []
+        a, b = np.triu_indices(n)
+        swap = z[b] > z[a]
+        A = np.where(swap, b, a)
+        B = np.where(swap, a, b)
+        T = np.array([self.type_index[(int(z[p]),)] if p == q else
+                      self.type_index[(int(z[p]), int(z[q]))] for p, q in zip(A, B)], dtype=np.int64)
+        O, F = _frames(xyz, z, A, B)
+        X = np.zeros((len(A), self.nfeat))
+        X[np.arange(len(A)), T] = 1.0
+        off = A != B
+        r = np.linalg.norm(xyz[B] - xyz[A], axis=1)
+        X[:, self.ntypes] = np.where(off, r, 0.0)
+        X[:, self.ntypes + 1] = np.where(off, np.exp(-0.5 * r), 0.0)
+        d = np.einsum("mij,mnj->mni", F, xyz[None, :, :] - O[:, None, :])   # frame coordinates
+        rj = np.linalg.norm(d, axis=2)
+        u = d / np.maximum(rj, 1e-12)[..., None]
+        g = np.exp(-((rj[..., None] - RADIAL_CENTRES) / RADIAL_WIDTH) ** 2)  # (m, n, nk)
+        keep = np.ones((len(A), n))
+        keep[np.arange(len(A)), A] = 0.0
+        keep[np.arange(len(A)), B] = 0.0
+        g = g * keep[..., None]
         nk = len(RADIAL_CENTRES)
-        for a in range(n):
-            for b in range(a, n):
-                aa, bb = a, b
-                if z[b] > z[a]:
-                    aa, bb = b, a           # heavier element first
-                if aa == bb:
-                    t = self.type_index[(int(z[aa]),)]
-                else:
-                    t = self.type_index[(int(z[aa]), int(z[bb]))]
-                o, F = _frame(xyz, z, aa, bb)
-                x = np.zeros(self.nfeat)
-                x[t] = 1.0
-                if aa != bb:
-                    r = np.linalg.norm(xyz[bb] - xyz[aa])
-                    x[self.ntypes] = r
-                    x[self.ntypes + 1] = math.exp(-0.5 * r)
-                base = self.ntypes + 2
-                for j in range(n):
-                    if j in (aa, bb):
-                        continue
-                    d = F @ (xyz[j] - o)
-                    rj = np.linalg.norm(d)
-                    g = np.exp(-((rj - RADIAL_CENTRES) / RADIAL_WIDTH) ** 2)
-                    e = self.elements.index(int(z[j]))
-                    blk = base + e * nk * 4
-                    u = d / max(rj, 1e-12)
-                    x[blk:blk + nk] += g
-                    x[blk + nk:blk + 2 * nk] += g * u[0]
-                    x[blk + 2 * nk:blk + 3 * nk] += g * u[1]
-                    x[blk + 3 * nk:blk + 4 * nk] += g * u[2]
-                pl.append((aa, bb))
-                tl.append(t)
-                fl.append(F)
-                xl.append(x)
-        return PairSet(np.array(pl, dtype=np.int64), np.array(tl, dtype=np.int64),
-                       np.array(fl), np.array(xl))
+        base = self.ntypes + 2
+        for e, ze in enumerate(self.elements):
+            sel = z == ze
+            if not sel.any():
+                continue
+            ge, ue = g[:, sel], u[:, sel]
+            blk = base + e * nk * 4
+            X[:, blk:blk + nk] = ge.sum(1)
+            for c in range(3):
+                X[:, blk + (c + 1) * nk:blk + (c + 2) * nk] = (ge * ue[:, :, c, None]).sum(1)
+        return PairSet(np.stack([A, B], 1).astype(np.int64), T, F, X)
+
+    def _rots(self, z, ps: PairSet, frames):
+        """Rotation matrices of the A and B atoms of every pair for the given
+        frames, batched per element."""
+        RA = [None] * len(ps.pairs)
+        RB = [None] * len(ps.pairs)
+        for side, R in ((0, RA), (1, RB)):
+            zs = z[ps.pairs[:, side]]
+            for ze in np.unique(zs):
+                sel = np.nonzero(zs == ze)[0]
+                rot = atom_rotation_batch(self.layouts[int(ze)], frames[sel])
+                for k, i in enumerate(sel):
+                    R[i] = rot[k]
+        return RA, RB
 
     def _rot(self, zz, F):
         return atom_rotation(self.layouts[zz], F)
@@ -283,12 +356,11 @@ class PairModel:
         lay = _atom_layout(m)
         Y = np.zeros((len(ps.pairs), self.nmax, self.nmax))
         M = np.zeros_like(Y)
-        for i, ((a, b), F) in enumerate(zip(ps.pairs, ps.frames)):
+        RA, RB = self._rots(z, ps, ps.frames)
+        for i, (a, b) in enumerate(ps.pairs):
             oa, _, na = lay[a]
             ob, _, nb = lay[b]
-            blk = P[oa:oa + na, ob:ob + nb]
-            loc = self._rot(int(z[a]), F).T @ blk @ self._rot(int(z[b]), F)
-            Y[i, :na, :nb] = loc
+            Y[i, :na, :nb] = RA[i].T @ P[oa:oa + na, ob:ob + nb] @ RB[i]
             M[i, :na, :nb] = 1.0
         return Y.reshape(len(ps.pairs), -1), M.reshape(len(ps.pairs), -1)
 
@@ -298,11 +370,11 @@ class PairModel:
         n = lay[-1][0] + lay[-1][2]
         P = np.zeros((n, n))
         Y = Yloc.reshape(len(ps.pairs), self.nmax, self.nmax)
-        for i, ((a, b), F) in enumerate(zip(ps.pairs, ps.frames)):
+        RA, RB = self._rots(z, ps, np.transpose(ps.frames, (0, 2, 1)))
+        for i, (a, b) in enumerate(ps.pairs):
             oa, _, na = lay[a]
             ob, _, nb = lay[b]
-            Ft = F.T
-            blk = self._rot(int(z[a]), Ft).T @ Y[i, :na, :nb] @ self._rot(int(z[b]), Ft)
+            blk = RA[i].T @ Y[i, :na, :nb] @ RB[i]
             if a == b:
                 blk = 0.5 * (blk + blk.T)
             P[oa:oa + na, ob:ob + nb] = blk

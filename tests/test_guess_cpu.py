@@ -145,3 +145,47 @@ def test_lowdin_density_round_trip():
     P0 = G.density_from_lowdin(Pt + noise + noise.T, S, m.nelec // 2)
     assert abs(np.sum(P0 * S) - m.nelec) < 1e-10
     np.testing.assert_allclose(P0 @ S @ P0, 2 * P0, atol=1e-10)
+
+
+def _pairs_loop(pm, m):
+    """Per-pair restatement of PairModel.pairs (frames by _frame), the
+    reference for the vectorised version."""
+    z, xyz = G.molecule_geometry(m)
+    n = len(z)
+    nk = len(G.RADIAL_CENTRES)
+    out = []
+    for a in range(n):
+        for b in range(a, n):
+            aa, bb = (b, a) if z[b] > z[a] else (a, b)
+            t = pm.type_index[(int(z[aa]),)] if aa == bb else pm.type_index[(int(z[aa]), int(z[bb]))]
+            o, F = G._frame(xyz, z, aa, bb)
+            x = np.zeros(pm.nfeat)
+            x[t] = 1.0
+            if aa != bb:
+                r = np.linalg.norm(xyz[bb] - xyz[aa])
+                x[pm.ntypes], x[pm.ntypes + 1] = r, np.exp(-0.5 * r)
+            for j in range(n):
+                if j in (aa, bb):
+                    continue
+                d = F @ (xyz[j] - o)
+                rj = np.linalg.norm(d)
+                g = np.exp(-((rj - G.RADIAL_CENTRES) / G.RADIAL_WIDTH) ** 2)
+                blk = pm.ntypes + 2 + pm.elements.index(int(z[j])) * nk * 4
+                u = d / max(rj, 1e-12)
+                x[blk:blk + nk] += g
+                for c in range(3):
+                    x[blk + (c + 1) * nk:blk + (c + 2) * nk] += g * u[c]
+            out.append(((aa, bb), t, F, x))
+    return out
+
+
+@pytest.mark.parametrize("mol", ["ring", "flake"])
+def test_vectorised_pairs_match_loop(mol):
+    m = synthetic.benzene_like(21) if mol == "ring" else synthetic.flake_like(20003)
+    pm = G.PairModel.from_molecule(synthetic.benzene_like(1))
+    ps = pm.pairs(m)
+    ref = _pairs_loop(pm, m)
+    assert [tuple(p) for p in ps.pairs] == [r[0] for r in ref]
+    assert list(ps.types) == [r[1] for r in ref]
+    np.testing.assert_allclose(ps.frames, np.array([r[2] for r in ref]), atol=1e-12)
+    np.testing.assert_allclose(ps.X, np.array([r[3] for r in ref]), atol=1e-12)
