@@ -115,49 +115,141 @@ __device__ __forceinline__ PrimPair make_pair(int si, int sj, bool ket, int e,
 
 __device__ __forceinline__ double cce_key(double c) { return c != c ? INFINITY : c; }
 
-// One warp per shell pair (pair 2q is the bra (i,j) of quartet q, 2q+1 the
-// ket): builds its primitive pairs and writes them ordered by ascending
-// screening key (NaN last, ties by position), so the ERI kernel can visit
-// only the passing prefix.  Pairs of up to 64 entries are ranked in
-// registers with shuffles; larger ones (K_i K_j > 64) go through `raw`.
-__global__ void k_pairs_sorted(const QuartetJob *__restrict__ jobs, long long nq,
+// One warp sorts shell pair pr (pair 2q is the bra (i,j) of quartet q,
+// 2q+1 the ket): builds its primitive pairs in natural order in `raw`, then
+// writes each at its rank by ascending screening key (NaN last, ties by
+// position), so the ERI kernel can visit only the passing prefix.
+__device__ void pair_sort_warp(long long pr, int lane, const QuartetJob *__restrict__ jobs,
                                const int *__restrict__ pair_off, const int *__restrict__ atm,
                                const int *__restrict__ bas, const double *__restrict__ env,
                                PrimPair *__restrict__ pp, PrimPair *__restrict__ raw) {
-  const long long pr = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (pr >= 2 * nq) return;   // whole warps exit together
   const QuartetJob j = jobs[pr >> 1];
   const bool ket = pr & 1;
   const int si = ket ? j.ksh : j.ish, sj = ket ? j.lsh : j.jsh;
   const int n = ket ? j.nkl : j.nij;
   const long long off = pair_off[pr];
-  if (n <= 64) {
-    const bool h0 = lane < n, h1 = lane + 32 < n;
-    PrimPair o0, o1;
-    double k0 = INFINITY, k1 = INFINITY;
-    if (h0) { o0 = make_pair(si, sj, ket, lane, atm, bas, env); k0 = cce_key(o0.cce); }
-    if (h1) { o1 = make_pair(si, sj, ket, lane + 32, atm, bas, env); k1 = cce_key(o1.cce); }
-    int r0 = 0, r1 = 0;
+  for (int e = lane; e < n; e += 32) raw[off + e] = make_pair(si, sj, ket, e, atm, bas, env);
+  __syncwarp();
+  for (int e = lane; e < n; e += 32) {
+    const double c = cce_key(raw[off + e].cce);
+    int rank = 0;
     for (int u = 0; u < n; ++u) {
-      const double ku = __shfl_sync(0xffffffffu, u < 32 ? k0 : k1, u & 31);
-      r0 += (ku < k0) || (ku == k0 && u < lane);
-      r1 += (ku < k1) || (ku == k1 && u < lane + 32);
+      const double cu = cce_key(raw[off + u].cce);
+      rank += (cu < c) || (cu == c && u < e);
     }
-    if (h0) pp[off + r0] = o0;
-    if (h1) pp[off + r1] = o1;
-  } else {
-    for (int e = lane; e < n; e += 32) raw[off + e] = make_pair(si, sj, ket, e, atm, bas, env);
-    __syncwarp();
-    for (int e = lane; e < n; e += 32) {
-      const double c = cce_key(raw[off + e].cce);
-      int rank = 0;
-      for (int u = 0; u < n; ++u) {
-        const double cu = cce_key(raw[off + u].cce);
-        rank += (cu < c) || (cu == c && u < e);
-      }
-      pp[off + rank] = raw[off + e];
+    pp[off + rank] = raw[off + e];
+  }
+}
+
+// Shell-pair constants of one block's pairs, staged once per pair so every
+// primitive of the pair needs only its four exponent/coefficient loads.
+struct PairHead {
+  double rix, riy, riz;   // centre of shell i
+  double dx, dy, dz;      // R_j - R_i
+  double rr, log_rr, cfac;
+  int ea, ca, eb, cb;     // env offsets of exponents / coefficients of i and j
+  int ki, first;          // primitives of i; first primitive pair (block-relative)
+};
+
+constexpr int PB_PAIRS = 64;      // shell pairs per block
+constexpr int PB_THREADS = 256;
+constexpr int PB_CAP = 4096;      // primitive pairs per block ranked through shared memory
+
+// Block of PB_PAIRS consecutive shell pairs: pass 1 writes every primitive
+// pair's screening key (the same expression as make_pair) to shared memory
+// with one thread per primitive pair, pass 2 rebuilds the pair and stores it
+// at its rank within its shell pair (ascending key, NaN last, ties by
+// position: the order pair_sort_warp produces).  Blocks whose primitive
+// pairs exceed PB_CAP sort warp by warp instead.
+__global__ void __launch_bounds__(PB_THREADS, 3)
+k_pairs_block(const QuartetJob *__restrict__ jobs, long long nq, const int *__restrict__ npair,
+              const int *__restrict__ pair_off, const int *__restrict__ atm,
+              const int *__restrict__ bas, const double *__restrict__ env,
+              PrimPair *__restrict__ pp, PrimPair *__restrict__ raw) {
+  __shared__ double skey[PB_CAP];
+  __shared__ PairHead head[PB_PAIRS];
+  __shared__ int soff[PB_PAIRS + 1];
+  const long long p0 = (long long)blockIdx.x * PB_PAIRS;
+  const int P = (int)min((long long)PB_PAIRS, 2 * nq - p0);
+  const int t = threadIdx.x;
+  if (t < P) {
+    const long long pr = p0 + t;
+    soff[t] = pair_off[pr];
+    if (t == P - 1) soff[P] = pair_off[pr] + npair[pr];
+    const QuartetJob j = jobs[pr >> 1];
+    const bool ket = pr & 1;
+    const int *bi = bas + 8 * (ket ? j.ksh : j.ish), *bj = bas + 8 * (ket ? j.lsh : j.jsh);
+    const int ki = bi[2], kj = bj[2];
+    const double *ri = env + atm[6 * bi[0] + 1], *rj = env + atm[6 * bj[0] + 1];
+    PairHead h;
+    h.rix = ri[0]; h.riy = ri[1]; h.riz = ri[2];
+    h.dx = ri[0] - rj[0]; h.dy = ri[1] - rj[1]; h.dz = ri[2] - rj[2];
+    h.rr = h.dx * h.dx + h.dy * h.dy + h.dz * h.dz;
+    h.dx = rj[0] - ri[0]; h.dy = rj[1] - ri[1]; h.dz = rj[2] - ri[2];
+    h.ea = bi[5]; h.ca = bi[6]; h.eb = bj[5]; h.cb = bj[6]; h.ki = ki;
+    const int lij = bi[1] + bj[1];
+    double log_rr = 1.7 - 1.5 * log(env[bi[5] + ki - 1] + env[bj[5] + kj - 1]);
+    if (lij > 0) log_rr += lij * log(sqrt(h.rr) + 1.0);
+    h.log_rr = log_rr;
+    // 2 pi^3 / sqrt(pi) = 2 pi^2.5 (reference src/g2e.rs:74-82), on the ket side
+    h.cfac = common_fac_sp(bi[1]) * common_fac_sp(bj[1]) * (ket ? 34.986836655249725 : 1.0);
+    head[t] = h;
+  }
+  __syncthreads();
+  const int base = soff[0], R = soff[P] - base;
+  if (R > PB_CAP) {
+    for (int w = t >> 5; w < P; w += PB_THREADS / 32)
+      pair_sort_warp(p0 + w, t & 31, jobs, pair_off, atm, bas, env, pp, raw);
+    return;
+  }
+  if (t < P) head[t].first = soff[t] - base;
+  __syncthreads();
+  // local shell pair of block-relative primitive pair e
+  auto find = [&](int e) {
+    int lo = 0, hi = P - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (soff[mid] - base <= e) lo = mid; else hi = mid - 1;
     }
+    return lo;
+  };
+  for (int e = t; e < R; e += PB_THREADS) {
+    const PairHead &h = head[find(e)];
+    const int k = e - h.first, ip = k % h.ki, jp = k / h.ki;
+    const double ai = env[h.ea + ip], aj = env[h.eb + jp];
+    const double ci = env[h.ca + ip], cj = env[h.cb + jp];
+    const double inv = 1.0 / (ai + aj);
+    const double eij = h.rr * ai * aj * inv;
+    skey[e] = eij - h.log_rr - log(fabs(ci)) - log(fabs(cj));
+  }
+  __syncthreads();
+  for (int e = t; e < R; e += PB_THREADS) {
+    const int p = find(e);
+    const PairHead &h = head[p];
+    const int k = e - h.first, ip = k % h.ki, jp = k / h.ki;
+    const double ai = env[h.ea + ip], aj = env[h.eb + jp];
+    const double ci = env[h.ca + ip], cj = env[h.cb + jp];
+    const double aij = ai + aj, inv = 1.0 / aij;
+    const double eij = h.rr * ai * aj * inv;
+    const double wj = aj * inv;
+    PrimPair o;
+    o.a = aij;
+    o.px = h.rix + wj * h.dx;
+    o.py = h.riy + wj * h.dy;
+    o.pz = h.riz + wj * h.dz;
+    const double fac = ci * cj * exp(-eij) * h.cfac;
+    o.fac = fac;
+    o.ia = inv;
+    o.facia = fac * inv;
+    o.cce = skey[e];
+    const double c = cce_key(o.cce);
+    const int n = (p + 1 < P ? head[p + 1].first : R) - h.first;
+    int rank = 0;
+    for (int u = 0; u < n; ++u) {
+      const double cu = cce_key(skey[h.first + u]);
+      rank += (cu < c) || (cu == c && u < k);
+    }
+    pp[base + h.first + rank] = o;
   }
 }
 
@@ -265,6 +357,12 @@ const double *rys_table_device() {
   return p;
 }
 
+const float *rys_table_device_f32() {
+  const float *p = nullptr;
+  cudaGetSymbolAddress((void **)&p, RYS32_TAB);
+  return p;
+}
+
 // ---------------------------------------------------------------- driver
 #define LRB_CK(x)                                        \
   do {                                                   \
@@ -363,9 +461,8 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   PrimPair *pp = (PrimPair *)w.reserve_pairs(st, 2 * (size_t)std::max(npp, 1LL) * sizeof(PrimPair));
   if (!pp) return set_error("workspace allocation failed"), LRB_ERR_ALLOC;
   if (npp > 0) {
-    const long long warps = 2 * nq;
-    k_pairs_sorted<<<(unsigned)((warps * 32 + T - 1) / T), T, 0, st>>>(jobs, nq, pair_off, d_atm,
-                                                                      d_bas, d_env, pp, pp + npp);
+    k_pairs_block<<<(unsigned)((2 * nq + PB_PAIRS - 1) / PB_PAIRS), PB_THREADS, 0, st>>>(
+        jobs, nq, npair, pair_off, d_atm, d_bas, d_env, pp, pp + npp);
     ++eng.launches;
   }
   LRB_CK(cudaGetLastError());

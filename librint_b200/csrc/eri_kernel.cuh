@@ -104,7 +104,7 @@ struct EriClass {
 template <class C, int MODE = 0, typename R = double>
 struct EriLayout {
   static constexpr int NKO_MAX = C::NKET;   // cartesian >= spherical
-  // per-slot sizes in doubles: roots, weights, 1/(1+u) (3 NR, FP64), then G
+  // per-slot sizes in doubles: roots, weights, 1/(1+u) (3 NR, type R), then G
   // (NR*3*GSZ) and per-unit bra-shift scratch (3*NR*TSZ) in the arithmetic
   // type R in the loop; block (NBRA*NKET, R) + ket-transformed block
   // (NBRA*NKO, output mode only) in the epilogue.  FP32 halves the R parts.
@@ -113,7 +113,10 @@ struct EriLayout {
   static constexpr int EPI = RD(C::NBRA * C::NKET) + (MODE == 0 ? C::NBRA * NKO_MAX : 0);
   static constexpr int SLOT = LOOP > EPI ? LOOP : EPI;
   static constexpr int WARP = C::SLOTS * SLOT;
-  static constexpr int TAB = (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR]);
+  // Rys table in doubles: FP64 coefficients, or the FP32 table for R = float
+  static constexpr int TAB = sizeof(R) == 8
+                                 ? (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR])
+                                 : RD(RYS32_TAB_OFFSET[C::NR + 1] - RYS32_TAB_OFFSET[C::NR]);
   static constexpr int C2S = 3 * 5 * 6;    // l <= 2, m, cart
   static constexpr size_t SMEM = sizeof(double) * (size_t)(TAB + C2S + ERI_WARPS * WARP);
 };
@@ -280,14 +283,22 @@ __device__ __forceinline__ void cart_comp_rt(int l, int n, int &x, int &y, int &
 // weights and pair data are always evaluated in FP64 and rounded after.
 template <int LI, int LJ, int LK, int LL, int MODE, typename R = double>
 __global__ void __launch_bounds__(ERI_THREADS)
-k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *counter) {
+k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *counter) {
   using C = EriClass<LI, LJ, LK, LL, true>;
   using L = EriLayout<C, MODE, R>;
   static_assert(MODE == 1 || sizeof(R) == 8, "output mode is FP64");
   extern __shared__ double smem[];
-  double *tab = smem;
+  double *tab = smem;                                    // FP64 table (R = double)
+  float *tab32 = reinterpret_cast<float *>(smem);        // FP32 table (R = float)
   double *c2s_s = smem + L::TAB;            // [3][5][6]
-  for (int i = threadIdx.x; i < L::TAB; i += blockDim.x) tab[i] = rys_tab_n[i];
+  if constexpr (sizeof(R) == 8) {
+    for (int i = threadIdx.x; i < L::TAB; i += blockDim.x)
+      tab[i] = static_cast<const double *>(rys_tab_n)[i];
+  } else {
+    constexpr int NT = RYS32_TAB_OFFSET[C::NR + 1] - RYS32_TAB_OFFSET[C::NR];
+    for (int i = threadIdx.x; i < NT; i += blockDim.x)
+      tab32[i] = static_cast<const float *>(rys_tab_n)[i];
+  }
   for (int i = threadIdx.x; i < L::C2S; i += blockDim.x) {
     const int l = i / 30, m = (i / 6) % 5, c = i % 6;
     c2s_s[i] = c_c2s[(l * C2S_M + m) * C2S_C + c];
@@ -301,7 +312,7 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
   const bool lane_live = slot < C::SLOTS;
   const int myslot = lane_live ? slot : C::SLOTS - 1;
   double *sb = wbuf + myslot * L::SLOT;        // this slot's area
-  double *RW = sb;                             // [3*NR] FP64 roots, weights, 1/(1+u)
+  R *RW = reinterpret_cast<R *>(sb);           // [3*NR] roots, weights, 1/(1+u)
   R *G = reinterpret_cast<R *>(sb + 3 * C::NR);            // [NR][3][GSZ]
   R *Tsc = G + C::NR * 3 * C::GSZ;                         // [3*NR][TSZ]
 
@@ -458,18 +469,29 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
           if (++ij == job.nij) { ij = 0; ++kl; }
         }
       }
-      double aij = 1.0, akl = 1.0, inv = 1.0, fac1 = 0.0, x = 0.0;
-      double pq[3] = {0, 0, 0};
+      R aij = 1, akl = 1, inv = 1, fac1 = 0, x = 0;
+      R pq[3] = {0, 0, 0};
       if (run) {
-        aij = bra.a; akl = ket.a;
-        inv = 1.0 / (aij + akl);
-        fac1 = sqrt(inv) * bra.facia * ket.facia;
-        pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
+        if constexpr (sizeof(R) == 8) {
+          aij = bra.a; akl = ket.a;
+          inv = 1.0 / (aij + akl);
+          fac1 = sqrt(inv) * bra.facia * ket.facia;
+          pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
+        } else {
+          // FP32 prefactors: differences of the FP64 pair data are formed in
+          // FP64 (cancellation), the rest in FP32
+          aij = (R)bra.a; akl = (R)ket.a;
+          inv = 1.0f / (aij + akl);
+          fac1 = sqrtf(inv) * (R)(bra.facia * ket.facia);
+          pq[0] = (R)(bra.px - ket.px); pq[1] = (R)(bra.py - ket.py); pq[2] = (R)(bra.pz - ket.pz);
+        }
         x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
         for (int f = rho; f < 2 * C::NR; f += C::LANES) {
-          const double v = rys_function<C::NR>(tab, x, f);
+          R v;
+          if constexpr (sizeof(R) == 8) v = rys_function<C::NR>(tab, x, f);
+          else v = rys_function_f32<C::NR>(tab32, x, f);
           RW[f] = v;
-          if (f < C::NR) RW[2 * C::NR + f] = 1.0 / (1.0 + v);   // t^2 complement 1/(1+u)
+          if (f < C::NR) RW[2 * C::NR + f] = (R)1 / ((R)1 + v);   // t^2 complement 1/(1+u)
         }
       }
       __syncwarp();
@@ -482,22 +504,22 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
           const int u = rho + k * C::LANES;
           if (u >= 3 * C::NR) break;
           const int r = u / 3, ax = u - 3 * r;
-          const double pa = pick3(bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2], ax);
-          const double qc = pick3(ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2], ax);
-          const double pqa = pick3(pq[0], pq[1], pq[2], ax);
-          const double ab = pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
-          const double cd = pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
+          const R pa = (R)pick3(bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2], ax);
+          const R qc = (R)pick3(ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2], ax);
+          const R pqa = pick3(pq[0], pq[1], pq[2], ax);
+          const R ab = (R)pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
+          const R cd = (R)pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
           // with d = 1/(1+u): B00 = u d / (2 (aij+akl)), B10 = B00 + d / (2 aij),
           // B01 = B00 + d / (2 akl) (u2 (aij+akl) + aij akl = aij akl (1+u))
-          const double d = RW[2 * C::NR + r];
-          const double tmp5 = 0.5 * inv * RW[r] * d;
-          const double b10 = tmp5 + 0.5 * bra.ia * d;
-          const double b01 = tmp5 + 0.5 * ket.ia * d;
-          const double cn = pa - 2.0 * tmp5 * akl * pqa;
-          const double cm = qc + 2.0 * tmp5 * aij * pqa;
-          const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;
-          vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, (R)v00, (R)cn, (R)cm,
-                             (R)b10, (R)b01, (R)tmp5, (R)ab, (R)cd);
+          const R d = RW[2 * C::NR + r];
+          const R tmp5 = (R)0.5 * inv * RW[r] * d;
+          const R b10 = tmp5 + (R)0.5 * (R)bra.ia * d;
+          const R b01 = tmp5 + (R)0.5 * (R)ket.ia * d;
+          const R cn = pa - (R)2 * tmp5 * akl * pqa;
+          const R cm = qc + (R)2 * tmp5 * aij * pqa;
+          const R v00 = ax == 2 ? RW[C::NR + r] * fac1 : (R)1;
+          vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, v00, cn, cm, b10, b01,
+                             tmp5, ab, cd);
         }
       }
       __syncwarp();

@@ -22,6 +22,7 @@
 namespace lrb {
 
 const double *rys_table_device();
+const float *rys_table_device_f32();
 
 #define FK_CK(x)                                  \
   do {                                            \
@@ -438,6 +439,7 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const double *rys = rys_table_device();
+    const float *rys32 = rys_table_device_f32();
     EriParams prm{};
     prm.pp = m.pp;
     prm.centers = m.centers;
@@ -472,8 +474,9 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
         cudaEventCreate(&rec.stop);
         cudaEventRecord(rec.start, st);
       }
-      ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(prm, fk, rys + RYS_TAB_OFFSET[ce.nr],
-                                                                  counters + cc);
+      const void *tabn = fi == 2 ? (const void *)(rys32 + RYS32_TAB_OFFSET[ce.nr])
+                                 : (const void *)(rys + RYS_TAB_OFFSET[ce.nr]);
+      ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(prm, fk, tabn, counters + cc);
       FK_CK(cudaGetLastError());
       eng.launches++;
       if (eng.profile) {
