@@ -88,6 +88,14 @@ def class_flops_bytes(cls, bas, shls):
     return flops, nbytes
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per shell quartet
+# of the output kernels, from one ncu capture of 65,536 quartets of the sweep
+# class (K = 1..6, spherical output); traffic grows with the quartets processed
+# (output block plus pair data), so a launch's traffic is this times its
+# quartet count.
+NCU_TRAFFIC_PER_QUARTET = {(2, 2, 2, 2): (81.393408e6 + 269.814016e6) / 65536}
+
+
 def class_id(c):
     """Kernel class id of (li, lj, lk, ll): P(P+1)/2 + Q over pair indices."""
     P = c[0] * (c[0] + 1) // 2 + c[1]
@@ -422,14 +430,18 @@ def main():
                        "l2": "outputs (%.1f GB/step) exceed L2; no flush needed" %
                              (sum(t['out'].numel() for t in dev_data) * 8 / 1e9),
                        "parallelism": f"dp{world} (independent quartet shards)"},
-            "roofline": {"bound": "fp64", "kernel": "k_eri_out<%d,%d,%d,%d>" % top,
+            "roofline": {"bound": "fp64", "kernel": "k_eri<%d,%d,%d,%d,0,double>" % top,
                          "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
                          "frac": achieved_tf / fp64_peak if fp64_peak > 0 else None,
                          "peak_source": "measured FP64 FMA probe (lrb_fp64_peak_probe) on this "
                                         "GPU; MEASURED_PEAKS.json has no FP64 figure",
                          "kernel_ms": top_ms, "kernel_share": top_ms / total_kernel_ms,
                          "flop_convention": "fixed per-quartet count, see class_flops_bytes",
-                         "traffic": None},
+                         "traffic": (NCU_TRAFFIC_PER_QUARTET[tuple(top)] * d_top[4].shape[0]
+                                     if tuple(top) in NCU_TRAFFIC_PER_QUARTET else None),
+                         "algorithmic_bytes": class_flops_bytes(top, d_top[2], d_top[4])[1],
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                           "65,536 quartets of this class, scaled per quartet"},
             "class_kernel_ms": {"%d%d%d%d" % c: round(v, 4) for c, v in cls_ms.items()},
             "cpu_baseline": cpu,
             "e2e": e2e,

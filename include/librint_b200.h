@@ -152,6 +152,8 @@ typedef struct {
   double fp32_until;  /* all-FP32 builds while ||dP|| is above this */
   double tau32;       /* then FP32 only for Schwarz x |dD| bounds below this */
   int rebuild_every;  /* full (non-incremental) Fock build period */
+  double tau_fp32;    /* screening threshold of the FP32 and split builds
+                         (0: tau); the FP64 phase always screens at tau */
 } LrbScfOptions;
 
 typedef struct {

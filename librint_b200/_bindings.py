@@ -67,7 +67,7 @@ class ScfOptions(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv", ctypes.c_double), ("guess", ctypes.c_int),
                 ("diis", ctypes.c_int), ("tau", ctypes.c_double), ("mixed", ctypes.c_int),
                 ("fp32_until", ctypes.c_double), ("tau32", ctypes.c_double),
-                ("rebuild_every", ctypes.c_int)]
+                ("rebuild_every", ctypes.c_int), ("tau_fp32", ctypes.c_double)]
 
 
 class ScfResult(ctypes.Structure):

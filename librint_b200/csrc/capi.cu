@@ -481,6 +481,7 @@ LRB_API int lrb_scf(LrbMol *m, long long nelec, const LrbScfOptions *opt, LrbScf
     o.max_iter = opt->max_iter; o.conv = opt->conv; o.guess = opt->guess; o.diis = opt->diis;
     o.tau = opt->tau; o.mixed = opt->mixed; o.fp32_until = opt->fp32_until;
     o.tau32 = opt->tau32; o.rebuild_every = opt->rebuild_every > 0 ? opt->rebuild_every : 6;
+    o.tau_fp32 = opt->tau_fp32;
   }
   ScfResult r;
   const int rc = scf_run(m->ctx, (size_t)nelec, o, &r, P_out, P0, nullptr);

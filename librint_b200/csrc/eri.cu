@@ -113,8 +113,6 @@ __device__ __forceinline__ PrimPair make_pair(int si, int sj, bool ket, int e,
   return o;
 }
 
-__device__ __forceinline__ double cce_key(double c) { return c != c ? INFINITY : c; }
-
 // One warp sorts shell pair pr (pair 2q is the bra (i,j) of quartet q,
 // 2q+1 the ket): builds its primitive pairs in natural order in `raw`, then
 // writes each at its rank by ascending screening key (NaN last, ties by

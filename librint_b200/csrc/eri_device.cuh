@@ -120,6 +120,9 @@ struct QuartetJob {
   int s_i, s_j, s_k, s_l; // output strides of the canonical indices
 };
 
+// Sort key of a primitive pair's screening value: NaN orders last.
+__device__ __forceinline__ double cce_key(double c) { return c != c ? INFINITY : c; }
+
 // A shell pair of a molecule's pair table (oriented l_i >= l_j).
 struct PairInfo {
   int ish, jsh;           // shells
@@ -189,24 +192,26 @@ __device__ __forceinline__ double rys_function(const double *tab, double x, int 
 
 // FP32 counterpart of rys_function for the mixed-precision Fock kernels:
 // economised degree-RYS32_DEG segments of rys_tables_f32.h (float table
-// staged in shared memory), the same large-x limit rounded to float.
+// staged in shared memory), the same large-x limit rounded to float.  The
+// argument x and the local variable t are formed in FP64 and only t is
+// rounded, so the table sees an x error of ~1e-7 absolute, not relative.
 template <int N>
-__device__ __forceinline__ float rys_function_f32(const float *tab, float x, int f) {
+__device__ __forceinline__ float rys_function_f32(const float *tab, double x, int f) {
   static_assert(N <= RYS32_NMAX, "FP32 Rys tables cover up to RYS32_NMAX roots");
-  constexpr float XBREAK = 43.0f + 5.0f * N;
+  constexpr double XBREAK = 43.0 + 5.0 * N;
   if (x >= XBREAK) {
     constexpr int off = N * (N - 1) / 2;
+    const float xf = (float)x;
     if (f < N) {
       const float r = (float)RYS_LARGEX_R[off + f];
-      return r / (x - r);
+      return r / (xf - r);
     }
-    return (float)RYS_LARGEX_W[off + f - N] * sqrtf(0.785398163f / x);  // pi/4
+    return (float)RYS_LARGEX_W[off + f - N] * sqrtf(0.785398163f / xf);  // pi/4
   }
   constexpr int NSEG = rys_nseg(N);
-  int seg = (int)(x * (float)(1.0 / RYS_SEG_WIDTH));
+  int seg = (int)(x * (1.0 / RYS_SEG_WIDTH));
   seg = seg < 0 ? 0 : (seg >= NSEG ? NSEG - 1 : seg);
-  const float t = (x - (seg * (float)RYS_SEG_WIDTH + (float)(0.5 * RYS_SEG_WIDTH))) *
-                  (float)(2.0 / RYS_SEG_WIDTH);
+  const float t = (float)((x - (seg * RYS_SEG_WIDTH + 0.5 * RYS_SEG_WIDTH)) * (2.0 / RYS_SEG_WIDTH));
   const float *c = tab + (seg * 2 * N + f) * RYS32_NCOEF;
   float r = c[RYS32_DEG];
 #pragma unroll

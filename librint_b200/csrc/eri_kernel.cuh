@@ -399,14 +399,14 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
       if (pk.ish == pk.jsh) wdeg *= 0.5;
       if (jb.x == jb.y) wdeg *= 0.5;
     }
-    // Primitive quartets to visit.  Output mode: each shell pair's primitive
-    // pairs are sorted by ascending screening key cce, so for ket pair kl the
-    // bra pairs that pass (bra.cce <= cutoff - ket.cce) are a prefix of
-    // length nb(kl), non-increasing in kl; only those are visited.  Fock mode
-    // (pairs in natural order) visits all and tests each.
+    // Primitive quartets to visit.  Each shell pair's primitive pairs are
+    // sorted by ascending screening key cce, so for ket pair kl the bra pairs
+    // that pass (bra.cce <= cutoff - ket.cce, reference src/cint2e.rs:367-393)
+    // are a prefix of length nb(kl), non-increasing in kl; only those are
+    // visited.
     const double cut = prm.expcutoff;
     int np = 0;
-    if constexpr (MODE == 0) {
+    {
       int nb = job.nij;
       for (int k = 0; k < job.nkl; ++k) {
         const double kc = prm.pp[job.pkl_off + k].cce;
@@ -415,8 +415,6 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
         if (nb == 0) break;
         np += nb;
       }
-    } else {
-      np = job.nij * job.nkl;
     }
     int npmax = np;
 #pragma unroll
@@ -441,51 +439,52 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
     for (int k = 0; k < (C::NEX > 0 ? C::NEX : 1); ++k) xacc[k] = 0;
 
     int ij = 0, kl = 0;
-    int nbk = job.nij;   // output mode: passing bra prefix of the current ket pair
-    if constexpr (MODE == 0) {
-      if (np > 0) {
-        const double kc = prm.pp[job.pkl_off].cce;
-        while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
-      }
+    int nbk = job.nij;   // passing bra prefix of the current ket pair
+    if (np > 0) {
+      const double kc = prm.pp[job.pkl_off].cce;
+      while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
     }
     for (int p = 0; p < npmax; ++p) {
-      bool run = p < np;
+      const bool run = p < np;
       PrimPair bra, ket;
       if (run) {
         ket = prm.pp[job.pkl_off + kl];
         bra = prm.pp[job.pij_off + ij];
-        if constexpr (MODE == 0) {
-          if (++ij == nbk) {
-            ij = 0;
-            ++kl;
-            if (p + 1 < np) {
-              const double kc = prm.pp[job.pkl_off + kl].cce;
-              while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
-            }
+        if (++ij == nbk) {
+          ij = 0;
+          ++kl;
+          if (p + 1 < np) {
+            const double kc = prm.pp[job.pkl_off + kl].cce;
+            while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
           }
-        } else {
-          // screening (reference src/cint2e.rs:367-393)
-          run = !(ket.cce > cut) && !(bra.cce > cut - ket.cce);
-          if (++ij == job.nij) { ij = 0; ++kl; }
         }
       }
-      R aij = 1, akl = 1, inv = 1, fac1 = 0, x = 0;
+      R aij = 1, akl = 1, inv = 1, fac1 = 0;
       R pq[3] = {0, 0, 0};
+      double x = 0.0;
       if (run) {
         if constexpr (sizeof(R) == 8) {
           aij = bra.a; akl = ket.a;
           inv = 1.0 / (aij + akl);
           fac1 = sqrt(inv) * bra.facia * ket.facia;
           pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
+          x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
         } else {
-          // FP32 prefactors: differences of the FP64 pair data are formed in
-          // FP64 (cancellation), the rest in FP32
+          // FP32 prefactors; differences of the FP64 pair data are formed in
+          // FP64 (cancellation).  x stays FP64: the Rys weights' relative
+          // sensitivity to x grows with x, so an FP32 x would cost ~x * 1e-7
+          // relative; the FP32 reciprocal refined by one Newton step replaces
+          // the FP64 division.
           aij = (R)bra.a; akl = (R)ket.a;
           inv = 1.0f / (aij + akl);
           fac1 = sqrtf(inv) * (R)(bra.facia * ket.facia);
-          pq[0] = (R)(bra.px - ket.px); pq[1] = (R)(bra.py - ket.py); pq[2] = (R)(bra.pz - ket.pz);
+          const double dx = bra.px - ket.px, dy = bra.py - ket.py, dz = bra.pz - ket.pz;
+          pq[0] = (R)dx; pq[1] = (R)dy; pq[2] = (R)dz;
+          const double sum = bra.a + ket.a;
+          double invd = (double)inv;
+          invd = fma(invd, fma(-sum, invd, 1.0), invd);
+          x = bra.a * ket.a * invd * (dx * dx + dy * dy + dz * dz);
         }
-        x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
         for (int f = rho; f < 2 * C::NR; f += C::LANES) {
           R v;
           if constexpr (sizeof(R) == 8) v = rys_function<C::NR>(tab, x, f);

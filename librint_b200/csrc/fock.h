@@ -17,7 +17,8 @@ struct MolCtx {
   double *env = nullptr, *Q = nullptr, *Dsh = nullptr;
   double *centers = nullptr;   // 3 doubles per shell
   PairInfo *pairs = nullptr;
-  PrimPair *pp = nullptr;
+  PrimPair *pp = nullptr;    // primitive pairs of each table pair, ip fastest
+  PrimPair *pps = nullptr;   // the same, each pair's entries by ascending cce
   // pairs by descending Schwarz factor: qorder[position] = pair, Qs = Q sorted;
   // per-position candidate counts / offsets and the density maximum of a build
   int *qorder = nullptr, *qcnt = nullptr;
@@ -39,6 +40,7 @@ struct ScfOptions {
   double fp32_until = 1e-3;   // all-FP32 builds while ||dP|| is above this
   double tau32 = 1e-7;     // afterwards FP32 only for bounds below this
   int rebuild_every = 6;   // full (non-incremental) build period
+  double tau_fp32 = 0.0;   // screening of the FP32 / split builds (0: tau)
 };
 
 struct ScfResult {

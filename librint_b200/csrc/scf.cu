@@ -280,13 +280,16 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
       const int want = !fp32_done ? 1 : (fp64_final ? 0 : 2);
       const bool full = want != phase || since_full >= o.rebuild_every;
       if (want != phase && phase >= 0) nd = 0;   // DIIS restarts with the new operator
+      // the FP32 phases screen at tau_fp32: their G carries the FP32 error
+      // already, and the FP64 phase starts with a full build at tau
+      const double tau_b = want == 0 ? o.tau : std::max(o.tau, o.tau_fp32);
       if (full) {
-        if ((rc = fock_build(m, P, Gc, o.tau, st, &fs, want, o.tau32, false))) return rc;
+        if ((rc = fock_build(m, P, Gc, tau_b, st, &fs, want, o.tau32, false))) return rc;
         since_full = 0;
         phase = want;
       } else {
         k_axpby<<<gb, 256, 0, st>>>(P, Pb, dPm, 1.0, -1.0, nn);
-        if ((rc = fock_build(m, dPm, Gc, o.tau, st, &fs, phase, o.tau32, true))) return rc;
+        if ((rc = fock_build(m, dPm, Gc, tau_b, st, &fs, phase, o.tau32, true))) return rc;
         ++since_full;
       }
       cudaMemcpyAsync(Pb, P, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);

@@ -72,15 +72,17 @@ class MolContext:
 
     def scf(self, nelec=None, max_iter=100, conv=1e-10, guess=0, diis=0, tau=0.0, P0=None,
             return_density=False, mixed=0, fp32_until=1e-3, tau32=1e-7, rebuild_every=6,
-            check=True):
+            check=True, tau_fp32=0.0):
         """RHF.  Defaults are the reference's algorithm (P0 = I, plain
         Roothaan, FP64, no screening); guess=1 / diis / tau / mixed select
         the faster schedules, which change iterations and time, not the
         converged energy (mixed: within the tolerance stated in the tests).
         check=False returns a non-converged result (``r.converged`` 0)
-        instead of raising."""
+        instead of raising.  tau_fp32 (mixed only) is the screening threshold
+        of the FP32 and split builds; the FP64 phase screens at tau."""
         nelec = self.m.nelec if nelec is None else nelec
-        o = B.ScfOptions(max_iter, conv, guess, diis, tau, mixed, fp32_until, tau32, rebuild_every)
+        o = B.ScfOptions(max_iter, conv, guess, diis, tau, mixed, fp32_until, tau32, rebuild_every,
+                         tau_fp32)
         r = B.ScfResult()
         P = np.empty((self.nao, self.nao))
         p0 = None if P0 is None else np.ascontiguousarray(P0, dtype=np.float64).ctypes.data_as(B.P_d)

@@ -126,13 +126,13 @@ def test_rys_tables_vs_exact():
 
 
 def _rys_f32_eval(tab, off, n, x):
-    """Float evaluation of rys_tables_f32.h at x (as rys_function_f32)."""
-    x = np.float32(x)
-    if x >= np.float32(43.0 + 5.0 * n):
+    """Float evaluation of rys_tables_f32.h at x (as rys_function_f32: x and
+    the local variable in FP64, t rounded to float, float Horner)."""
+    if x >= 43.0 + 5.0 * n:
         return None
     nseg = (43 + 5 * n + 3) // 4
-    seg = min(max(int(x * np.float32(0.25)), 0), nseg - 1)
-    t = np.float32((x - np.float32(seg * 4.0 + 2.0)) * np.float32(0.5))
+    seg = min(max(int(x * 0.25), 0), nseg - 1)
+    t = np.float32((x - (seg * 4.0 + 2.0)) * 0.5)
     out = []
     for f in range(2 * n):
         c = tab[off[n] + (seg * 2 * n + f) * 11: off[n] + (seg * 2 * n + f + 1) * 11]
@@ -168,7 +168,7 @@ def test_rys_tables_f32_vs_oracle():
         xs = np.concatenate([[0.0, 1e-6, 3.999, 4.0, 42.9 + 5 * n], rng.uniform(0, 43 + 5 * n, 40)])
         for x in xs:
             u32, w32 = _rys_f32_eval(tab, off, n, x)
-            u, w = oracle.rys_roots(n, float(np.float32(x)))
+            u, w = oracle.rys_roots(n, float(x))
             np.testing.assert_allclose(u32, u, rtol=1.5e-6, err_msg=f"n={n} x={x}")
             np.testing.assert_allclose(w32, w, rtol=1.5e-6, err_msg=f"n={n} x={x}")
 
