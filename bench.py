@@ -454,13 +454,21 @@ def main():
         dist.destroy_process_group()
 
 
+# Screening threshold of the FP32 SCF phases (hc_cluster, learned + mixed):
+# 1e-12 -> 2.14x, 1e-11 -> 2.33x, 1e-10 -> 2.18x (more iterations), 1e-9 ->
+# 1.22x over plain FP64; every setting ends at the FP64 energy to 2e-11 Eh.
+TAU_FP32 = 1e-11
+
+
 def run_rhf(guess_file=None):
     """RHF wall time on the C/H flake (hc_cluster: 34 C + 20 H, 610 cartesian
     AOs, DZP-like basis).
 
     reference: FP64, core-H guess, DIIS(8), Schwarz 1e-13, ||dP||/2 <= 1e-8;
     plain:     the same schedule stopped at 1e-5 (the FP64 GPU path);
-    mixed:     incremental Fock builds with FP32 quartets, same stop;
+    mixed:     incremental Fock builds with FP32 quartets, same stop; the
+               FP32 phases screen at tau_fp32 = 1e-11 (the FP64 phase at
+               1e-13, after a full rebuild);
     learned:   mixed, started from the learned guess when its network applies
                to this basis (otherwise absent).
     Energies are compared with the reference run; times exclude the one-off
@@ -486,7 +494,7 @@ def run_rhf(guess_file=None):
                      % (ctx.nao, mol.nbas, mol.nelec), "setup_s": setup}
     out["reference"] = run("reference", 1e-8)
     out["plain"] = run("plain", 1e-5)
-    out["mixed"] = run("mixed", 1e-5, mixed=1)
+    out["mixed"] = run("mixed", 1e-5, mixed=1, tau_fp32=TAU_FP32)
     if guess_file and os.path.exists(guess_file):
         from librint_b200.guess import LearnedGuess
         g = LearnedGuess.load(guess_file)
@@ -496,7 +504,8 @@ def run_rhf(guess_file=None):
             P0 = g.predict(mol, S=S_ov)
             t_pred = (time.perf_counter() - tp) * 1e3
             out["learned_fp64"] = run("learned_fp64", 1e-5, P0=P0, extra_ms=t_pred)
-            out["learned_mixed"] = run("learned_mixed", 1e-5, P0=P0, extra_ms=t_pred, mixed=1)
+            out["learned_mixed"] = run("learned_mixed", 1e-5, P0=P0, extra_ms=t_pred, mixed=1,
+                                       tau_fp32=TAU_FP32)
             out["predict_ms"] = t_pred
     e_ref = out["reference"]["energy"]
     for k in ("plain", "mixed", "learned_fp64", "learned_mixed"):

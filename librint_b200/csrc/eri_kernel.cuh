@@ -10,7 +10,8 @@
 //     l, as src/g2e.rs:113-181 chooses -- then shifts it to the partners by
 //     the horizontal recurrences on these 1D arrays, giving G[a][b][c][d];
 //   * gout: every lane owns one row of the final cartesian block (the smaller
-//     of the bra/ket sides) and accumulates all columns in registers:
+//     of the bra/ket sides, but the bra of (dd|ps), (dd|pp), (dd|dp)) and
+//     accumulates all columns in registers:
 //     I(row, col) += Gx Gy Gz (src/cint2e.rs:2456-2895).
 // The recurrences stay per primitive (as the reference does) because shifting
 // after contraction acts on 3D products and loses ~2 digits for distant
@@ -37,7 +38,14 @@ struct EriClass {
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
   static constexpr int NI = ncart(LI), NJ = ncart(LJ), NK = ncart(LK), NL = ncart(LL);
   static constexpr int NBRA = NI * NJ, NKET = NK * NL;
-  static constexpr bool ROWKET = NKET <= NBRA;          // rows are ket components
+  // Rows are the smaller side, except (dd|ps), (dd|pp) and (dd|dp) of the
+  // ERI / Fock kernels (PACK), which run 36 bra rows (32 lanes plus split
+  // extras) against ket columns: measured on the K = 1..6 sweep, 17 %, 38 %
+  // and 4.5 % faster than 3, 9 or 18 ket rows (fewer accumulators per lane,
+  // one round of (root, axis) units over 32 lanes).
+  static constexpr bool BRA_ROWS =
+      PACK && LI_ == 2 && LJ_ == 2 && ((LK_ == 1 && LL_ <= 1) || (LK_ == 2 && LL_ == 1));
+  static constexpr bool ROWKET = !BRA_ROWS && NKET <= NBRA;   // rows are ket components
   static constexpr int NROWS = ROWKET ? NKET : NBRA;
   static constexpr int NCOLS = ROWKET ? NBRA : NKET;
   // Lanes per slot.  Each of the LANES lanes owns one row; rows beyond LANES
@@ -104,7 +112,7 @@ struct EriClass {
 template <class C, int MODE = 0, typename R = double>
 struct EriLayout {
   static constexpr int NKO_MAX = C::NKET;   // cartesian >= spherical
-  // per-slot sizes in doubles: roots, weights, 1/(1+u) (3 NR, type R), then G
+  // per-slot sizes in doubles: roots, weights, 1/(1+u) (3 NR, FP64), then G
   // (NR*3*GSZ) and per-unit bra-shift scratch (3*NR*TSZ) in the arithmetic
   // type R in the loop; block (NBRA*NKET, R) + ket-transformed block
   // (NBRA*NKO, output mode only) in the epilogue.  FP32 halves the R parts.
@@ -312,7 +320,7 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
   const bool lane_live = slot < C::SLOTS;
   const int myslot = lane_live ? slot : C::SLOTS - 1;
   double *sb = wbuf + myslot * L::SLOT;        // this slot's area
-  R *RW = reinterpret_cast<R *>(sb);           // [3*NR] roots, weights, 1/(1+u)
+  double *RW = sb;                             // [3*NR] FP64 roots, weights, 1/(1+u)
   R *G = reinterpret_cast<R *>(sb + 3 * C::NR);            // [NR][3][GSZ]
   R *Tsc = G + C::NR * 3 * C::GSZ;                         // [3*NR][TSZ]
 
@@ -459,38 +467,26 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
           }
         }
       }
-      R aij = 1, akl = 1, inv = 1, fac1 = 0;
-      R pq[3] = {0, 0, 0};
-      double x = 0.0;
+      // Prefactors and the per-unit coefficients are FP64 in both variants
+      // and rounded once to R at the recurrence; the FP32 variant takes its
+      // roots and weights from the economised FP32 tables (x stays FP64, so
+      // the table sees a ~1e-7 absolute error in its local variable).  FP32
+      // prefactors and coefficients were measured to raise the FP32 G error
+      // about 4x (1.2e-5 vs 3.1e-6 on a 120-AO ring).
+      double aij = 1.0, akl = 1.0, inv = 1.0, fac1 = 0.0, x = 0.0;
+      double pq[3] = {0, 0, 0};
       if (run) {
-        if constexpr (sizeof(R) == 8) {
-          aij = bra.a; akl = ket.a;
-          inv = 1.0 / (aij + akl);
-          fac1 = sqrt(inv) * bra.facia * ket.facia;
-          pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
-          x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
-        } else {
-          // FP32 prefactors; differences of the FP64 pair data are formed in
-          // FP64 (cancellation).  x stays FP64: the Rys weights' relative
-          // sensitivity to x grows with x, so an FP32 x would cost ~x * 1e-7
-          // relative; the FP32 reciprocal refined by one Newton step replaces
-          // the FP64 division.
-          aij = (R)bra.a; akl = (R)ket.a;
-          inv = 1.0f / (aij + akl);
-          fac1 = sqrtf(inv) * (R)(bra.facia * ket.facia);
-          const double dx = bra.px - ket.px, dy = bra.py - ket.py, dz = bra.pz - ket.pz;
-          pq[0] = (R)dx; pq[1] = (R)dy; pq[2] = (R)dz;
-          const double sum = bra.a + ket.a;
-          double invd = (double)inv;
-          invd = fma(invd, fma(-sum, invd, 1.0), invd);
-          x = bra.a * ket.a * invd * (dx * dx + dy * dy + dz * dz);
-        }
+        aij = bra.a; akl = ket.a;
+        inv = 1.0 / (aij + akl);
+        fac1 = sqrt(inv) * bra.facia * ket.facia;
+        pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
+        x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
         for (int f = rho; f < 2 * C::NR; f += C::LANES) {
-          R v;
+          double v;
           if constexpr (sizeof(R) == 8) v = rys_function<C::NR>(tab, x, f);
-          else v = rys_function_f32<C::NR>(tab32, x, f);
+          else v = (double)rys_function_f32<C::NR>(tab32, x, f);
           RW[f] = v;
-          if (f < C::NR) RW[2 * C::NR + f] = (R)1 / ((R)1 + v);   // t^2 complement 1/(1+u)
+          if (f < C::NR) RW[2 * C::NR + f] = 1.0 / (1.0 + v);   // t^2 complement 1/(1+u)
         }
       }
       __syncwarp();
@@ -503,22 +499,22 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
           const int u = rho + k * C::LANES;
           if (u >= 3 * C::NR) break;
           const int r = u / 3, ax = u - 3 * r;
-          const R pa = (R)pick3(bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2], ax);
-          const R qc = (R)pick3(ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2], ax);
-          const R pqa = pick3(pq[0], pq[1], pq[2], ax);
-          const R ab = (R)pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
-          const R cd = (R)pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
+          const double pa = pick3(bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2], ax);
+          const double qc = pick3(ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2], ax);
+          const double pqa = pick3(pq[0], pq[1], pq[2], ax);
+          const double ab = pick3(rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2], ax);
+          const double cd = pick3(rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2], ax);
           // with d = 1/(1+u): B00 = u d / (2 (aij+akl)), B10 = B00 + d / (2 aij),
           // B01 = B00 + d / (2 akl) (u2 (aij+akl) + aij akl = aij akl (1+u))
-          const R d = RW[2 * C::NR + r];
-          const R tmp5 = (R)0.5 * inv * RW[r] * d;
-          const R b10 = tmp5 + (R)0.5 * (R)bra.ia * d;
-          const R b01 = tmp5 + (R)0.5 * (R)ket.ia * d;
-          const R cn = pa - (R)2 * tmp5 * akl * pqa;
-          const R cm = qc + (R)2 * tmp5 * aij * pqa;
-          const R v00 = ax == 2 ? RW[C::NR + r] * fac1 : (R)1;
-          vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, v00, cn, cm, b10, b01,
-                             tmp5, ab, cd);
+          const double d = RW[2 * C::NR + r];
+          const double tmp5 = 0.5 * inv * RW[r] * d;
+          const double b10 = tmp5 + 0.5 * bra.ia * d;
+          const double b01 = tmp5 + 0.5 * ket.ia * d;
+          const double cn = pa - 2.0 * tmp5 * akl * pqa;
+          const double cm = qc + 2.0 * tmp5 * aij * pqa;
+          const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;
+          vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, (R)v00, (R)cn, (R)cm,
+                             (R)b10, (R)b01, (R)tmp5, (R)ab, (R)cd);
         }
       }
       __syncwarp();

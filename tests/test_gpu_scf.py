@@ -135,13 +135,17 @@ def test_fp32_fock_build_error(golden, which):
 @pytest.mark.parametrize("which", ["ring", "h2o/def2svp"])
 def test_mixed_scf_matches_fp64(golden, which):
     """The mixed schedule ends with FP64 builds, so it converges to the FP64
-    energy (1e-9 Eh) at the same density threshold."""
+    energy (1e-9 Eh) at the same density threshold, also when its FP32
+    phases screen at the looser tau_fp32 the RHF benchmark uses."""
     m = _ring() if which == "ring" else Molecule(
         golden["mol/h2o/def2svp/atm"], golden["mol/h2o/def2svp/bas"],
         golden["mol/h2o/def2svp/env"], 10)
     ctx = scf.MolContext(m)
     r64 = ctx.scf(conv=1e-8, guess=1, diis=8, tau=1e-13)
     rmx = ctx.scf(conv=1e-8, guess=1, diis=8, tau=1e-13, mixed=1)
+    rlo = ctx.scf(conv=1e-8, guess=1, diis=8, tau=1e-13, mixed=1, tau_fp32=1e-11)
     ctx.close()
     assert rmx.converged and rmx.fp32_quartets > 0
     assert abs(rmx.energy - r64.energy) < 1e-9, (rmx.energy, r64.energy)
+    assert rlo.converged and rlo.quartets < rmx.quartets
+    assert abs(rlo.energy - r64.energy) < 1e-9, (rlo.energy, r64.energy)
