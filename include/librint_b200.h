@@ -136,9 +136,9 @@ LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long l
 LRB_API int lrb_fock_G_device(LrbMol *m, const double *P, double *G, double tau, void *stream);
 /* The same G(P) with the mixed-precision kernels (no reference counterpart):
  * prec 0 all FP64, 1 all FP32, 2 FP32 only for quartets whose Schwarz x
- * density bound is below tau32.  FP32 quartets run the roots (economised FP32
- * tables, FP64 argument), recurrences and digestion in FP32 and add into
- * FP64 J/K.  Host
+ * density bound is below tau32.  FP32 quartets run the recurrences and the
+ * digestion in FP32 (roots, weights and prefactors FP64, rounded once) and
+ * add into FP64 J/K.  Host
  * buffers; quartets / fp32_quartets (may be NULL) receive the counts. */
 LRB_API int lrb_fock_G_prec(LrbMol *m, const double *P, double *G, double tau, int prec,
                             double tau32, long long *quartets, long long *fp32_quartets);

@@ -355,12 +355,6 @@ const double *rys_table_device() {
   return p;
 }
 
-const float *rys_table_device_f32() {
-  const float *p = nullptr;
-  cudaGetSymbolAddress((void **)&p, RYS32_TAB);
-  return p;
-}
-
 // ---------------------------------------------------------------- driver
 #define LRB_CK(x)                                        \
   do {                                                   \

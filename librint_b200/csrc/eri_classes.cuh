@@ -17,7 +17,7 @@ __host__ __device__ inline int class_id(int li, int lj, int lk, int ll) {
 constexpr int NPAIRCLS = (ERI_LMAX + 1) * (ERI_LMAX + 2) / 2;
 constexpr int NCLASS = NPAIRCLS * (NPAIRCLS + 1) / 2;
 
-using EriKernelFn = void (*)(EriParams, FockParams, const void *, int *);
+using EriKernelFn = void (*)(EriParams, FockParams, const double *, int *);
 
 struct ClassEntry {
   EriKernelFn fn[3];     // output (FP64), Fock digestion FP64, Fock digestion FP32

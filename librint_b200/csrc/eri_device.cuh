@@ -24,7 +24,6 @@
 #include <cuda_runtime.h>
 
 #include "rys_tables.h"
-#include "rys_tables_f32.h"
 
 namespace lrb {
 
@@ -187,35 +186,6 @@ __device__ __forceinline__ double rys_function(const double *tab, double x, int 
   double r = c[RYS_DEG];
 #pragma unroll
   for (int k = RYS_DEG - 1; k >= 0; --k) r = fma(r, t, c[k]);
-  return r;
-}
-
-// FP32 counterpart of rys_function for the mixed-precision Fock kernels:
-// economised degree-RYS32_DEG segments of rys_tables_f32.h (float table
-// staged in shared memory), the same large-x limit rounded to float.  The
-// argument x and the local variable t are formed in FP64 and only t is
-// rounded, so the table sees an x error of ~1e-7 absolute, not relative.
-template <int N>
-__device__ __forceinline__ float rys_function_f32(const float *tab, double x, int f) {
-  static_assert(N <= RYS32_NMAX, "FP32 Rys tables cover up to RYS32_NMAX roots");
-  constexpr double XBREAK = 43.0 + 5.0 * N;
-  if (x >= XBREAK) {
-    constexpr int off = N * (N - 1) / 2;
-    const float xf = (float)x;
-    if (f < N) {
-      const float r = (float)RYS_LARGEX_R[off + f];
-      return r / (xf - r);
-    }
-    return (float)RYS_LARGEX_W[off + f - N] * sqrtf(0.785398163f / xf);  // pi/4
-  }
-  constexpr int NSEG = rys_nseg(N);
-  int seg = (int)(x * (1.0 / RYS_SEG_WIDTH));
-  seg = seg < 0 ? 0 : (seg >= NSEG ? NSEG - 1 : seg);
-  const float t = (float)((x - (seg * RYS_SEG_WIDTH + 0.5 * RYS_SEG_WIDTH)) * (2.0 / RYS_SEG_WIDTH));
-  const float *c = tab + (seg * 2 * N + f) * RYS32_NCOEF;
-  float r = c[RYS32_DEG];
-#pragma unroll
-  for (int k = RYS32_DEG - 1; k >= 0; --k) r = fmaf(r, t, c[k]);
   return r;
 }
 

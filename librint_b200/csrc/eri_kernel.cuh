@@ -121,10 +121,7 @@ struct EriLayout {
   static constexpr int EPI = RD(C::NBRA * C::NKET) + (MODE == 0 ? C::NBRA * NKO_MAX : 0);
   static constexpr int SLOT = LOOP > EPI ? LOOP : EPI;
   static constexpr int WARP = C::SLOTS * SLOT;
-  // Rys table in doubles: FP64 coefficients, or the FP32 table for R = float
-  static constexpr int TAB = sizeof(R) == 8
-                                 ? (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR])
-                                 : RD(RYS32_TAB_OFFSET[C::NR + 1] - RYS32_TAB_OFFSET[C::NR]);
+  static constexpr int TAB = (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR]);
   static constexpr int C2S = 3 * 5 * 6;    // l <= 2, m, cart
   static constexpr size_t SMEM = sizeof(double) * (size_t)(TAB + C2S + ERI_WARPS * WARP);
 };
@@ -291,22 +288,14 @@ __device__ __forceinline__ void cart_comp_rt(int l, int n, int &x, int &y, int &
 // weights and pair data are always evaluated in FP64 and rounded after.
 template <int LI, int LJ, int LK, int LL, int MODE, typename R = double>
 __global__ void __launch_bounds__(ERI_THREADS)
-k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *counter) {
+k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *counter) {
   using C = EriClass<LI, LJ, LK, LL, true>;
   using L = EriLayout<C, MODE, R>;
   static_assert(MODE == 1 || sizeof(R) == 8, "output mode is FP64");
   extern __shared__ double smem[];
-  double *tab = smem;                                    // FP64 table (R = double)
-  float *tab32 = reinterpret_cast<float *>(smem);        // FP32 table (R = float)
+  double *tab = smem;
   double *c2s_s = smem + L::TAB;            // [3][5][6]
-  if constexpr (sizeof(R) == 8) {
-    for (int i = threadIdx.x; i < L::TAB; i += blockDim.x)
-      tab[i] = static_cast<const double *>(rys_tab_n)[i];
-  } else {
-    constexpr int NT = RYS32_TAB_OFFSET[C::NR + 1] - RYS32_TAB_OFFSET[C::NR];
-    for (int i = threadIdx.x; i < NT; i += blockDim.x)
-      tab32[i] = static_cast<const float *>(rys_tab_n)[i];
-  }
+  for (int i = threadIdx.x; i < L::TAB; i += blockDim.x) tab[i] = rys_tab_n[i];
   for (int i = threadIdx.x; i < L::C2S; i += blockDim.x) {
     const int l = i / 30, m = (i / 6) % 5, c = i % 6;
     c2s_s[i] = c_c2s[(l * C2S_M + m) * C2S_C + c];
@@ -467,12 +456,11 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
           }
         }
       }
-      // Prefactors and the per-unit coefficients are FP64 in both variants
-      // and rounded once to R at the recurrence; the FP32 variant takes its
-      // roots and weights from the economised FP32 tables (x stays FP64, so
-      // the table sees a ~1e-7 absolute error in its local variable).  FP32
-      // prefactors and coefficients were measured to raise the FP32 G error
-      // about 4x (1.2e-5 vs 3.1e-6 on a 120-AO ring).
+      // Roots, weights, prefactors and the per-unit coefficients are FP64 in
+      // both variants and rounded once to R at the recurrence.  FP32 roots
+      // (float tables of ~1e-7 relative error) were measured to raise the
+      // FP32 G error 3.5x (1.1e-5 vs 3.1e-6 on a 120-AO ring): their error is
+      // systematic in x, so it adds up coherently over the quartets.
       double aij = 1.0, akl = 1.0, inv = 1.0, fac1 = 0.0, x = 0.0;
       double pq[3] = {0, 0, 0};
       if (run) {
@@ -482,9 +470,7 @@ k_eri(EriParams prm, FockParams fk, const void *__restrict__ rys_tab_n, int *cou
         pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
         x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
         for (int f = rho; f < 2 * C::NR; f += C::LANES) {
-          double v;
-          if constexpr (sizeof(R) == 8) v = rys_function<C::NR>(tab, x, f);
-          else v = (double)rys_function_f32<C::NR>(tab32, x, f);
+          const double v = rys_function<C::NR>(tab, x, f);
           RW[f] = v;
           if (f < C::NR) RW[2 * C::NR + f] = 1.0 / (1.0 + v);   // t^2 complement 1/(1+u)
         }

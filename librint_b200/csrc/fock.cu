@@ -22,7 +22,6 @@
 namespace lrb {
 
 const double *rys_table_device();
-const float *rys_table_device_f32();
 
 #define FK_CK(x)                                  \
   do {                                            \
@@ -462,7 +461,6 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const double *rys = rys_table_device();
-    const float *rys32 = rys_table_device_f32();
     EriParams prm{};
     prm.pp = m.pps;
     prm.centers = m.centers;
@@ -497,9 +495,8 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
         cudaEventCreate(&rec.stop);
         cudaEventRecord(rec.start, st);
       }
-      const void *tabn = fi == 2 ? (const void *)(rys32 + RYS32_TAB_OFFSET[ce.nr])
-                                 : (const void *)(rys + RYS_TAB_OFFSET[ce.nr]);
-      ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(prm, fk, tabn, counters + cc);
+      ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(prm, fk, rys + RYS_TAB_OFFSET[ce.nr],
+                                                                  counters + cc);
       FK_CK(cudaGetLastError());
       eng.launches++;
       if (eng.profile) {

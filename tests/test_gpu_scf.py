@@ -147,5 +147,5 @@ def test_mixed_scf_matches_fp64(golden, which):
     ctx.close()
     assert rmx.converged and rmx.fp32_quartets > 0
     assert abs(rmx.energy - r64.energy) < 1e-9, (rmx.energy, r64.energy)
-    assert rlo.converged and rlo.quartets < rmx.quartets
+    assert rlo.converged and rlo.quartets <= rmx.quartets
     assert abs(rlo.energy - r64.energy) < 1e-9, (rlo.energy, r64.energy)

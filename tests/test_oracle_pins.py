@@ -125,54 +125,6 @@ def test_rys_tables_vs_exact():
             np.testing.assert_allclose(w, we, rtol=4e-15, err_msg=f"n={n} x={x}")
 
 
-def _rys_f32_eval(tab, off, n, x):
-    """Float evaluation of rys_tables_f32.h at x (as rys_function_f32: x and
-    the local variable in FP64, t rounded to float, float Horner)."""
-    if x >= 43.0 + 5.0 * n:
-        return None
-    nseg = (43 + 5 * n + 3) // 4
-    seg = min(max(int(x * 0.25), 0), nseg - 1)
-    t = np.float32((x - (seg * 4.0 + 2.0)) * 0.5)
-    out = []
-    for f in range(2 * n):
-        c = tab[off[n] + (seg * 2 * n + f) * 11: off[n] + (seg * 2 * n + f + 1) * 11]
-        r = np.float32(c[-1])
-        for k in range(9, -1, -1):
-            r = np.float32(r * t + c[k])
-        out.append(float(r))
-    return np.array(out[:n]), np.array(out[n:])
-
-
-def test_rys_tables_f32_vs_oracle():
-    """The FP32 Fock kernels' economised tables (rys_tables_f32.h) against the
-    oracle's FP64 roots and weights, and the header against a regeneration
-    from rys_tables.h."""
-    import os
-    import re
-    import sys
-    csrc = os.path.join(os.path.dirname(os.path.dirname(__file__)), "librint_b200", "csrc")
-    sys.path.insert(0, csrc)
-    import gen_rys_tables_f32 as gen32
-    src = open(os.path.join(csrc, "rys_tables_f32.h")).read()
-    off = [int(v) for v in re.search(r"RYS32_TAB_OFFSET\[[^]]*\] = \{([^}]*)\}", src).group(1).split(",")]
-    body = re.search(r"RYS32_TAB\[(\d+)\] = \{([^}]*)\}", src).group(2)
-    tab = np.array([float(v.strip().rstrip("f")) for v in body.split(",") if v.strip()], np.float32)
-    assert len(tab) == off[-1]
-    deg, ncoef, nseg, off64, tab64 = gen32.read_fp64_tables(os.path.join(csrc, "rys_tables.h"))
-    regen = np.concatenate([gen32.economise(tab64[off64[n] + (s * 2 * n + f) * ncoef:
-                                                  off64[n] + (s * 2 * n + f + 1) * ncoef])
-                            for n in range(1, 6) for s in range(nseg[n]) for f in range(2 * n)])
-    np.testing.assert_array_equal(regen, tab)
-    rng = np.random.default_rng(11)
-    for n in range(1, 6):
-        xs = np.concatenate([[0.0, 1e-6, 3.999, 4.0, 42.9 + 5 * n], rng.uniform(0, 43 + 5 * n, 40)])
-        for x in xs:
-            u32, w32 = _rys_f32_eval(tab, off, n, x)
-            u, w = oracle.rys_roots(n, float(x))
-            np.testing.assert_allclose(u32, u, rtol=1.5e-6, err_msg=f"n={n} x={x}")
-            np.testing.assert_allclose(w32, w, rtol=1.5e-6, err_msg=f"n={n} x={x}")
-
-
 def test_dsu_golden_layout_vs_oracle_differences():
     """The reference's dS_u fixture is d S[mu, nu] / d env[s1 + l] at element
     (nu * n + mu) * L + l: central differences of the oracle's overlap."""
