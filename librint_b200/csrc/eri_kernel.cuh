@@ -396,14 +396,16 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
       if (pk.ish == pk.jsh) wdeg *= 0.5;
       if (jb.x == jb.y) wdeg *= 0.5;
     }
-    // Primitive quartets to visit.  Each shell pair's primitive pairs are
-    // sorted by ascending screening key cce, so for ket pair kl the bra pairs
-    // that pass (bra.cce <= cutoff - ket.cce, reference src/cint2e.rs:367-393)
-    // are a prefix of length nb(kl), non-increasing in kl; only those are
-    // visited.
+    // Primitive quartets to visit.  Output mode: each shell pair's primitive
+    // pairs are sorted by ascending screening key cce, so for ket pair kl the
+    // bra pairs that pass (bra.cce <= cutoff - ket.cce) are a prefix of
+    // length nb(kl), non-increasing in kl; only those are visited.  Fock mode
+    // keeps the pairs in natural order and tests each quartet: a cce-sorted
+    // walk adds the largest contributions to the FP32 accumulators first and
+    // was measured to raise the FP32 G error 3.5x, at no gain in time.
     const double cut = prm.expcutoff;
     int np = 0;
-    {
+    if constexpr (MODE == 0) {
       int nb = job.nij;
       for (int k = 0; k < job.nkl; ++k) {
         const double kc = prm.pp[job.pkl_off + k].cce;
@@ -412,6 +414,8 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
         if (nb == 0) break;
         np += nb;
       }
+    } else {
+      np = job.nij * job.nkl;
     }
     int npmax = np;
 #pragma unroll
@@ -436,31 +440,36 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
     for (int k = 0; k < (C::NEX > 0 ? C::NEX : 1); ++k) xacc[k] = 0;
 
     int ij = 0, kl = 0;
-    int nbk = job.nij;   // passing bra prefix of the current ket pair
-    if (np > 0) {
-      const double kc = prm.pp[job.pkl_off].cce;
-      while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
+    int nbk = job.nij;   // output mode: passing bra prefix of the current ket pair
+    if constexpr (MODE == 0) {
+      if (np > 0) {
+        const double kc = prm.pp[job.pkl_off].cce;
+        while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
+      }
     }
     for (int p = 0; p < npmax; ++p) {
-      const bool run = p < np;
+      bool run = p < np;
       PrimPair bra, ket;
       if (run) {
         ket = prm.pp[job.pkl_off + kl];
         bra = prm.pp[job.pij_off + ij];
-        if (++ij == nbk) {
-          ij = 0;
-          ++kl;
-          if (p + 1 < np) {
-            const double kc = prm.pp[job.pkl_off + kl].cce;
-            while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
+        if constexpr (MODE == 0) {
+          if (++ij == nbk) {
+            ij = 0;
+            ++kl;
+            if (p + 1 < np) {
+              const double kc = prm.pp[job.pkl_off + kl].cce;
+              while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
+            }
           }
+        } else {
+          // screening (reference src/cint2e.rs:367-393)
+          run = !(ket.cce > cut) && !(bra.cce > cut - ket.cce);
+          if (++ij == job.nij) { ij = 0; ++kl; }
         }
       }
       // Roots, weights, prefactors and the per-unit coefficients are FP64 in
-      // both variants and rounded once to R at the recurrence.  FP32 roots
-      // (float tables of ~1e-7 relative error) were measured to raise the
-      // FP32 G error 3.5x (1.1e-5 vs 3.1e-6 on a 120-AO ring): their error is
-      // systematic in x, so it adds up coherently over the quartets.
+      // both variants and rounded once to R at the recurrence.
       double aij = 1.0, akl = 1.0, inv = 1.0, fac1 = 0.0, x = 0.0;
       double pq[3] = {0, 0, 0};
       if (run) {

@@ -38,26 +38,6 @@ __device__ inline double fac_sp_d(int l) {
   return l == 0 ? 0.28209479177387814 : (l == 1 ? 0.48860251190291992 : 1.0);
 }
 
-// One warp per table pair: its primitive pairs ordered by ascending
-// screening key (NaN last, ties by position), so the Fock kernels visit only
-// the passing prefix of every bra for a given ket.
-__global__ void k_sort_mol_pairs(const PairInfo *__restrict__ pairs, int npairs,
-                                 const PrimPair *__restrict__ pp, PrimPair *__restrict__ pps) {
-  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= npairs) return;
-  const PairInfo pr = pairs[w];
-  for (int e = lane; e < pr.npp; e += 32) {
-    const double c = cce_key(pp[pr.pp_off + e].cce);
-    int rank = 0;
-    for (int u = 0; u < pr.npp; ++u) {
-      const double cu = cce_key(pp[pr.pp_off + u].cce);
-      rank += (cu < c) || (cu == c && u < e);
-    }
-    pps[pr.pp_off + rank] = pp[pr.pp_off + e];
-  }
-}
-
 // Primitive pairs of every table pair (one thread per primitive pair).
 // sqrt(2 pi^2.5) is folded into every pair so bra.fac * ket.fac carries the
 // class prefactor 2 pi^3 / sqrt(pi) (reference src/g2e.rs:74-82).
@@ -302,8 +282,7 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
   if (!al((void **)&m.atm, sizeof(int) * 6 * natm) || !al((void **)&m.bas, sizeof(int) * 8 * nbas) ||
       !al((void **)&m.env, sizeof(double) * nenv) || !al((void **)&m.aooff, sizeof(int) * (nbas + 1)) ||
       !al((void **)&m.pairs, sizeof(PairInfo) * m.npairs) || !al((void **)&m.pcls, sizeof(int) * m.npairs) ||
-      !al((void **)&m.pp, sizeof(PrimPair) * npp) || !al((void **)&m.pps, sizeof(PrimPair) * npp) ||
-      !al((void **)&m.Q, sizeof(double) * m.npairs) ||
+      !al((void **)&m.pp, sizeof(PrimPair) * npp) || !al((void **)&m.Q, sizeof(double) * m.npairs) ||
       !al((void **)&m.Dsh, sizeof(double) * nbas * nbas) ||
       !al((void **)&m.centers, sizeof(double) * 3 * nbas))
     return set_error("molecule: device allocation failed"), LRB_ERR_ALLOC;
@@ -321,9 +300,7 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
     FK_CK(cudaStreamSynchronize(st));   // cen goes out of scope
   }
   k_mol_pairs<<<(npp + 255) / 256, 256, 0, st>>>(m.pairs, m.npairs, m.atm, m.bas, m.env, m.pp, npp);
-  k_sort_mol_pairs<<<(unsigned)(((long long)m.npairs * 32 + 255) / 256), 256, 0, st>>>(m.pairs, m.npairs,
-                                                                                      m.pp, m.pps);
-  engine().launches += 2;
+  engine().launches++;
   FK_CK(cudaGetLastError());
   // Schwarz factors from (IJ|IJ) cartesian blocks
   std::vector<int> quart(4 * (size_t)m.npairs), dims(2 * (size_t)m.npairs);
@@ -378,7 +355,7 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
 
 void mol_destroy(MolCtx &m, cudaStream_t st) {
   for (void *p : {(void *)m.atm, (void *)m.bas, (void *)m.env, (void *)m.aooff, (void *)m.pairs,
-                  (void *)m.pcls, (void *)m.pp, (void *)m.pps, (void *)m.Q, (void *)m.Dsh, (void *)m.centers,
+                  (void *)m.pcls, (void *)m.pp, (void *)m.Q, (void *)m.Dsh, (void *)m.centers,
                   (void *)m.qorder, (void *)m.Qs, (void *)m.qcnt, (void *)m.qoff, (void *)m.dmax})
     if (p) cudaFreeAsync(p, st);
   cudaStreamSynchronize(st);
@@ -462,7 +439,7 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const double *rys = rys_table_device();
     EriParams prm{};
-    prm.pp = m.pps;
+    prm.pp = m.pp;
     prm.centers = m.centers;
     prm.expcutoff = eng.expcutoff;
     prm.sph = 0;

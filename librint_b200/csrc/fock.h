@@ -18,7 +18,6 @@ struct MolCtx {
   double *centers = nullptr;   // 3 doubles per shell
   PairInfo *pairs = nullptr;
   PrimPair *pp = nullptr;    // primitive pairs of each table pair, ip fastest
-  PrimPair *pps = nullptr;   // the same, each pair's entries by ascending cce
   // pairs by descending Schwarz factor: qorder[position] = pair, Qs = Q sorted;
   // per-position candidate counts / offsets and the density maximum of a build
   int *qorder = nullptr, *qcnt = nullptr;
