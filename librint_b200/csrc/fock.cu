@@ -148,8 +148,11 @@ __global__ void k_cand_count(const double *__restrict__ Qs, int npairs,
   cnt[i] = c;
 }
 
-// Screen the candidates (sorted positions i >= j) and append survivors; the
-// per-quartet test, precision choice and sort key are those of k_screen.
+// Screen the candidates (sorted positions i >= j) and append survivors: a
+// quartet is kept when Q_IJ Q_KL max(2|D_IJ|, 2|D_KL|, |D_IK|, |D_IL|,
+// |D_JK|, |D_JL|) >= tau, runs in FP32 for prec 1 (or prec 2 with the bound
+// below tau32), and is keyed by (precision, class, primitive count) for the
+// radix sort that groups the class launches.
 __global__ void k_screen_sorted(const PairInfo *__restrict__ pairs, const int *__restrict__ pcls,
                                 const double *__restrict__ Q, const int *__restrict__ qorder,
                                 const long long *__restrict__ qoff, int npairs,
