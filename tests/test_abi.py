@@ -35,3 +35,58 @@ def test_library_exports_every_declared_symbol():
 def test_bindings_load():
     L = B.lib()
     assert L.lrb_last_error() is not None
+
+
+_CTYPES = {"int": ctypes.c_int, "double": ctypes.c_double, "long long": ctypes.c_longlong,
+           "size_t": ctypes.c_size_t}
+
+
+def _header_struct(name):
+    """(field, ctype) list of `typedef struct {...} name;` in include/librint_b200.h."""
+    text = open(os.path.join(ROOT, "include", "librint_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = re.search(r"typedef struct \{([^}]*)\}\s*" + name + r"\s*;", text).group(1)
+    fields = []
+    for decl in body.split(";"):
+        decl = " ".join(decl.split())
+        if not decl:
+            continue
+        m = re.match(r"(long long|size_t|double|int) (.*)", decl)
+        assert m, decl
+        for f in m.group(2).split(","):
+            fields.append((f.strip(), _CTYPES[m.group(1)]))
+    return fields
+
+
+def test_ctypes_structs_match_header():
+    """The Python mirrors of the options / result structs carry the header's
+    fields in the header's order and types (lrb_scf reads them by layout)."""
+    for cname, py in (("LrbScfOptions", B.ScfOptions), ("LrbScfResult", B.ScfResult)):
+        assert [(n, t) for n, t in py._fields_] == _header_struct(cname), cname
+
+
+def test_ctypes_struct_layout_matches_c_compiler(tmp_path):
+    """Offsets and sizes of the structs as gcc lays them out from the header
+    equal the ctypes mirrors'."""
+    import shutil
+    import subprocess
+    import pytest
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "librint_b200.h"',
+             'int main(void) {']
+    for cname, _ in (("LrbScfOptions", 0), ("LrbScfResult", 0)):
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _t in _header_struct(cname):
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in (("LrbScfOptions", B.ScfOptions), ("LrbScfResult", B.ScfResult)):
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _t in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
