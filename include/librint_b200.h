@@ -71,7 +71,11 @@ LRB_API int lrb_int2e_batch_device(double *out, int coord, const int *shls, long
  * fit, are rejected with LRB_ERR_INPUT and the sizes in lrb_last_error().
  * Calls share the array: each clears what must start at zero itself, and
  * calls whose GPU work overlaps race.  The first call on a device sets up
- * (symbol lookup, kernel table); make it before any stream capture. */
+ * (symbol lookup, kernel table); make it before any stream capture.  Under
+ * CUDA's default lazy module loading the array is placed in device memory at
+ * that first call, so make it (a warm-up call will do) before other code
+ * reserves the GPU's free memory, or set CUDA_MODULE_LOADING=EAGER.  A call
+ * synchronises `stream` three times while preparing the batch. */
 #define LRB_NOALLOC_SCRATCH_BYTES (64ull << 20)
 #define LRB_NOALLOC_MAX_QUARTETS 65536
 LRB_API int lrb_int2e_batch_device_noalloc(double *out, int coord, const int *shls, long long nq,

@@ -6,6 +6,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "engine.h"
@@ -330,22 +331,39 @@ void fill_c2s(double *c) {
 ClassEntry g_classes[NCLASS];
 
 const ClassEntry *class_table() {
-  static bool init = false;
-  if (!init) {
-    double h[C2S_L * C2S_M * C2S_C];
-    fill_c2s(h);
-    eri_register_bra0(g_classes, h);
-    eri_register_bra1(g_classes, h);
-    eri_register_bra2(g_classes, h);
-    eri_register_bra3(g_classes, h);
-    eri_register_bra4(g_classes, h);
-    eri_register_bra5(g_classes, h);
-    for (int c = 0; c < NCLASS; ++c)
-      for (int m = 0; m < 3; ++m)
-        cudaFuncSetAttribute(g_classes[c].fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)g_classes[c].smem[m]);
-    init = true;
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static bool filled = false;
+  static bool ready[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    set_error("ERI kernel table: no usable current device");
+    return nullptr;
   }
+  std::lock_guard<std::mutex> g(mu);
+  if (ready[dev]) return g_classes;
+  double h[C2S_L * C2S_M * C2S_C];
+  fill_c2s(h);
+  ClassEntry *t = filled ? nullptr : g_classes;
+  cudaError_t e = cudaSuccess;
+  for (auto reg : {eri_register_bra0, eri_register_bra1, eri_register_bra2, eri_register_bra3,
+                   eri_register_bra4, eri_register_bra5})
+    if (e == cudaSuccess) e = reg(t, h);
+  if (e == cudaSuccess) filled = true;
+  for (int c = 0; c < NCLASS && e == cudaSuccess && filled; ++c)
+    for (int m = 0; m < 3 && e == cudaSuccess; ++m)
+      e = cudaFuncSetAttribute(g_classes[c].fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)g_classes[c].smem[m]);
+  if (e != cudaSuccess) {
+    char msg[160];
+    snprintf(msg, sizeof msg, "ERI kernel table set-up on device %d failed: %s", dev,
+             cudaGetErrorString(e));
+    cudaGetLastError();
+    set_error(msg);
+    return nullptr;
+  }
+  ready[dev] = true;
   return g_classes;
 }
 
@@ -386,6 +404,7 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   if (nq <= 0) return LRB_OK;
   if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
   const ClassEntry *tab = class_table();
+  if (!tab) return LRB_ERR_CUDA;
   // workspace
   Workspace &w = eng.ws;
   const size_t q = (size_t)nq;

@@ -5,10 +5,12 @@
 
 namespace lrb {
 
-void eri_register_bra1(ClassEntry *t, const double *c2s_host) {
-  cudaMemcpyToSymbol(c_c2s, c2s_host, sizeof(c_c2s));
+cudaError_t eri_register_bra1(ClassEntry *t, const double *c2s_host) {
+  const cudaError_t e = cudaMemcpyToSymbol(c_c2s, c2s_host, sizeof(c_c2s));
+  if (e != cudaSuccess || !t) return e;
   t[class_id(1, 0, 0, 0)] = make_entry<1, 0, 0, 0>();
   t[class_id(1, 0, 1, 0)] = make_entry<1, 0, 1, 0>();
+  return cudaSuccess;
 }
 
 }  // namespace lrb

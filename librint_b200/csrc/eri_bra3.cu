@@ -5,12 +5,14 @@
 
 namespace lrb {
 
-void eri_register_bra3(ClassEntry *t, const double *c2s_host) {
-  cudaMemcpyToSymbol(c_c2s, c2s_host, sizeof(c_c2s));
+cudaError_t eri_register_bra3(ClassEntry *t, const double *c2s_host) {
+  const cudaError_t e = cudaMemcpyToSymbol(c_c2s, c2s_host, sizeof(c_c2s));
+  if (e != cudaSuccess || !t) return e;
   t[class_id(2, 0, 0, 0)] = make_entry<2, 0, 0, 0>();
   t[class_id(2, 0, 1, 0)] = make_entry<2, 0, 1, 0>();
   t[class_id(2, 0, 1, 1)] = make_entry<2, 0, 1, 1>();
   t[class_id(2, 0, 2, 0)] = make_entry<2, 0, 2, 0>();
+  return cudaSuccess;
 }
 
 }  // namespace lrb

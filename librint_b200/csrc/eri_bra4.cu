@@ -5,13 +5,15 @@
 
 namespace lrb {
 
-void eri_register_bra4(ClassEntry *t, const double *c2s_host) {
-  cudaMemcpyToSymbol(c_c2s, c2s_host, sizeof(c_c2s));
+cudaError_t eri_register_bra4(ClassEntry *t, const double *c2s_host) {
+  const cudaError_t e = cudaMemcpyToSymbol(c_c2s, c2s_host, sizeof(c_c2s));
+  if (e != cudaSuccess || !t) return e;
   t[class_id(2, 1, 0, 0)] = make_entry<2, 1, 0, 0>();
   t[class_id(2, 1, 1, 0)] = make_entry<2, 1, 1, 0>();
   t[class_id(2, 1, 1, 1)] = make_entry<2, 1, 1, 1>();
   t[class_id(2, 1, 2, 0)] = make_entry<2, 1, 2, 0>();
   t[class_id(2, 1, 2, 1)] = make_entry<2, 1, 2, 1>();
+  return cudaSuccess;
 }
 
 }  // namespace lrb

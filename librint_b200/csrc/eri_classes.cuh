@@ -40,15 +40,21 @@ ClassEntry make_entry() {
   return e;
 }
 
-// Class table (instantiates on first use; uploads the cart->sph table).
+// Class table.  The kernel pointers and shared-memory sizes are host data,
+// filled once per process; the cart->sph constants of every translation unit
+// and the large-shared-memory attribute of every kernel belong to a device
+// and are set up once for each device the process uses.  Returns NULL (with
+// the error set) when that per-device set-up fails.
 const ClassEntry *class_table();
 void fill_c2s(double *c);
 
-void eri_register_bra0(ClassEntry *t, const double *c2s_host);   // (ss|
-void eri_register_bra1(ClassEntry *t, const double *c2s_host);   // (ps|
-void eri_register_bra2(ClassEntry *t, const double *c2s_host);   // (pp|
-void eri_register_bra3(ClassEntry *t, const double *c2s_host);   // (ds|
-void eri_register_bra4(ClassEntry *t, const double *c2s_host);   // (dp|
-void eri_register_bra5(ClassEntry *t, const double *c2s_host);   // (dd|
+// Each registration uploads its unit's cart->sph constants to the current
+// device and, when t is not NULL, fills its classes' table entries.
+cudaError_t eri_register_bra0(ClassEntry *t, const double *c2s_host);   // (ss|
+cudaError_t eri_register_bra1(ClassEntry *t, const double *c2s_host);   // (ps|
+cudaError_t eri_register_bra2(ClassEntry *t, const double *c2s_host);   // (pp|
+cudaError_t eri_register_bra3(ClassEntry *t, const double *c2s_host);   // (ds|
+cudaError_t eri_register_bra4(ClassEntry *t, const double *c2s_host);   // (dp|
+cudaError_t eri_register_bra5(ClassEntry *t, const double *c2s_host);   // (dd|
 
 }  // namespace lrb

@@ -369,6 +369,7 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
                FockStats *stats, int prec, double tau32, bool accumulate) {
   Engine &eng = engine();
   const ClassEntry *tab = class_table();
+  if (!tab) return LRB_ERR_CUDA;
   const int n = m.nao, nbas = m.nbas;
   // candidates: sorted positions i >= j with Q_i Q_j 2 max|D| >= tau
   k_dens_max<<<(nbas * nbas + 255) / 256, 256, 0, st>>>(dP, n, m.aooff, nbas, m.Dsh);

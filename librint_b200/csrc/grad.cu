@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #define RYS_OMIT_TAB
@@ -33,23 +34,44 @@ int scf_dense_fock(MolCtx &m, const double *P, double *F, cudaStream_t st);
 
 GradEntry g_grad_classes[NGRADCLS][NGRADMODE];
 
-static void grad_table_init() {
-  static bool init = false;
-  if (init) return;
-  GradEntry *t = &g_grad_classes[0][0];
-  for (int i = 0; i < NGRADCLS * NGRADMODE; ++i) t[i] = GradEntry{nullptr, 0, 1, 1};
-  grad_register_x0(t);
-  grad_register_x1(t);
-  grad_register_x2(t);
-  grad_register_n0(t);
-  grad_register_n1(t);
-  grad_register_n2(t);
+// Kernel pointers and shared-memory sizes are filled once per process; the
+// large-shared-memory attribute is per device and set for each device used.
+static int grad_table_init() {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static bool filled = false;
+  static bool ready[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return set_error("gradient kernel table: no usable current device"), LRB_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> g(mu);
+  if (ready[dev]) return LRB_OK;
+  if (!filled) {
+    GradEntry *t = &g_grad_classes[0][0];
+    for (int i = 0; i < NGRADCLS * NGRADMODE; ++i) t[i] = GradEntry{nullptr, 0, 1, 1};
+    grad_register_x0(t);
+    grad_register_x1(t);
+    grad_register_x2(t);
+    grad_register_n0(t);
+    grad_register_n1(t);
+    grad_register_n2(t);
+    filled = true;
+  }
   for (int c = 0; c < NGRADCLS; ++c)
     for (int r = 0; r < NGRADMODE; ++r)
-      if (g_grad_classes[c][r].fn)
-        cudaFuncSetAttribute(g_grad_classes[c][r].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)g_grad_classes[c][r].smem);
-  init = true;
+      if (g_grad_classes[c][r].fn) {
+        const cudaError_t e = cudaFuncSetAttribute(g_grad_classes[c][r].fn,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)g_grad_classes[c][r].smem);
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          return set_error(cudaGetErrorString(e)), LRB_ERR_CUDA;
+        }
+      }
+  ready[dev] = true;
+  return LRB_OK;
 }
 
 namespace {
@@ -517,7 +539,7 @@ static int grad_eri_pass(MolCtx &m, const double *Ps, double tau, int slot0, int
 
 int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, double tau,
              double *d_grad, int s1, cudaStream_t st) {
-  grad_table_init();
+  if (int rc0 = grad_table_init()) return rc0;
   Engine &eng = engine();
   const int n = m.nao, nbas = m.nbas;
   const long long nn = (long long)n * n;
@@ -630,7 +652,7 @@ int d1e_env_run(MolCtx &m, int op, double *d_out, cudaStream_t st) {
 }
 
 int grad_nuc_run(MolCtx &m, const double *d_P, double tau, double *d_gatom, cudaStream_t st) {
-  grad_table_init();
+  if (int rc0 = grad_table_init()) return rc0;
   Engine &eng = engine();
   const int n = m.nao, nbas = m.nbas;
   const long long nn = (long long)n * n;

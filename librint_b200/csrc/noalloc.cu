@@ -24,9 +24,16 @@
 //    between them, or different host threads) race on the array: order them.
 //  * The first call on a device looks up the array's device address and
 //    sets up the kernel table; make that first call before any stream
-//    capture starts.
-//  * Like lrb_int2e_batch_device it synchronises `stream` twice while
-//    preparing the batch (to read back sizes and the error flag).
+//    capture starts.  With CUDA's default lazy module loading the array
+//    itself is only placed in device memory at that first call, so make the
+//    first call (a warm-up call will do) before the framework reserves the
+//    GPU's free memory, or load modules eagerly (CUDA_MODULE_LOADING=EAGER);
+//    an out-of-memory failure of that first call says so.
+//  * It synchronises `stream` three times while preparing the batch: after
+//    counting the primitive pairs, after checking the molecule's indices,
+//    and after reading back the block sizes and class boundaries.
+//  * Kernel timing (lrb_profile_enable) and the launch counter
+//    (lrb_launch_count) cover this entry point like the others.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -84,9 +91,16 @@ int noalloc_setup(int dev, NoallocDevice *&nd) {
   void *p = nullptr;
   const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess || !p) {
-    char msg[160];
-    snprintf(msg, sizeof msg, "no-alloc scratch: cudaGetSymbolAddress failed (%s)",
-             cudaGetErrorString(e));
+    char msg[320];
+    if (e == cudaErrorMemoryAllocation)
+      snprintf(msg, sizeof msg,
+               "no-alloc scratch: the %llu-byte static array could not be placed in device "
+               "memory (%s); make the first call before other code reserves the GPU's free "
+               "memory, or set CUDA_MODULE_LOADING=EAGER so it is placed when the library loads",
+               (unsigned long long)LRB_NOALLOC_SCRATCH_BYTES, cudaGetErrorString(e));
+    else
+      snprintf(msg, sizeof msg, "no-alloc scratch: cudaGetSymbolAddress failed (%s)",
+               cudaGetErrorString(e));
     cudaGetLastError();
     return set_error(msg), LRB_ERR_CUDA;
   }
@@ -174,7 +188,15 @@ extern "C" LRB_API int lrb_int2e_batch_device_noalloc(double *out, int coord, co
   w.aux.size = o_pairs - o_aux;
   w.pairs.ptr = nd->base + o_pairs;
   w.pairs.size = cap - o_pairs;
+  // the shared engine's settings and counters cover this entry point too
+  Engine &shared = engine();
+  nd->eng.expcutoff = shared.expcutoff;
+  nd->eng.profile = shared.profile;
+  const long long launches0 = nd->eng.launches;
   rc = eri_batch_device(nd->eng, out, coord, shls, nq, atm, natm, bas, nbas, env, nenv, st, nullptr);
+  shared.launches += nd->eng.launches - launches0 + 1;   // + k_count_pairs
+  for (ProfRecord &r : nd->eng.prof) shared.prof.push_back(r);
+  nd->eng.prof.clear();
   if (rc == LRB_ERR_ALLOC)
     set_error("no-alloc batch: the batch needs more scratch than this entry point has; split it");
   return rc;

@@ -34,7 +34,9 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from librint_b200 import synthetic  # noqa: E402
 from librint_b200.basis import Molecule, read_molecule  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {os.path.basename(__file__)} <path of the reference checkout>")
+REF = sys.argv[1]
 P = ctypes.POINTER
 
 

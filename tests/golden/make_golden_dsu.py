@@ -26,7 +26,9 @@ from librint_b200 import synthetic  # noqa: E402
 from librint_b200.basis import read_molecule  # noqa: E402
 from make_golden import LIBC, P, _args, grad_len, mol_arrays  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {os.path.basename(__file__)} <path of the reference checkout>")
+REF = sys.argv[1]
 
 
 def main():

@@ -2,8 +2,10 @@
 callers that may not allocate device memory (for example inside a framework
 whose caching allocator already holds the GPU's free memory).  It must give
 the same integrals as lrb_int2e_batch_device, call after call, while taking
-all scratch from its fixed static array.  This file sorts last so that a run
-stopping at the first failure has run every other test before it."""
+all scratch from its fixed static array: once warm, its calls change neither
+the device's free memory nor the stream-ordered pool's reserved or used bytes.
+This file sorts last so that a run stopping at the first failure has run every
+other test before it."""
 import ctypes
 
 import numpy as np
@@ -33,6 +35,32 @@ def _noalloc(out, coord, sh, atm, bas, env):
                                                   env.numel(), ctypes.c_void_p(st))
 
 
+class _DriverMemory:
+    """Device free memory (cuMemGetInfo) and the default stream-ordered
+    pool's reserved / used bytes (cuMemPoolGetAttribute), read through the
+    CUDA driver on the calling thread's current context."""
+
+    RESERVED_CURRENT, RESERVED_HIGH, USED_CURRENT, USED_HIGH = 5, 6, 7, 8
+
+    def __init__(self):
+        self.cu = ctypes.CDLL("libcuda.so.1")
+        dev = ctypes.c_int()
+        assert self.cu.cuCtxGetDevice(ctypes.byref(dev)) == 0
+        self.pool = ctypes.c_void_p()
+        assert self.cu.cuDeviceGetDefaultMemPool(ctypes.byref(self.pool), dev) == 0
+
+    def snapshot(self):
+        free, total = ctypes.c_size_t(), ctypes.c_size_t()
+        assert self.cu.cuMemGetInfo_v2(ctypes.byref(free), ctypes.byref(total)) == 0
+        out = {"free": free.value}
+        for name, attr in (("reserved", self.RESERVED_CURRENT), ("reserved_high", self.RESERVED_HIGH),
+                           ("used", self.USED_CURRENT), ("used_high", self.USED_HIGH)):
+            v = ctypes.c_uint64()
+            assert self.cu.cuMemPoolGetAttribute(self.pool, attr, ctypes.byref(v)) == 0
+            out[name] = v.value
+        return out
+
+
 def _batches(golden):
     """A real molecule with shared shells and a high-momentum sweep class."""
     m = Molecule(golden["mol/h2o/def2svp/atm"], golden["mol/h2o/def2svp/bas"],
@@ -59,6 +87,31 @@ def test_noalloc_matches_batch_device_twice(golden):
                 torch.cuda.synchronize()
                 assert_eri_close(out.cpu().numpy(), ref.cpu().numpy(),
                                  what=f"{name} coord {coord} call {call}")
+
+
+def test_noalloc_allocates_no_device_memory(golden):
+    """After a warm-up call (which places the static array and sets up the
+    kernel table), further calls leave the device's free memory and the
+    default pool's reserved / used bytes and their high-water marks as they
+    were; every input and output is allocated before the first reading."""
+    batches = []
+    for name, m, shls in _batches(golden):
+        d = dict(atm=_dev(m.atm, np.int32), bas=_dev(m.bas, np.int32), env=_dev(m.env, np.float64),
+                 sh=_dev(shls, np.int32))
+        d["out"] = torch.empty(eri.batch_len(m, shls, 1), dtype=torch.float64, device="cuda")
+        batches.append(d)
+    for d in batches:                      # warm-up
+        assert _noalloc(d["out"], 1, d["sh"], d["atm"], d["bas"], d["env"]) == 0
+    torch.cuda.synchronize()
+    mem = _DriverMemory()
+    before = mem.snapshot()
+    for _ in range(3):
+        for d in batches:
+            rc = _noalloc(d["out"], 1, d["sh"], d["atm"], d["bas"], d["env"])
+            assert rc == 0, B.lib().lrb_last_error().decode()
+    torch.cuda.synchronize()
+    after = mem.snapshot()
+    assert after == before, (before, after)
 
 
 def test_noalloc_rejects_batches_beyond_its_scratch():
