@@ -37,6 +37,7 @@ from librint_b200 import shard, synthetic  # noqa: E402
 CLASSES = synthetic.canonical_classes(2)
 METRIC = "ERI shell quartets/s (FP64 Rys sweep, (ss|ss)..(dd|dd), K=1..6, spherical)"
 UNIT = "quartets/s"
+CPU_STEP_S = 3.0        # seconds of oracle work per CPU pass (bounded sample)
 
 
 # ------------------------------------------------------------ workload
@@ -250,7 +251,7 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def pick_sample(data, threads, budget_s=12.0):
+def pick_sample(data, threads, budget_s=CPU_STEP_S):
     """Sample size per class so one oracle pass takes about budget_s (two
     probes: a small one, then one of about a tenth of the budget)."""
     nmax = data[0][4].shape[0]
@@ -263,6 +264,22 @@ def pick_sample(data, threads, budget_s=12.0):
     return max(64, min(s, nmax))
 
 
+def cpu_rate(data, threads, steps, warmup, sample=None):
+    """The CPU restatement on the first ``sample`` quartets of every class
+    (sized by pick_sample when None): ``warmup`` untimed passes, then
+    ``steps`` timed passes.  The cpu_baseline leg and ``--impl reference``
+    both measure through this function on the same generated workload, so
+    their figures are the same measurement.  Returns (quartets/s, sample,
+    seconds timed)."""
+    s = sample or pick_sample(data, threads)
+    for _ in range(warmup):
+        cpu_sample(data, s, threads)
+    tt = 0.0
+    for _ in range(steps):
+        tt += cpu_sample(data, s, threads)[1]
+    return steps * len(data) * s / tt, s, tt
+
+
 # ------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -273,8 +290,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--rhf", type=int, default=0,
-                    help="also time RHF on the 60-atom C/H cluster (plain FP64 vs mixed)")
+    ap.add_argument("--rhf", type=int, default=1,
+                    help="time RHF on the 60-atom C/H cluster (plain FP64 vs mixed / learned); "
+                         "single-GPU runs only")
     ap.add_argument("--guess", default=os.path.join(ROOT, "librint_b200", "data", "guess_ch.npz"),
                     help="learned-guess network for the --rhf runs")
     ap.add_argument("--classes", default="",
@@ -404,14 +422,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        s = pick_sample(data, threads)
-        v, tcpu = cpu_sample(data, s, threads)
+        v, s, tcpu = cpu_rate(data, threads, steps=3, warmup=1)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {s} quartets of each of the {len(CLASSES)} classes of the same "
-                         f"workload ({len(CLASSES) * s} quartets, {tcpu:.1f} s), oracle/ C++ restatement, "
-                         f"OpenMP over quartets"}
+                         f"workload, 1 untimed + 3 timed passes ({3 * len(CLASSES) * s} quartets, "
+                         f"{tcpu:.1f} s), oracle/ C++ restatement, OpenMP over quartets"}
 
-    rhf = run_rhf(args.guess) if (args.rhf and rank == 0) else None
+    rhf = run_rhf(args.guess, threads, fp64_peak, cpu=not args.no_cpu) \
+        if (args.rhf and world == 1) else None
 
     if rank == 0:
         line = {
@@ -420,16 +438,8 @@ def main():
             "ms_per_step": elapsed / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded, distribution of the ERI sweep config)",
-            "config": {"workload": "ERI sweep: %s x %d quartets per "
-                                   "class per GPU, K=1..6, exponents log-uniform [0.05,5000], "
-                                   "centres in a 10 A cube, spherical output"
-                                   % ("21 classes (ss|ss)..(dd|dd)" if len(CLASSES) == 21 else
-                                      "classes " + ",".join("%d%d%d%d" % c for c in CLASSES),
-                                      args.nq),
-                       "quartets_per_step": len(CLASSES) * args.nq * world,
-                       "l2": "outputs (%.1f GB/step) exceed L2; no flush needed" %
-                             (sum(t['out'].numel() for t in dev_data) * 8 / 1e9),
-                       "parallelism": f"dp{world} (independent quartet shards)"},
+            "config": sweep_config(args, world,
+                                   sum(t['out'].numel() for t in dev_data) * 8 / 1e9),
             "roofline": {"bound": "fp64", "kernel": "k_eri<%d,%d,%d,%d,0,double>" % top,
                          "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
                          "frac": achieved_tf / fp64_peak if fp64_peak > 0 else None,
@@ -454,47 +464,148 @@ def main():
         dist.destroy_process_group()
 
 
-# Screening threshold of the FP32 SCF phases (hc_cluster, learned + mixed):
-# 1e-12 -> 2.14x, 1e-11 -> 2.33x, 1e-10 -> 2.18x (more iterations), 1e-9 ->
-# 1.22x over plain FP64; every setting ends at the FP64 energy to 2e-11 Eh.
+# Screening threshold of the FP32 SCF phases (learned + mixed): the FP32
+# phases skip quartets whose Schwarz x density bound is below it; the FP64
+# phase screens at TAU after a full rebuild, so the fixed point is the FP64
+# operator's.
 TAU_FP32 = 1e-11
+TAU = 1e-13
+RHF_TARGET_EH = 1e-6     # |E - E_FP64| a leg must reach to count
 
 
-def run_rhf(guess_file=None):
-    """RHF wall time on the C/H flake (hc_cluster: 34 C + 20 H, 610 cartesian
-    AOs, DZP-like basis).
+def fock_flops(cls, prim_quartets, quartets):
+    """FLOPs of Fock-mode work of one class: the per-primitive convention of
+    class_flops_bytes for the screened primitive quartets, plus 8 prod(nc)
+    per shell quartet for the J/K digestion (cartesian blocks, no cart2sph)."""
+    li, lj, lk, ll = cls
+    nmax, mmax = li + lj, lk + ll
+    nr = (nmax + mmax) // 2 + 1
+    nf = ncart(li) * ncart(lj) * ncart(lk) * ncart(ll)
+    H = sum((nmax - i + 1) * (mmax + 1) for i in range(1, li + 1)) + \
+        (lj + 1) * (li + 1) * sum(mmax - k + 1 for k in range(1, lk + 1))
+    per_prim = 50 + nr * (64 + 15 * (nmax + 1) * (mmax + 1) + 6 * H + 3 * nf)
+    return float(prim_quartets) * per_prim + 8.0 * nf * float(quartets)
 
-    reference: FP64, core-H guess, DIIS(8), Schwarz 1e-13, ||dP||/2 <= 1e-8;
-    plain:     the same schedule stopped at 1e-5 (the FP64 GPU path);
-    mixed:     incremental Fock builds with FP32 quartets, same stop; the
-               FP32 phases screen at tau_fp32 = 1e-11 (the FP64 phase at
-               1e-13, after a full rebuild);
-    learned:   mixed, started from the learned guess when its network applies
-               to this basis (otherwise absent).
-    Energies are compared with the reference run; times exclude the one-off
-    pair table / Schwarz set-up (reported separately)."""
+
+def fock_measure(ctx, P, fp64_peak, builds=3):
+    """Fock builds G(P) of the cluster at its converged density: FP64 and
+    all-FP32 builds per second (host wall clock around lrb_fock_G_prec,
+    copies of P and G included), per-class kernel times (CUDA events) and
+    counts, and the FP64 roofline of the dominant FP64 class."""
+    import ctypes
+    import torch
+    from librint_b200 import _bindings as B
+    L = B.lib()
+    out = {}
+    for prec, name in ((0, "fp64"), (1, "fp32")):
+        ctx.fock_G_prec(P, prec, tau=TAU)          # warm
+        torch.cuda.synchronize()
+        L.lrb_profile_read((ctypes.c_double * 64)(), 64)
+        L.lrb_fock_class_counts((ctypes.c_longlong * 64)(), (ctypes.c_longlong * 64)(), 64)
+        L.lrb_profile_enable(1)
+        t0 = time.perf_counter()
+        for _ in range(builds):
+            _, nq, _ = ctx.fock_G_prec(P, prec, tau=TAU)
+        dt = (time.perf_counter() - t0) / builds
+        L.lrb_profile_enable(0)
+        ms = (ctypes.c_double * 64)()
+        L.lrb_profile_read(ms, 64)
+        qn, pn = (ctypes.c_longlong * 64)(), (ctypes.c_longlong * 64)()
+        L.lrb_fock_class_counts(qn, pn, 64)
+        off = 0 if prec == 0 else len(CLASSES)
+        cls_rows = {}
+        for c in CLASSES:
+            i = class_id(c) + off
+            if qn[i] == 0:
+                continue
+            k_ms = ms[i] / builds
+            fl = fock_flops(c, pn[i] / builds, qn[i] / builds)
+            cls_rows["%d%d%d%d" % c] = {"ms": round(k_ms, 3), "quartets": qn[i] // builds,
+                                        "prim_quartets": pn[i] // builds,
+                                        "tflops": round(fl / (k_ms * 1e-3) / 1e12, 3) if k_ms > 0 else None}
+        kern = sum(v["ms"] for v in cls_rows.values())
+        out[name] = {"build_s": dt, "builds_per_s": 1.0 / dt, "quartets": nq,
+                     "kernel_ms": round(kern, 2), "classes": cls_rows}
+        if prec == 0:
+            top = max(cls_rows, key=lambda k: cls_rows[k]["ms"])
+            r = cls_rows[top]
+            out["roofline"] = {"bound": "fp64", "kernel": "k_eri<%s,%s,%s,%s,1,double>" % tuple(top),
+                               "achieved": r["tflops"], "peak": fp64_peak, "unit": "TFLOP/s",
+                               "frac": r["tflops"] / fp64_peak if fp64_peak > 0 else None,
+                               "kernel_ms": r["ms"], "kernel_share": r["ms"] / kern,
+                               "flop_convention": "fock_flops: screened primitive quartets x "
+                                                 "per-primitive count + 8 nf per quartet",
+                               "peak_source": "lrb_fp64_peak_probe (measured FP64 FMA rate)"}
+    return out
+
+
+def rhf_cpu_baseline(mol, P, threads, iterations, budget_s=10.0, seed=7):
+    """The reference's Fock build (src/scf.rs:316-410: every one of the
+    nbas^4 shell quartets, digested into G) restated by the oracle on the
+    host cores, timed on a uniform random sample of those quartets and
+    extrapolated to one build and to the plain schedule's iteration count."""
+    import oracle
+    nb = mol.nbas
+    rng = np.random.default_rng(seed)
+    n = 2048
+    for _ in range(3):
+        sh = rng.integers(0, nb, size=(n, 4)).astype(np.int32)
+        t0 = time.perf_counter()
+        oracle.fock_G_quartets(mol, P, sh, nthreads=threads)
+        t = time.perf_counter() - t0
+        if t >= 0.5 * budget_s:
+            break
+        n = int(min(n * budget_s / max(t, 1e-3), 50_000_000))
+    rate = n / t
+    build_s = float(nb) ** 4 / rate
+    return {"value": build_s * iterations, "unit": "s", "cores": threads, "kind": "port",
+            "fock_build_s": build_s, "iterations": iterations,
+            "sample": f"{n} shell quartets drawn uniformly from the nbas^4 = {nb ** 4} of one "
+                      f"Fock build of this system ({t:.1f} s, {rate:.0f} quartets/s), oracle/ "
+                      f"restatement of the reference's build, OpenMP; one build = nbas^4 / rate, "
+                      f"times the {iterations} iterations of the plain GPU schedule (the "
+                      f"reference's own P = I Roothaan loop needs more)"}
+
+
+def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True):
+    """RHF wall time on the 60-atom C/H cluster (synthetic.c3_cluster: 36 C +
+    24 H, 660 cartesian AOs, the seed-3 per-element C 3s2p1d / H 2s1p basis
+    with K = 1..6).
+
+    reference: FP64, core-H guess, DIIS(8), Schwarz x density tau = 1e-13,
+               ||dP||/2 <= 1e-8: the FP64 energy every leg is judged against;
+    plain:     the same FP64 GPU schedule stopped at 1e-5;
+    mixed:     incremental Fock builds with FP32 quartets, same stop (FP32
+               phases screen at tau_fp32 = 1e-11, the FP64 finish at 1e-13
+               after a full rebuild);
+    learned_*: started from the learned guess (when its network applies to
+               this basis), FP64 or mixed; the host prediction is timed in.
+    chosen = the fastest leg within 1e-6 Eh of the FP64 energy.  Times
+    exclude the one-off pair table / Schwarz set-up (setup_s)."""
     import torch
     from librint_b200 import scf as S
-    mol = synthetic.hc_cluster()
+    mol = synthetic.c3_cluster()
     t0 = time.perf_counter()
     ctx = S.MolContext(mol)
     torch.cuda.synchronize()
     setup = time.perf_counter() - t0
-    base = dict(guess=1, diis=8, tau=1e-13, max_iter=300, check=False)
+    base = dict(guess=1, diis=8, tau=TAU, max_iter=300, check=False)
 
-    def run(name, conv, P0=None, extra_ms=0.0, **kw):
+    def run(conv, P0=None, extra_ms=0.0, density=False, **kw):
         t0 = time.perf_counter()
-        r = ctx.scf(conv=conv, P0=P0, **dict(base, **kw))
+        r, Pc = ctx.scf(conv=conv, P0=P0, return_density=True, **dict(base, **kw))
         dt = time.perf_counter() - t0 + extra_ms / 1e3
-        return {"wall_s": dt, "energy": r.energy, "iterations": r.iterations,
-                "converged": bool(r.converged), "delta": r.delta, "fock_ms": r.fock_ms,
-                "quartets": r.quartets, "fp32_quartets": r.fp32_quartets}
+        res = {"wall_s": dt, "energy": r.energy, "iterations": r.iterations,
+               "converged": bool(r.converged), "delta": r.delta, "fock_s": r.fock_ms / 1e3,
+               "quartets": r.quartets, "fp32_quartets": r.fp32_quartets}
+        return (res, Pc) if density else res
 
-    out = {"system": "hc_cluster seed 3: %d cartesian AOs, %d shells, %d electrons"
-                     % (ctx.nao, mol.nbas, mol.nelec), "setup_s": setup}
-    out["reference"] = run("reference", 1e-8)
-    out["plain"] = run("plain", 1e-5)
-    out["mixed"] = run("mixed", 1e-5, mixed=1, tau_fp32=TAU_FP32)
+    out = {"system": "c3_cluster seed 3: %d atoms, %d cartesian AOs, %d shells, %d electrons"
+                     % (mol.natm, ctx.nao, mol.nbas, mol.nelec), "setup_s": setup,
+           "target_eh": RHF_TARGET_EH}
+    out["reference"], P_ref = run(1e-8, density=True)
+    out["plain"] = run(1e-5)
+    out["mixed"] = run(1e-5, mixed=1, tau_fp32=TAU_FP32)
     if guess_file and os.path.exists(guess_file):
         from librint_b200.guess import LearnedGuess
         g = LearnedGuess.load(guess_file)
@@ -503,46 +614,65 @@ def run_rhf(guess_file=None):
             tp = time.perf_counter()
             P0 = g.predict(mol, S=S_ov)
             t_pred = (time.perf_counter() - tp) * 1e3
-            out["learned_fp64"] = run("learned_fp64", 1e-5, P0=P0, extra_ms=t_pred)
-            out["learned_mixed"] = run("learned_mixed", 1e-5, P0=P0, extra_ms=t_pred, mixed=1,
-                                       tau_fp32=TAU_FP32)
+            out["learned_fp64"] = run(1e-5, P0=P0, extra_ms=t_pred)
+            out["learned_mixed"] = run(1e-5, P0=P0, extra_ms=t_pred, mixed=1, tau_fp32=TAU_FP32)
             out["predict_ms"] = t_pred
+        else:
+            out["learned"] = "network does not apply to this basis"
     e_ref = out["reference"]["energy"]
-    for k in ("plain", "mixed", "learned_fp64", "learned_mixed"):
-        if k in out:
-            out[k]["dE_vs_reference"] = out[k]["energy"] - e_ref
-            out[k]["speedup_vs_plain"] = out["plain"]["wall_s"] / out[k]["wall_s"]
+    legs = [k for k in ("plain", "mixed", "learned_fp64", "learned_mixed") if k in out]
+    for k in legs:
+        out[k]["dE_vs_reference"] = out[k]["energy"] - e_ref
+        out[k]["speedup_vs_plain"] = out["plain"]["wall_s"] / out[k]["wall_s"]
+    ok = [k for k in legs if out[k]["converged"] and abs(out[k]["dE_vs_reference"]) <= RHF_TARGET_EH]
+    if ok:
+        best = min(ok, key=lambda k: out[k]["wall_s"])
+        out["chosen"] = best
+        out["chosen_wall_s"] = out[best]["wall_s"]
+        out["plain_wall_s"] = out["plain"]["wall_s"]
+        out["speedup_chosen_vs_plain"] = out["plain"]["wall_s"] / out[best]["wall_s"]
+    out["fock"] = fock_measure(ctx, P_ref, fp64_peak)
     ctx.close()
+    if cpu:
+        out["cpu_baseline"] = rhf_cpu_baseline(mol, P_ref, threads, out["plain"]["iterations"])
     return out
 
 
 def run_reference(args, rank, world, threads):
+    """The reference arm: the CPU restatement of the reference algorithm
+    (oracle/, OpenMP on every host thread) on the same generated workload as
+    the GPU arm, each step one bounded pass over the first quartets of every
+    class (cpu_rate, the same measurement as the GPU arm's cpu_baseline)."""
     if rank != 0:
         return
-    data = generate(1 << 16, 2, procs=threads)
-    s = pick_sample(data, threads)
-    for _ in range(args.warmup):
-        cpu_sample(data, max(16, s // 8), threads)
-    vals, tt = [], 0.0
-    for _ in range(args.steps):
-        v, t = cpu_sample(data, s, threads)
-        vals.append(v)
-        tt += t
-    value = len(vals) * 21 * s / tt
+    data = generate(args.nq, shard.shard_seed(2, 0), procs=threads)
+    value, s, tt = cpu_rate(data, threads, steps=args.steps, warmup=args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded, distribution of the ERI sweep config)",
-        "config": {"workload": "ERI sweep: 21 classes (ss|ss)..(dd|dd), bounded sample of "
-                               "%d quartets per class per step" % s},
+        "config": sweep_config(args, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{s} quartets per class per step; the reference (Rust) "
-                                   f"cannot be built here, so its CPU restatement in oracle/ "
-                                   f"runs with OpenMP over quartets"},
+                         "sample": f"each step: the first {s} quartets of each of the "
+                                   f"{len(CLASSES)} classes of this workload; the reference "
+                                   f"(Rust, nightly Enzyme toolchain) cannot be built here, so "
+                                   f"its CPU restatement in oracle/ runs with OpenMP over quartets"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def sweep_config(args, world, out_gb=None):
+    cfg = {"workload": "ERI sweep: %s x %d quartets per class per GPU, K=1..6, exponents "
+                       "log-uniform [0.05,5000], centres in a 10 A cube, spherical output"
+                       % ("21 classes (ss|ss)..(dd|dd)" if len(CLASSES) == 21 else
+                          "classes " + ",".join("%d%d%d%d" % c for c in CLASSES), args.nq),
+           "quartets_per_step": len(CLASSES) * args.nq * world,
+           "parallelism": f"dp{world} (independent quartet shards)"}
+    if out_gb is not None:
+        cfg["l2"] = "outputs (%.1f GB/step) exceed L2; no flush needed" % out_gb
+    return cfg
 
 
 if __name__ == "__main__":

@@ -46,7 +46,7 @@ LRB_API const char *lrb_last_error(void);
  * shls holds nq quartets (4 shell indices each).  Every quartet's block is
  * written in libcint layout (out[i + ni*(j + nj*(k + nk*l))]) and the blocks
  * are packed back to back in quartet order; lrb_int2e_batch_len gives the
- * total length in doubles.  Shells: l <= 2, 1..31 primitives, nctr == 1.
+ * total length in doubles.  Shells: l <= 3, 1..31 primitives, nctr == 1.
  * Screening is the reference's (expcutoff 60, src/cint2e.rs:367-393).
  * -------------------------------------------------------------------*/
 LRB_API long long lrb_int2e_batch_len(int coord, const int *shls, long long nq, const int *bas, int nbas);
@@ -90,6 +90,10 @@ LRB_API int lrb_int2e_batch_device_noalloc(double *out, int coord, const int *sh
  * launches; lrb_fp64_peak_probe measures FP64 FMA throughput (TFLOP/s). */
 LRB_API void lrb_profile_enable(int on);
 LRB_API int lrb_profile_read(double *ms, int n);
+/* Fock builds run while profiling: per Fock class id (canonical class id,
+ * plus 55 for the FP32 kernels) the shell quartets and the primitive
+ * quartets that passed screening, since the last read (which clears them). */
+LRB_API int lrb_fock_class_counts(long long *quartets, long long *prim_quartets, int n);
 LRB_API long long lrb_launch_count(void);
 LRB_API double lrb_fp64_peak_probe(int ms);
 
@@ -138,6 +142,17 @@ LRB_API int lrb_mol_nao(const LrbMol *m);
  * (tau = 0 keeps every quartet the reference keeps).  Host or device. */
 LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long long *quartets);
 LRB_API int lrb_fock_G_device(LrbMol *m, const double *P, double *G, double tau, void *stream);
+/* One rank's share of G(P) for a Fock build split over nranks GPUs (no
+ * reference counterpart; the reference's integral2e_fock, src/scf.rs:316-410,
+ * is serial): the screened quartet candidates are enumerated in one order
+ * fixed by the Schwarz-sorted shell pairs, and rank r digests the candidates
+ * whose index is r mod nranks.  The shares are disjoint and complete, so the
+ * sum over ranks (one all-reduce of n*n doubles) is lrb_fock_G's G.  Host
+ * buffers, or device buffers on `stream` (_device). */
+LRB_API int lrb_fock_G_part(LrbMol *m, const double *P, double *G, double tau, int rank,
+                            int nranks, long long *quartets);
+LRB_API int lrb_fock_G_part_device(LrbMol *m, const double *P, double *G, double tau, int rank,
+                                   int nranks, long long *quartets, void *stream);
 /* The same G(P) with the mixed-precision kernels (no reference counterpart):
  * prec 0 all FP64, 1 all FP32, 2 FP32 only for quartets whose Schwarz x
  * density bound is below tau32.  FP32 quartets run the recurrences and the

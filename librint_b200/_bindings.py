@@ -83,12 +83,16 @@ def _optional(L):
         "lrb_profile_enable": (None, (c_int,)),
         "lrb_profile_read": (c_int, (P_d, c_int)),
         "lrb_launch_count": (c_ll, ()),
+        "lrb_fock_class_counts": (c_int, (ctypes.POINTER(c_ll), ctypes.POINTER(c_ll), c_int)),
         "lrb_fp64_peak_probe": (c_d, (c_int,)),
         "lrb_mol_create": (c_int, (ctypes.POINTER(c_vp), P_i, c_int, P_i, c_int, P_d, c_ll)),
         "lrb_mol_destroy": (None, (c_vp,)),
         "lrb_mol_nao": (c_int, (c_vp,)),
         "lrb_fock_G": (c_int, (c_vp, P_d, P_d, c_d, ctypes.POINTER(c_ll))),
         "lrb_fock_G_device": (c_int, (c_vp, c_vp, c_vp, c_d, c_vp)),
+        "lrb_fock_G_part": (c_int, (c_vp, P_d, P_d, c_d, c_int, c_int, ctypes.POINTER(c_ll))),
+        "lrb_fock_G_part_device": (c_int, (c_vp, c_vp, c_vp, c_d, c_int, c_int,
+                                           ctypes.POINTER(c_ll), c_vp)),
         "lrb_fock_G_prec": (c_int, (c_vp, P_d, P_d, c_d, c_int, c_d, ctypes.POINTER(c_ll),
                                     ctypes.POINTER(c_ll))),
         "lrb_scf": (c_int, (c_vp, c_ll, ctypes.POINTER(ScfOptions), ctypes.POINTER(ScfResult),

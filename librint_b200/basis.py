@@ -118,6 +118,22 @@ class Builder:
         self.bas.append([atom, l, len(exps), 1, 0, pe, pc, 0])
         return len(self.bas) - 1
 
+    def add_shell_gc(self, atom: int, l: int, exps, coef_sets, normalise: bool = True) -> int:
+        """A generally contracted shell: one exponent set, nctr contractions
+        (coef_sets[c] over the primitives; each normalised like add_shell).
+        env holds the coefficients contraction-major, c[ctr * nprim + prim]
+        (libcint's PTR_COEFF layout)."""
+        exps = [float(a) for a in exps]
+        sets = [normalise_contraction(l, exps, c) if normalise else np.asarray(c, float)
+                for c in coef_sets]
+        pe = len(self.env)
+        self.env += exps
+        pc = len(self.env)
+        for cs in sets:
+            self.env += [float(c) for c in cs]
+        self.bas.append([atom, l, len(exps), len(sets), 0, pe, pc, 0])
+        return len(self.bas) - 1
+
     def build(self, name: str = "", **meta) -> Molecule:
         return Molecule(np.array(self.atm, dtype=np.int32).ravel(),
                         np.array(self.bas, dtype=np.int32).ravel(),

@@ -142,15 +142,10 @@ int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq
 // non-blocking streams: chunk c's output copy to the host overlaps chunk
 // c+1's preparation and kernels.  A chunk starts only after the previous
 // chunk's kernels (event), because both share the engine's workspace.
-int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const int *atm,
-                    int natm, const int *bas, int nbas, const double *env, long long nenv) {
-  if (nq == 0) return LRB_OK;
-  if (!out || !shls || nq < 0) return set_error("bad output or quartet list"), LRB_ERR_INPUT;
-  int rc = check_common(atm, natm, bas, nbas, env, nenv);
-  if (rc) return rc;
-  if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
-  for (long long q = 0; q < 4 * nq; ++q)
-    if (shls[q] < 0 || shls[q] >= nbas) return set_error("shell index out of range"), LRB_ERR_INPUT;
+static int batch_host(double *out, int coord, const int *shls, long long nq, const int *atm,
+                      int natm, const int *bas, int nbas, const double *env, long long nenv,
+                      int gc_screen) {
+  int rc = LRB_OK;
   // chunk boundaries: at most CHUNK_Q quartets and about CHUNK_OUT doubles each
   constexpr long long CHUNK_Q = 1 << 17, CHUNK_OUT = 1 << 25;
   std::vector<long long> qb{0}, ob{0};
@@ -208,7 +203,7 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
       break;
     }
     rc = eri_batch_device(eng, d_o, coord, d_sh, nqc, m.atm, natm, m.bas, nbas, m.env, nenv, st,
-                          nullptr, cen);
+                          nullptr, cen, gc_screen);
     if (rc) break;
     if (cudaEventRecord(eng.done[X], st) != cudaSuccess ||
         cudaMemcpyAsync(out + ob[c], d_o, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost,
@@ -226,6 +221,68 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
   return rc;
 }
 
+int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const int *atm,
+                    int natm, const int *bas, int nbas, const double *env, long long nenv) {
+  if (nq == 0) return LRB_OK;
+  if (!out || !shls || nq < 0) return set_error("bad output or quartet list"), LRB_ERR_INPUT;
+  int rc = check_common(atm, natm, bas, nbas, env, nenv);
+  if (rc) return rc;
+  if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
+  for (long long q = 0; q < 4 * nq; ++q)
+    if (shls[q] < 0 || shls[q] >= nbas) return set_error("shell index out of range"), LRB_ERR_INPUT;
+  GcExpanded x;
+  if ((rc = gc_expand(bas, nbas, env, nenv, x))) return rc;
+  if (!x.any) return batch_host(out, coord, shls, nq, atm, natm, bas, nbas, env, nenv, 0);
+  // Generally contracted shells: every quartet becomes prod(nctr) quartets of
+  // segmented sub-shells (contraction of i fastest), computed as one batch
+  // and placed into the quartet's block at rows ctr * nf + component
+  // (libcint's layout of a shell with several contractions).
+  std::vector<int> sub;
+  for (long long q = 0; q < nq; ++q) {
+    const int *s4 = shls + 4 * q;
+    const int nc[4] = {bas[8 * s4[0] + 3], bas[8 * s4[1] + 3], bas[8 * s4[2] + 3], bas[8 * s4[3] + 3]};
+    for (int cl = 0; cl < nc[3]; ++cl)
+      for (int ck = 0; ck < nc[2]; ++ck)
+        for (int cj = 0; cj < nc[1]; ++cj)
+          for (int ci = 0; ci < nc[0]; ++ci) {
+            const int t[4] = {x.first[s4[0]] + ci, x.first[s4[1]] + cj, x.first[s4[2]] + ck,
+                              x.first[s4[3]] + cl};
+            sub.insert(sub.end(), t, t + 4);
+          }
+  }
+  const long long nsub = (long long)sub.size() / 4;
+  const int nbx = (int)(x.bas.size() / 8);
+  std::vector<double> tmp((size_t)eri_batch_out_len(coord, sub.data(), nsub, x.bas.data()));
+  rc = batch_host(tmp.data(), coord, sub.data(), nsub, atm, natm, x.bas.data(), nbx, x.env.data(),
+                  (long long)x.env.size(), 1);
+  if (rc) return rc;
+  size_t src = 0, dst = 0;
+  for (long long q = 0; q < nq; ++q) {
+    const int *s4 = shls + 4 * q;
+    int nf[4], nc[4], N[4];
+    for (int a = 0; a < 4; ++a) {
+      const int l = bas[8 * s4[a] + 1];
+      nf[a] = coord == 0 ? ncart(l) : nsph(l);
+      nc[a] = bas[8 * s4[a] + 3];
+      N[a] = nf[a] * nc[a];
+    }
+    for (int cl = 0; cl < nc[3]; ++cl)
+      for (int ck = 0; ck < nc[2]; ++ck)
+        for (int cj = 0; cj < nc[1]; ++cj)
+          for (int ci = 0; ci < nc[0]; ++ci)
+            for (int d = 0; d < nf[3]; ++d)
+              for (int c = 0; c < nf[2]; ++c)
+                for (int b = 0; b < nf[1]; ++b)
+                  for (int a = 0; a < nf[0]; ++a)
+                    out[dst + (ci * nf[0] + a) +
+                        (size_t)N[0] * ((cj * nf[1] + b) +
+                                        (size_t)N[1] * ((ck * nf[2] + c) + (size_t)N[2] * (cl * nf[3] + d)))] =
+                        tmp[src++];
+    dst += (size_t)N[0] * N[1] * N[2] * N[3];
+  }
+  return LRB_OK;
+}
+
 // ------------------------------------------------------------ libcint ABI
 static int int2e_one(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
                      double *env, CINTOpt *opt, int coord) {
@@ -236,6 +293,8 @@ static int int2e_one(double *out, int *dims, int *shls, int *atm, int natm, int 
   }
   const long long blk = (long long)d[0] * d[1] * d[2] * d[3];
   if (!out) return (int)blk;
+  bool gc = false;
+  for (int a = 0; a < 4; ++a) gc = gc || bas[8 * shls[a] + 3] > 1;
   cudaStream_t st = nullptr;
   DevMol local;
   const DevMol *m = nullptr;
@@ -251,7 +310,11 @@ static int int2e_one(double *out, int *dims, int *shls, int *atm, int natm, int 
   double *d_out = nullptr;
   std::vector<double> blkbuf(blk);
   int rc = 0;
-  if (cudaMallocAsync((void **)&d_sh, 4 * sizeof(int), st) != cudaSuccess ||
+  if (gc) {
+    // generally contracted shells go through the host batch path
+    rc = lrb_int2e_batch(blkbuf.data(), coord, shls, 1, atm, natm, bas, nbas, env,
+                         env_extent(atm, natm, bas, nbas));
+  } else if (cudaMallocAsync((void **)&d_sh, 4 * sizeof(int), st) != cudaSuccess ||
       cudaMallocAsync((void **)&d_out, sizeof(double) * blk, st) != cudaSuccess) {
     rc = -1;
   } else {
@@ -328,9 +391,21 @@ void free_c(double *ptr, size_t len) {
 
 double *int2e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, size_t env_l,
                 int coord) {
-  const int natm = (int)(atm_l / 6), nbas = (int)(bas_l / 8);
+  const int natm = (int)(atm_l / 6);
+  int nbas = (int)(bas_l / 8);
   if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), nullptr;
   if (check_common(atm_p, natm, bas_p, nbas, env_p, (long long)env_l)) return nullptr;
+  // generally contracted shells: the tensor of the segmented sub-shells is
+  // the same tensor (same AO order)
+  GcExpanded x;
+  if (gc_expand(bas_p, nbas, env_p, (long long)env_l, x)) return nullptr;
+  const int gc_screen = x.any ? 1 : 0;
+  if (x.any) {
+    bas_p = x.bas.data();
+    nbas = (int)(x.bas.size() / 8);
+    env_p = x.env.data();
+    env_l = x.env.size();
+  }
   std::vector<int> aooff(nbas + 1, 0), dim(nbas);
   for (int s = 0; s < nbas; ++s) {
     dim[s] = shell_dim(coord, bas_p, s);
@@ -378,7 +453,7 @@ double *int2e_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_
     cudaMemcpyAsync(d_dim, dim.data(), sizeof(int) * dim.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_boff, boff.data(), sizeof(long long) * boff.size(), cudaMemcpyHostToDevice, st);
     rc = eri_batch_device(engine(), d_blk, coord, d_q, nq, m.atm, natm, m.bas, nbas, m.env,
-                          (long long)env_l, st, nullptr);
+                          (long long)env_l, st, nullptr, nullptr, gc_screen);
   }
   if (!rc) {
     k_scatter8<<<(unsigned)nq, 128, 0, st>>>(d_blk, d_boff, d_q, d_ao, d_dim, (int)nq, n, d_R);
@@ -470,6 +545,34 @@ LRB_API int lrb_fock_G_prec(LrbMol *m, const double *P, double *G, double tau, i
   if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
   if (quartets) *quartets = fs.quartets;
   if (fp32_quartets) *fp32_quartets = fs.fp32_quartets;
+  return rc;
+}
+
+LRB_API int lrb_fock_G_part_device(LrbMol *m, const double *P, double *G, double tau, int rank,
+                                   int nranks, long long *quartets, void *stream) {
+  if (!m || !P || !G) return set_error("NULL argument"), LRB_ERR_INPUT;
+  FockStats fs;
+  const int rc = fock_build(m->ctx, P, G, tau, (cudaStream_t)stream, &fs, 0, 0.0, false, rank,
+                            nranks);
+  if (quartets) *quartets = fs.quartets;
+  return rc;
+}
+
+LRB_API int lrb_fock_G_part(LrbMol *m, const double *P, double *G, double tau, int rank,
+                            int nranks, long long *quartets) {
+  if (!m || !P || !G) return set_error("NULL argument"), LRB_ERR_INPUT;
+  const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
+  cudaStream_t st = nullptr;
+  double *dP = nullptr, *dG = nullptr;
+  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
+      cudaMallocAsync((void **)&dG, nn * 8, st) != cudaSuccess)
+    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
+  int rc = lrb_fock_G_part_device(m, dP, dG, tau, rank, nranks, quartets, st);
+  if (!rc) cudaMemcpyAsync(G, dG, nn * 8, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dP, st);
+  cudaFreeAsync(dG, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = (set_error("CUDA error"), LRB_ERR_CUDA);
   return rc;
 }
 

@@ -1,3 +1,5 @@
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -47,6 +49,40 @@ Engine &engine() {
     per_dev[dev] = new Engine();
   }
   return *per_dev[dev];
+}
+
+int gc_expand(const int *bas, int nbas, const double *env, long long nenv, GcExpanded &x) {
+  x = GcExpanded();
+  x.first.assign(nbas + 1, 0);
+  for (int s = 0; s < nbas; ++s) {
+    const int *b = bas + 8 * s;
+    if (b[3] < 1 || b[2] < 1 || b[5] < 0 || b[6] < 0 || (long long)b[5] + b[2] > nenv ||
+        (long long)b[6] + (long long)b[2] * b[3] > nenv)
+      return set_error("bas entry out of range (nprim, nctr or env pointers)"), LRB_ERR_INPUT;
+    x.first[s + 1] = x.first[s] + b[3];
+    x.any = x.any || b[3] > 1;
+  }
+  if (!x.any) return LRB_OK;
+  x.env.assign(env, env + nenv);
+  x.bas.reserve(8 * (size_t)x.first[nbas]);
+  for (int s = 0; s < nbas; ++s) {
+    const int *b = bas + 8 * s;
+    const int nprim = b[2], nctr = b[3];
+    int scr = 0;
+    if (nctr > 1) {
+      scr = (int)x.env.size();
+      for (int p = 0; p < nprim; ++p) {
+        double m = 0.0;
+        for (int c = 0; c < nctr; ++c) m = std::max(m, std::fabs(env[b[6] + c * nprim + p]));
+        x.env.push_back(m);
+      }
+    }
+    for (int c = 0; c < nctr; ++c) {
+      const int sub[8] = {b[0], b[1], nprim, 1, b[4], b[5], b[6] + c * nprim, scr};
+      x.bas.insert(x.bas.end(), sub, sub + 8);
+    }
+  }
+  return LRB_OK;
 }
 
 // FP64 FMA throughput probe: 8 independent chains per thread keep the FP64
@@ -99,6 +135,25 @@ LRB_API int lrb_profile_read(double *ms, int n) {
 }
 
 LRB_API long long lrb_launch_count(void) { return engine().launches; }
+
+// Per Fock class (id = canonical class, +55 for the FP32 kernels) the shell
+// quartets and the screened primitive quartets of the Fock builds run while
+// profiling was enabled, since the last read; clears them.
+LRB_API int lrb_fock_class_counts(long long *quartets, long long *prim_quartets, int n) {
+  Engine &e = engine();
+  unsigned long long h[128] = {};
+  if (e.fock_prim) {
+    if (cudaMemcpy(h, e.fock_prim, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(e.fock_prim, 0, sizeof h) != cudaSuccess)
+      return set_error("fock class counts: copy failed"), LRB_ERR_CUDA;
+  }
+  for (int i = 0; i < n; ++i) {
+    quartets[i] = i < 128 ? e.fock_quartets[i] : 0;
+    prim_quartets[i] = i < 128 ? (long long)h[i] : 0;
+  }
+  for (long long &q : e.fock_quartets) q = 0;
+  return LRB_OK;
+}
 
 // Measured FP64 FMA throughput of the current device in TFLOP/s (about
 // `ms` milliseconds of work, timed with CUDA events).

@@ -11,7 +11,7 @@
 
 namespace lrb {
 
-constexpr int ERI_LMAX = 2;    // shells up to d in the compiled classes
+constexpr int ERI_LMAX = 3;    // shells up to f (d: templated kernels, f: eri_gen.cu)
 constexpr int ERI_KMAX = 31;   // primitives per shell (sort-key packing limit)
 
 void set_error(const char *msg);
@@ -59,6 +59,11 @@ struct Engine {
   bool profile = false;
   std::vector<ProfRecord> prof;
   long long launches = 0;    // kernels of this library launched so far
+  // Fock-build class counts while profiling (index = Fock class id: class,
+  // +55 for the FP32 kernels): shell quartets, and on the device the
+  // primitive quartets that passed screening
+  long long fock_quartets[128] = {};
+  unsigned long long *fock_prim = nullptr;   // 128 device counters
   // host-buffer entry points: two non-blocking streams that alternate over
   // chunks (copy-out of one chunk overlaps the next chunk's kernels) and
   // per-stream device buffers that only grow
@@ -74,10 +79,27 @@ struct EriBatchStats {
 
 // centers_ready: shell centres already computed (and the molecule's indices
 // checked) by eri_centers for this molecule; NULL computes them per call.
+// gc_screen: bas slot 7 of a shell, when positive, points at the screening
+// coefficients (largest |c| over the contractions of the generally contracted
+// shell it was split from); set only for bas arrays built by gc_expand.
 int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, long long nq,
                      const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
                      long long nenv, cudaStream_t st, EriBatchStats *stats,
-                     const double *centers_ready = nullptr);
+                     const double *centers_ready = nullptr, int gc_screen = 0);
+
+// Generally contracted shells (nctr > 1) as nctr consecutive segmented
+// sub-shells with the same exponents (coefficient pointer advanced by
+// c * nprim), so the AO numbering is unchanged.  env gains, per such shell,
+// the largest |coefficient| of each primitive over its contractions (the
+// reference's screening coefficient, src/optimizer.rs:661-687), referenced by
+// the sub-shells' bas slot 7.  any == false: nothing to expand.
+struct GcExpanded {
+  bool any = false;
+  std::vector<int> bas;      // 8 ints per sub-shell
+  std::vector<double> env;   // the input env followed by the screening arrays
+  std::vector<int> first;    // first sub-shell of each input shell (nbas + 1)
+};
+int gc_expand(const int *bas, int nbas, const double *env, long long nenv, GcExpanded &x);
 // Shell centres (3 doubles per shell) with every atm/bas/env index checked;
 // d_err is one device int; synchronises st to read it.
 int eri_centers(const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,

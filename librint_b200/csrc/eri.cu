@@ -84,7 +84,7 @@ __device__ inline double common_fac_sp(int l) {
 __device__ __forceinline__ PrimPair make_pair(int si, int sj, bool ket, int e,
                                               const int *__restrict__ atm,
                                               const int *__restrict__ bas,
-                                              const double *__restrict__ env) {
+                                              const double *__restrict__ env, int gc_screen) {
   const int *bi = bas + 8 * si, *bj = bas + 8 * sj;
   const int ki = bi[2], kj = bj[2];
   const int ip = e % ki, jp = e / ki;
@@ -110,7 +110,11 @@ __device__ __forceinline__ PrimPair make_pair(int si, int sj, bool ket, int e,
   o.fac = fac;
   o.ia = inv;
   o.facia = fac * inv;
-  o.cce = eij - log_rr - log(fabs(ci)) - log(fabs(cj));
+  // sub-shells of a generally contracted shell screen with the largest
+  // |coefficient| over its contractions (bas slot 7 when gc_screen)
+  const double si_c = gc_screen && bi[7] > 0 ? env[bi[7] + ip] : ci;
+  const double sj_c = gc_screen && bj[7] > 0 ? env[bj[7] + jp] : cj;
+  o.cce = eij - log_rr - log(fabs(si_c)) - log(fabs(sj_c));
   return o;
 }
 
@@ -121,13 +125,15 @@ __device__ __forceinline__ PrimPair make_pair(int si, int sj, bool ket, int e,
 __device__ void pair_sort_warp(long long pr, int lane, const QuartetJob *__restrict__ jobs,
                                const int *__restrict__ pair_off, const int *__restrict__ atm,
                                const int *__restrict__ bas, const double *__restrict__ env,
-                               PrimPair *__restrict__ pp, PrimPair *__restrict__ raw) {
+                               PrimPair *__restrict__ pp, PrimPair *__restrict__ raw,
+                               int gc_screen) {
   const QuartetJob j = jobs[pr >> 1];
   const bool ket = pr & 1;
   const int si = ket ? j.ksh : j.ish, sj = ket ? j.lsh : j.jsh;
   const int n = ket ? j.nkl : j.nij;
   const long long off = pair_off[pr];
-  for (int e = lane; e < n; e += 32) raw[off + e] = make_pair(si, sj, ket, e, atm, bas, env);
+  for (int e = lane; e < n; e += 32)
+    raw[off + e] = make_pair(si, sj, ket, e, atm, bas, env, gc_screen);
   __syncwarp();
   for (int e = lane; e < n; e += 32) {
     const double c = cce_key(raw[off + e].cce);
@@ -147,6 +153,7 @@ struct PairHead {
   double dx, dy, dz;      // R_j - R_i
   double rr, log_rr, cfac;
   int ea, ca, eb, cb;     // env offsets of exponents / coefficients of i and j
+  int sa, sb;             // env offsets of the screening coefficients of i and j
   int ki, first;          // primitives of i; first primitive pair (block-relative)
 };
 
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(PB_THREADS, 3)
 k_pairs_block(const QuartetJob *__restrict__ jobs, long long nq, const int *__restrict__ npair,
               const int *__restrict__ pair_off, const int *__restrict__ atm,
               const int *__restrict__ bas, const double *__restrict__ env,
-              PrimPair *__restrict__ pp, PrimPair *__restrict__ raw) {
+              PrimPair *__restrict__ pp, PrimPair *__restrict__ raw, int gc_screen) {
   __shared__ double skey[PB_CAP];
   __shared__ PairHead head[PB_PAIRS];
   __shared__ int soff[PB_PAIRS + 1];
@@ -186,6 +193,8 @@ k_pairs_block(const QuartetJob *__restrict__ jobs, long long nq, const int *__re
     h.rr = h.dx * h.dx + h.dy * h.dy + h.dz * h.dz;
     h.dx = rj[0] - ri[0]; h.dy = rj[1] - ri[1]; h.dz = rj[2] - ri[2];
     h.ea = bi[5]; h.ca = bi[6]; h.eb = bj[5]; h.cb = bj[6]; h.ki = ki;
+    h.sa = gc_screen && bi[7] > 0 ? bi[7] : bi[6];
+    h.sb = gc_screen && bj[7] > 0 ? bj[7] : bj[6];
     const int lij = bi[1] + bj[1];
     double log_rr = 1.7 - 1.5 * log(env[bi[5] + ki - 1] + env[bj[5] + kj - 1]);
     if (lij > 0) log_rr += lij * log(sqrt(h.rr) + 1.0);
@@ -198,7 +207,7 @@ k_pairs_block(const QuartetJob *__restrict__ jobs, long long nq, const int *__re
   const int base = soff[0], R = soff[P] - base;
   if (R > PB_CAP) {
     for (int w = t >> 5; w < P; w += PB_THREADS / 32)
-      pair_sort_warp(p0 + w, t & 31, jobs, pair_off, atm, bas, env, pp, raw);
+      pair_sort_warp(p0 + w, t & 31, jobs, pair_off, atm, bas, env, pp, raw, gc_screen);
     return;
   }
   if (t < P) head[t].first = soff[t] - base;
@@ -216,7 +225,7 @@ k_pairs_block(const QuartetJob *__restrict__ jobs, long long nq, const int *__re
     const PairHead &h = head[find(e)];
     const int k = e - h.first, ip = k % h.ki, jp = k / h.ki;
     const double ai = env[h.ea + ip], aj = env[h.eb + jp];
-    const double ci = env[h.ca + ip], cj = env[h.cb + jp];
+    const double ci = env[h.sa + ip], cj = env[h.sb + jp];
     const double inv = 1.0 / (ai + aj);
     const double eij = h.rr * ai * aj * inv;
     skey[e] = eij - h.log_rr - log(fabs(ci)) - log(fabs(cj));
@@ -350,11 +359,30 @@ const ClassEntry *class_table() {
   for (auto reg : {eri_register_bra0, eri_register_bra1, eri_register_bra2, eri_register_bra3,
                    eri_register_bra4, eri_register_bra5})
     if (e == cudaSuccess) e = reg(t, h);
+  if (e == cudaSuccess) e = eri_register_gen(h);
+  if (e == cudaSuccess && !filled) {
+    // the f classes: k_eri_gen with run-time class sizes
+    for (int li = 0; li <= ERI_LMAX; ++li)
+      for (int lj = 0; lj <= li; ++lj)
+        for (int lk = 0; lk <= ERI_LMAX; ++lk)
+          for (int ll = 0; ll <= lk; ++ll) {
+            if (pair_index(lk, ll) > pair_index(li, lj) || li < 3) continue;
+            ClassEntry &ce = g_classes[class_id(li, lj, lk, ll)];
+            ce = ClassEntry{};
+            ce.gen = 1;
+            ce.g = gen_class(li, lj, lk, ll);
+            ce.nr = ce.g.nr;
+            ce.slots = 1;
+            ce.smem[0] = gen_smem_bytes(ce.g, 0);
+            ce.smem[1] = gen_smem_bytes(ce.g, 1);
+          }
+  }
   if (e == cudaSuccess) filled = true;
   for (int c = 0; c < NCLASS && e == cudaSuccess && filled; ++c)
     for (int m = 0; m < 3 && e == cudaSuccess; ++m)
-      e = cudaFuncSetAttribute(g_classes[c].fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)g_classes[c].smem[m]);
+      if (!g_classes[c].gen)
+        e = cudaFuncSetAttribute(g_classes[c].fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)g_classes[c].smem[m]);
   if (e != cudaSuccess) {
     char msg[160];
     snprintf(msg, sizeof msg, "ERI kernel table set-up on device %d failed: %s", dev,
@@ -400,7 +428,7 @@ int eri_centers(const int *d_atm, int natm, const int *d_bas, int nbas, const do
 int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, long long nq,
                      const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
                      long long nenv, cudaStream_t st, EriBatchStats *stats,
-                     const double *centers_ready) {
+                     const double *centers_ready, int gc_screen) {
   if (nq <= 0) return LRB_OK;
   if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
   const ClassEntry *tab = class_table();
@@ -465,7 +493,7 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   LRB_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * (NCLASS + 1), cudaMemcpyDeviceToHost, st));
   LRB_CK(cudaStreamSynchronize(st));
   if (herr == 2) return set_error("shell index out of range"), LRB_ERR_INPUT;
-  if (herr) return set_error("shell with l > 2, nprim > 31 or nctr != 1"), LRB_ERR_UNSUPPORTED;
+  if (herr) return set_error("shell with l > 3, nprim > 31 or nctr != 1"), LRB_ERR_UNSUPPORTED;
   const long long npp = (long long)last_poff + last_np;
   if (npp > 2147483647LL) return set_error("too many primitive pairs in one batch"), LRB_ERR_INPUT;
   // pairs in natural order go to the second half, sorted ones to the first
@@ -473,7 +501,7 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   if (!pp) return set_error("workspace allocation failed"), LRB_ERR_ALLOC;
   if (npp > 0) {
     k_pairs_block<<<(unsigned)((2 * nq + PB_PAIRS - 1) / PB_PAIRS), PB_THREADS, 0, st>>>(
-        jobs, nq, npair, pair_off, d_atm, d_bas, d_env, pp, pp + npp);
+        jobs, nq, npair, pair_off, d_atm, d_bas, d_env, pp, pp + npp, gc_screen);
     ++eng.launches;
   }
   LRB_CK(cudaGetLastError());
@@ -495,11 +523,14 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
     prm.order = idx2 + cls_begin[c];
     prm.njobs = (int)(end - cls_begin[c]);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[0], ERI_THREADS, ce.smem[0]);
+    if (ce.gen)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gen_kernel(0), GEN_THREADS, ce.smem[0]);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[0], ERI_THREADS, ce.smem[0]);
     if (per_sm < 1) per_sm = 1;
     const long long tasks = (prm.njobs + ce.slots - 1) / ce.slots;
     long long grid = (long long)nsm * per_sm;
-    const long long need = (tasks + ERI_WARPS - 1) / ERI_WARPS;
+    const long long need = ce.gen ? tasks : (tasks + ERI_WARPS - 1) / ERI_WARPS;
     if (grid > need) grid = need;
     ProfRecord rec{c, nullptr, nullptr};
     if (eng.profile) {
@@ -508,8 +539,14 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
       cudaEventRecord(rec.start, st);
     }
     FockParams nofock{};
-    ce.fn[0]<<<(unsigned)grid, ERI_THREADS, ce.smem[0], st>>>(prm, nofock, rys + RYS_TAB_OFFSET[ce.nr],
-                                                              counters + c);
+    if (ce.gen)
+      gen_kernel(0)<<<(unsigned)grid, GEN_THREADS, ce.smem[0], st>>>(prm, nofock, ce.g,
+                                                                     rys + RYS_TAB_OFFSET[ce.nr],
+                                                                     counters + c);
+    else
+      ce.fn[0]<<<(unsigned)grid, ERI_THREADS, ce.smem[0], st>>>(prm, nofock,
+                                                                rys + RYS_TAB_OFFSET[ce.nr],
+                                                                counters + c);
     LRB_CK(cudaGetLastError());
     ++eng.launches;
     if (eng.profile) {

@@ -15,14 +15,32 @@ __host__ __device__ inline int class_id(int li, int lj, int lk, int ll) {
   return P * (P + 1) / 2 + Q;
 }
 constexpr int NPAIRCLS = (ERI_LMAX + 1) * (ERI_LMAX + 2) / 2;
-constexpr int NCLASS = NPAIRCLS * (NPAIRCLS + 1) / 2;
+constexpr int NCLASS = NPAIRCLS * (NPAIRCLS + 1) / 2;   // 55 for l <= 3
+constexpr int NCLASS_TPL = 21;   // l <= 2: the templated kernels; ids 21.. carry an f shell
 
 using EriKernelFn = void (*)(EriParams, FockParams, const double *, int *);
+
+// Classes with an f shell run k_eri_gen (eri_gen.cu), one quartet per CTA.
+constexpr int GEN_THREADS = 128;
+struct GenClass {
+  int li, lj, lk, ll, nr;
+  int ib, kb;              // bra base is i (else j); ket base is k (else l)
+  int la, lb, lc, ld;      // base / partner momenta of bra and ket
+  int ni, nj, nk, nl;      // cartesian counts
+  int gsz;                 // (la+1)(lb+1)(lc+1)(ld+1)
+};
+using GenKernelFn = void (*)(EriParams, FockParams, GenClass, const double *, int *);
+GenClass gen_class(int li, int lj, int lk, int ll);
+GenKernelFn gen_kernel(int mode);                 // 0 output, 1 Fock (FP64)
+size_t gen_smem_bytes(const GenClass &g, int mode);
+cudaError_t eri_register_gen(const double *c2s_host);   // per device
 
 struct ClassEntry {
   EriKernelFn fn[3];     // output (FP64), Fock digestion FP64, Fock digestion FP32
   size_t smem[3];
   int slots, nr;
+  int gen;               // 1: k_eri_gen with `g` (fn unused)
+  GenClass g;
 };
 
 template <int LI, int LJ, int LK, int LL>
@@ -37,6 +55,7 @@ ClassEntry make_entry() {
   e.smem[2] = EriLayout<C, 1, float>::SMEM;
   e.slots = C::SLOTS;
   e.nr = C::NR;
+  e.gen = 0;
   return e;
 }
 

@@ -137,6 +137,9 @@ struct FockParams {
   const double *P;        // n x n row-major
   double *J, *K;          // n x n accumulators
   int n;
+  // measurement only: when not NULL, the launch adds the number of primitive
+  // quartets that passed screening (one atomic per warp at its end)
+  unsigned long long *prim_count;
 };
 
 struct EriParams {

@@ -372,6 +372,7 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
   const int NKo = sph ? nsph(LK) : C::NK, NLo = sph ? nsph(LL) : C::NL;
   const int NKO = NKo * NLo, NBO = NIo * NJo;
   const int ntasks = (prm.njobs + C::SLOTS - 1) / C::SLOTS;
+  unsigned long long nprim = 0;   // MODE 1, measurement: primitive quartets run
 
   for (;;) {
     int task = 0;
@@ -466,6 +467,7 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
           // screening (reference src/cint2e.rs:367-393)
           run = !(ket.cce > cut) && !(bra.cce > cut - ket.cce);
           if (++ij == job.nij) { ij = 0; ++kl; }
+          nprim += run && rho == 0;
         }
       }
       // Roots, weights, prefactors and the per-unit coefficients are FP64 in
@@ -606,6 +608,11 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
     }
     if (MODE == 1 && have) fock_digest<C::NI, C::NJ, C::NK, C::NL, R>(Bk, job, wdeg, fk, rho, C::LANES);
     __syncwarp();
+  }
+  if (MODE == 1 && fk.prim_count) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nprim += __shfl_xor_sync(0xffffffffu, nprim, o);
+    if (lane == 0 && nprim) atomicAdd(fk.prim_count, nprim);
   }
 }
 

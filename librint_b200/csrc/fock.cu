@@ -43,7 +43,8 @@ __device__ inline double fac_sp_d(int l) {
 // class prefactor 2 pi^3 / sqrt(pi) (reference src/g2e.rs:74-82).
 __global__ void k_mol_pairs(const PairInfo *__restrict__ pairs, int npairs,
                             const int *__restrict__ atm, const int *__restrict__ bas,
-                            const double *__restrict__ env, PrimPair *pp, int npp_total) {
+                            const double *__restrict__ env, PrimPair *pp, int npp_total,
+                            int gc_screen) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npp_total) return;
   int lo = 0, hi = npairs - 1;
@@ -75,7 +76,11 @@ __global__ void k_mol_pairs(const PairInfo *__restrict__ pairs, int npairs,
   o.fac = ci * cj * exp(-eij) * fac_sp_d(bi[1]) * fac_sp_d(bj[1]) * 5.9149671727956129;
   o.ia = 1.0 / aij;
   o.facia = o.fac * o.ia;
-  o.cce = eij - log_rr - log(fabs(ci)) - log(fabs(cj));
+  // sub-shells of generally contracted shells screen with the largest
+  // |coefficient| over the contractions (bas slot 7)
+  const double sci = gc_screen && bi[7] > 0 ? env[bi[7] + ip] : ci;
+  const double scj = gc_screen && bj[7] > 0 ? env[bj[7] + jp] : cj;
+  o.cce = eij - log_rr - log(fabs(sci)) - log(fabs(scj));
   pp[t] = o;
 }
 
@@ -157,13 +162,17 @@ __global__ void k_screen_sorted(const PairInfo *__restrict__ pairs, const int *_
                                 const double *__restrict__ Q, const int *__restrict__ qorder,
                                 const long long *__restrict__ qoff, int npairs,
                                 const double *__restrict__ Dsh, int nbas, long long ncand,
-                                double tau, int prec, double tau32, int2 *jobs, unsigned *keys,
-                                int *idx, unsigned long long *count, unsigned long long cap) {
+                                double tau, int prec, double tau32, int rank, int nranks,
+                                int2 *jobs, unsigned *keys, int *idx, unsigned long long *count,
+                                unsigned long long cap) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   bool keep = false;
   int b = 0, k = 0;
   unsigned key = 0;
-  if (t < ncand) {
+  // a rank takes the candidates t = rank (mod nranks): the candidate index is
+  // a function of the Schwarz-sorted pair positions only, so every rank
+  // enumerates the same list and the shares are disjoint and complete
+  if (t < ncand && t % nranks == rank) {
     int lo = 0, hi = npairs - 1;   // last position i with qoff[i] <= t
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -179,13 +188,15 @@ __global__ void k_screen_sorted(const PairInfo *__restrict__ pairs, const int *_
     const double bound = Q[b] * Q[k] * d;
     keep = bound >= tau;
     if (keep) {
-      const bool f32 = prec == 1 || (prec == 2 && bound < tau32);
       int cb = pcls[b], ck = pcls[k];
       if (cb < ck) {
         const int tmp = b; b = k; k = tmp;
         const int tc = cb; cb = ck; ck = tc;
       }
-      const int cid = cb * (cb + 1) / 2 + ck + (f32 ? NCLASS : 0);
+      const int cid0 = cb * (cb + 1) / 2 + ck;
+      // classes with an f shell have FP64 kernels only
+      const bool f32 = (prec == 1 || (prec == 2 && bound < tau32)) && cid0 < NCLASS_TPL;
+      const int cid = cid0 + (f32 ? NCLASS : 0);
       const int kprod = pairs[b].npp * pairs[k].npp;
       key = ((unsigned)cid << 20) | (unsigned)(0xfffff - kprod);
     }
@@ -237,8 +248,24 @@ void dens_max_device(MolCtx &m, const double *dP, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------ context
+static int mol_create_segmented(MolCtx &m, const int *atm, int natm, const int *bas, int nbas,
+                                const double *env, long long nenv, cudaStream_t st);
+
+// Generally contracted shells are split into segmented sub-shells first
+// (gc_expand): the AO order is unchanged, so every matrix of the context is
+// the one of the input basis.
 int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, const double *env,
                long long nenv, cudaStream_t st) {
+  GcExpanded x;
+  if (int rc = gc_expand(bas, nbas, env, nenv, x)) return rc;
+  if (!x.any) return mol_create_segmented(m, atm, natm, bas, nbas, env, nenv, st);
+  m.gc = 1;
+  return mol_create_segmented(m, atm, natm, x.bas.data(), (int)(x.bas.size() / 8), x.env.data(),
+                              (long long)x.env.size(), st);
+}
+
+static int mol_create_segmented(MolCtx &m, const int *atm, int natm, const int *bas, int nbas,
+                                const double *env, long long nenv, cudaStream_t st) {
   m.natm = natm; m.nbas = nbas; m.nenv = nenv;
   m.h_atm.assign(atm, atm + 6 * natm);
   m.h_bas.assign(bas, bas + 8 * nbas);
@@ -246,7 +273,7 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
   for (int s = 0; s < nbas; ++s) {
     const int *b = bas + 8 * s;
     if (b[1] < 0 || b[1] > ERI_LMAX || b[3] != 1 || b[2] < 1 || b[2] > ERI_KMAX)
-      return set_error("molecule: shells must have l <= 2, 1..31 primitives, nctr == 1"),
+      return set_error("molecule: shells must have l <= 3 and 1..31 primitives"),
              LRB_ERR_UNSUPPORTED;
     if (b[0] < 0 || b[0] >= natm || b[5] < 0 || b[6] < 0 || (long long)b[5] + b[2] > nenv ||
         (long long)b[6] + b[2] > nenv)
@@ -302,7 +329,8 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
     FK_CK(cudaMemcpyAsync(m.centers, cen.data(), sizeof(double) * 3 * nbas, cudaMemcpyHostToDevice, st));
     FK_CK(cudaStreamSynchronize(st));   // cen goes out of scope
   }
-  k_mol_pairs<<<(npp + 255) / 256, 256, 0, st>>>(m.pairs, m.npairs, m.atm, m.bas, m.env, m.pp, npp);
+  k_mol_pairs<<<(npp + 255) / 256, 256, 0, st>>>(m.pairs, m.npairs, m.atm, m.bas, m.env, m.pp, npp,
+                                                  m.gc);
   engine().launches++;
   FK_CK(cudaGetLastError());
   // Schwarz factors from (IJ|IJ) cartesian blocks
@@ -326,7 +354,7 @@ int mol_create(MolCtx &m, const int *atm, int natm, const int *bas, int nbas, co
   FK_CK(cudaMemcpyAsync(d_dims, dims.data(), sizeof(int) * dims.size(), cudaMemcpyHostToDevice, st));
   FK_CK(cudaMemcpyAsync(d_boff, boff.data(), sizeof(long long) * boff.size(), cudaMemcpyHostToDevice, st));
   int rc = eri_batch_device(engine(), d_blk, 0, d_q, m.npairs, m.atm, natm, m.bas, nbas, m.env,
-                            nenv, st, nullptr);
+                            nenv, st, nullptr, nullptr, m.gc);
   if (rc) return rc;
   k_schwarz<<<(m.npairs + 255) / 256, 256, 0, st>>>(d_blk, d_boff, d_dims, m.npairs, m.Q);
   engine().launches++;
@@ -366,7 +394,9 @@ void mol_destroy(MolCtx &m, cudaStream_t st) {
 
 // ------------------------------------------------------------ build
 int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t st,
-               FockStats *stats, int prec, double tau32, bool accumulate) {
+               FockStats *stats, int prec, double tau32, bool accumulate, int rank, int nranks) {
+  if (nranks < 1 || rank < 0 || rank >= nranks)
+    return set_error("fock: need 0 <= rank < nranks"), LRB_ERR_INPUT;
   Engine &eng = engine();
   const ClassEntry *tab = class_table();
   if (!tab) return LRB_ERR_CUDA;
@@ -398,8 +428,8 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
   const size_t cap = (size_t)std::max(ncand, 1LL);
   const size_t need = carve_size(sizeof(int2) * cap) + 2 * carve_size(sizeof(unsigned) * cap) +
                       2 * carve_size(sizeof(int) * cap) + 2 * carve_size(sizeof(double) * (size_t)n * n) +
-                      carve_size(sizeof(long long) * 64) + carve_size(sizeof(unsigned long long)) +
-                      carve_size(sizeof(int) * 64);
+                      carve_size(sizeof(long long) * 128) + carve_size(sizeof(unsigned long long)) +
+                      carve_size(sizeof(int) * 128);
   char *base = eng.ws.reserve_extra(st, need) ? (char *)eng.ws.extra.ptr : nullptr;
   if (!base) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
   Carver cv(base);
@@ -407,17 +437,17 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
   unsigned *keys = cv.take<unsigned>(cap), *keys2 = cv.take<unsigned>(cap);
   int *idx = cv.take<int>(cap), *idx2 = cv.take<int>(cap);
   double *J = cv.take<double>((size_t)n * n), *K = cv.take<double>((size_t)n * n);
-  long long *starts = cv.take<long long>(64);
+  long long *starts = cv.take<long long>(128);
   unsigned long long *count = cv.take<unsigned long long>(1);
-  int *counters = cv.take<int>(64);
+  int *counters = cv.take<int>(128);
   FK_CK(cudaMemsetAsync(J, 0, sizeof(double) * (size_t)n * n, st));
   FK_CK(cudaMemsetAsync(K, 0, sizeof(double) * (size_t)n * n, st));
   FK_CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
-  FK_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 64, st));
+  FK_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 128, st));
   if (ncand > 0) {
     k_screen_sorted<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(
         m.pairs, m.pcls, m.Q, m.qorder, m.qoff, m.npairs, m.Dsh, nbas, ncand, tau, prec, tau32,
-        jobs, keys, idx, count, cap);
+        rank, nranks, jobs, keys, idx, count, cap);
     ++eng.launches;
   }
   FK_CK(cudaGetLastError());
@@ -432,7 +462,8 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     void *tmp = eng.ws.reserve_aux(st, tmpb + 64);
     if (!tmp) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
     FK_CK(cub::DeviceRadixSort::SortPairs(tmp, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st));
-    k_class_starts_f<<<1, 64, 0, st>>>(keys2, (long long)nj, 2 * NCLASS, starts);
+    static_assert(2 * NCLASS + 1 <= 128, "class starts launch covers 128 ids");
+    k_class_starts_f<<<1, 128, 0, st>>>(keys2, (long long)nj, 2 * NCLASS, starts);
     eng.launches++;
     long long cls_begin[2 * NCLASS + 1];
     FK_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * (2 * NCLASS + 1),
@@ -455,6 +486,12 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     fk.J = J;
     fk.K = K;
     fk.n = n;
+    fk.prim_count = nullptr;
+    if (eng.profile && !eng.fock_prim) {
+      if (cudaMalloc((void **)&eng.fock_prim, 128 * sizeof(unsigned long long)) != cudaSuccess)
+        return set_error("fock: counter allocation failed"), LRB_ERR_ALLOC;
+      FK_CK(cudaMemset(eng.fock_prim, 0, 128 * sizeof(unsigned long long)));
+    }
     for (int cc = 0; cc < 2 * NCLASS; ++cc) {
       const long long b0 = cls_begin[cc], b1 = cls_begin[cc + 1];
       if (b1 <= b0) continue;
@@ -464,20 +501,31 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
       prm.order = idx2 + b0;
       prm.njobs = (int)(b1 - b0);
       int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[fi], ERI_THREADS, ce.smem[fi]);
+      if (ce.gen)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gen_kernel(1), GEN_THREADS, ce.smem[1]);
+      else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[fi], ERI_THREADS, ce.smem[fi]);
       if (per_sm < 1) per_sm = 1;
       const long long tasks = (prm.njobs + ce.slots - 1) / ce.slots;
       long long grid = (long long)nsm * per_sm;
-      const long long needg = (tasks + ERI_WARPS - 1) / ERI_WARPS;
+      const long long needg = ce.gen ? tasks : (tasks + ERI_WARPS - 1) / ERI_WARPS;
       if (grid > needg) grid = needg;
       ProfRecord rec{cc, nullptr, nullptr};
       if (eng.profile) {
         cudaEventCreate(&rec.start);
         cudaEventCreate(&rec.stop);
         cudaEventRecord(rec.start, st);
+        fk.prim_count = eng.fock_prim + cc;
+        eng.fock_quartets[cc] += b1 - b0;
+      } else {
+        fk.prim_count = nullptr;
       }
-      ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(prm, fk, rys + RYS_TAB_OFFSET[ce.nr],
-                                                                  counters + cc);
+      if (ce.gen)
+        gen_kernel(1)<<<(unsigned)grid, GEN_THREADS, ce.smem[1], st>>>(
+            prm, fk, ce.g, rys + RYS_TAB_OFFSET[ce.nr], counters + cc);
+      else
+        ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(
+            prm, fk, rys + RYS_TAB_OFFSET[ce.nr], counters + cc);
       FK_CK(cudaGetLastError());
       eng.launches++;
       if (eng.profile) {

@@ -9,6 +9,7 @@ namespace lrb {
 
 struct MolCtx {
   int natm = 0, nbas = 0, nao = 0, npairs = 0, npp = 0;
+  int gc = 0;   // built from generally contracted shells (h_bas holds the sub-shells)
   long long nenv = 0;
   std::vector<int> h_atm, h_bas, h_aooff;
   std::vector<double> h_env;
@@ -63,8 +64,12 @@ void mol_destroy(MolCtx &m, cudaStream_t st);
 // quartets whose Schwarz x density bound is below tau32.  FP32 quartets
 // compute the recurrences and the digestion in FP32 and add into the FP64
 // J/K accumulators; roots and weights stay FP64.
+// rank / nranks: the share of the screened quartets this call digests (the
+// candidates whose enumeration index is rank mod nranks); the shares of all
+// ranks sum to the full G.
 int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t st,
-               FockStats *stats, int prec = 0, double tau32 = 0.0, bool accumulate = false);
+               FockStats *stats, int prec = 0, double tau32 = 0.0, bool accumulate = false,
+               int rank = 0, int nranks = 1);
 void fill_c2s(double *c);
 int int1e_device(int typec, int coord, const int *d_atm, int natm, const int *d_bas, int nbas,
                  const double *d_env, const int *h_bas, double *out, cudaStream_t st,

@@ -36,6 +36,16 @@ GradEntry g_grad_classes[NGRADCLS][NGRADMODE];
 
 // Kernel pointers and shared-memory sizes are filled once per process; the
 // large-shared-memory attribute is per device and set for each device used.
+// The adjoint kernels cover shells up to d.
+static int grad_shells_supported(const MolCtx &m) {
+  if (m.gc) return set_error("gradients: generally contracted shells are not supported"),
+            LRB_ERR_UNSUPPORTED;
+  for (int s = 0; s < m.nbas; ++s)
+    if (m.h_bas[8 * s + 1] > 2)
+      return set_error("gradients: shells up to l = 2 are supported"), LRB_ERR_UNSUPPORTED;
+  return LRB_OK;
+}
+
 static int grad_table_init() {
   constexpr int kMaxDevices = 64;
   static std::mutex mu;
@@ -539,6 +549,7 @@ static int grad_eri_pass(MolCtx &m, const double *Ps, double tau, int slot0, int
 
 int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, double tau,
              double *d_grad, int s1, cudaStream_t st) {
+  if (int rc0 = grad_shells_supported(m)) return rc0;
   if (int rc0 = grad_table_init()) return rc0;
   Engine &eng = engine();
   const int n = m.nao, nbas = m.nbas;
@@ -613,6 +624,7 @@ int grad_run(MolCtx &m, const double *d_P, double cH, double cR, double cS, doub
 }
 
 int dS_u_run(MolCtx &m, int s1, int L, double *d_out, cudaStream_t st) {
+  if (int rc0 = grad_shells_supported(m)) return rc0;
   const int n = m.nao, nbas = m.nbas;
   const long long nn = (long long)n * n;
   std::vector<int> ao_shell, ao_comp;
@@ -632,6 +644,7 @@ int dS_u_run(MolCtx &m, int s1, int L, double *d_out, cudaStream_t st) {
 }
 
 int d1e_env_run(MolCtx &m, int op, double *d_out, cudaStream_t st) {
+  if (int rc0 = grad_shells_supported(m)) return rc0;
   const int n = m.nao, nbas = m.nbas;
   const long long nn = (long long)n * n;
   std::vector<int> ao_shell, ao_comp;
@@ -652,6 +665,7 @@ int d1e_env_run(MolCtx &m, int op, double *d_out, cudaStream_t st) {
 }
 
 int grad_nuc_run(MolCtx &m, const double *d_P, double tau, double *d_gatom, cudaStream_t st) {
+  if (int rc0 = grad_shells_supported(m)) return rc0;
   if (int rc0 = grad_table_init()) return rc0;
   Engine &eng = engine();
   const int n = m.nao, nbas = m.nbas;

@@ -52,6 +52,29 @@ class MolContext:
         B.check(rc, "lrb_fock_G")
         return G
 
+    def fock_G_part(self, P, tau: float, rank: int, nranks: int):
+        """This rank's share of G(P) (lrb_fock_G_part); the shares of ranks
+        0..nranks-1 sum to fock_G(P, tau).  Returns (G share, quartets)."""
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        G = np.empty_like(P)
+        nq = ctypes.c_longlong(0)
+        rc = B.lib().lrb_fock_G_part(self.h, P.ctypes.data_as(B.P_d), G.ctypes.data_as(B.P_d), tau,
+                                     rank, nranks, ctypes.byref(nq))
+        B.check(rc, "lrb_fock_G_part")
+        return G, nq.value
+
+    def fock_G_part_device(self, P, G, tau: float, rank: int, nranks: int, stream=None):
+        """Device form: P and G are device tensors (n x n float64, contiguous)
+        on the current device; runs on ``stream`` (default: the current
+        torch stream)."""
+        import torch
+        st = torch.cuda.current_stream() if stream is None else stream
+        nq = ctypes.c_longlong(0)
+        rc = B.lib().lrb_fock_G_part_device(self.h, P.data_ptr(), G.data_ptr(), tau, rank, nranks,
+                                            ctypes.byref(nq), ctypes.c_void_p(st.cuda_stream))
+        B.check(rc, "lrb_fock_G_part_device")
+        return nq.value
+
     def fock_G_prec(self, P, prec: int, tau: float = 0.0, tau32: float = 0.0):
         """G(P) with the mixed-precision kernels (0 FP64, 1 FP32, 2 FP32 for
         quartets with Schwarz x density bound below tau32); returns

@@ -12,15 +12,18 @@ contraction coefficients are positive and PySCF-normalised
 * ``eri_sweep``      -- independent shell quartets of one angular class; every
   shell has its own centre (uniform in a 10 A cube), K uniform in 1..6 and
   exponents log-uniform in [0.05, 5000].
-* ``hc_cluster``     -- C on a perturbed hexagonal lattice (C-C 1.40 +- 0.05 A)
-  with H at 1.09 A on edge carbons; the even-tempered DZP-like set
-  (``DZP_C``/``DZP_H``: C 3s2p1d, H 2s1p).
+* ``ch_basis``       -- the C/H basis every C/H system below uses: one shell
+  set per element drawn from seed 3 (C 3s2p1d, H 2s1p, K uniform in 1..6,
+  exponents log-uniform in [0.1, 5000] for C and [0.1, 50] for H).
+* ``c3_cluster``     -- the 60-atom RHF system: 36 C on a perturbed hexagonal
+  lattice (C-C 1.40 +- 0.05 A) and 24 H at 1.09 A on edge carbons,
+  660 cartesian AOs.
+* ``hc_cluster``     -- the same flake construction for any carbon count.
 * ``hc_chain``       -- zig-zag C_nH_(2n+2) chain, C-C 1.54 A, C-H 1.09 A,
-  +-0.03 A noise, random C 3s2p1d / H 2s1p shells (K uniform in 1..6).
+  +-0.03 A noise (n = 6: 20 atoms).
 * ``flake_like``     -- hc_cluster construction with 8..20 carbons, for
   training the learned guess on flake environments.
-* ``benzene_like``   -- C6H6 ring, bonds +-0.05 A, angles +-3 deg, the
-  DZP-like set (or random shells per element from ``basis_seed``).
+* ``benzene_like``   -- C6H6 ring, bonds +-0.05 A, angles +-3 deg.
 """
 from __future__ import annotations
 
@@ -134,6 +137,7 @@ C_SHELLS = (0, 0, 0, 1, 1, 2)       # 3s2p1d
 H_SHELLS = (0, 0, 1)                # 2s1p
 C_RANGE = (0.1, 5000.0)
 H_RANGE = (0.1, 50.0)
+CH_BASIS_SEED = 3                   # the one basis every C/H system here uses
 
 
 def _draw_shells(rng, z, kmax):
@@ -145,74 +149,57 @@ def _draw_shells(rng, z, kmax):
     return out
 
 
-def _add_ch_basis(b: Builder, rng, atoms_z, kmax=6, per_element=False):
-    """Per-atom random shells, or (per_element) one draw per element shared
-    by every atom of that element, like a named basis set."""
-    table = {}
-    if per_element:
-        for z in sorted(set(atoms_z), reverse=True):
-            table[z] = _draw_shells(rng, z, kmax)
-    for atom, z in enumerate(atoms_z):
-        for l, e, c in (table[z] if per_element else _draw_shells(rng, z, kmax)):
-            b.add_shell(atom, l, e, c)
+def ch_basis(seed: int = CH_BASIS_SEED, kmax: int = 6) -> dict:
+    """One shell set per element, like a named basis: C 3s2p1d, H 2s1p, K
+    uniform in 1..kmax per shell, exponents log-uniform in [0.1, 5000] (C)
+    or [0.1, 50] (H), coefficients uniform in [0.2, 1] (normalised when the
+    shell is added).  C is drawn first, then H, from default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    return {z: _draw_shells(rng, z, kmax) for z in (6, 1)}
 
 
-# Even-tempered split-valence set with polarisation ("DZP-like"): C 3s2p1d,
-# H 2s1p, the same shell counts as the random sets above.  The exponents are
-# round geometric sequences chosen for this library (not a published basis);
-# coefficients are positive and normalised like every other shell here.
-DZP_C = ((0, (3000.0, 450.0, 100.0, 28.0, 9.0, 3.2), (0.002, 0.015, 0.07, 0.24, 0.48, 0.33)),
-         (0, (7.5, 1.8, 0.55), (0.05, 0.3, 0.75)),
-         (0, (0.16,), (1.0,)),
-         (1, (18.0, 4.2, 1.2, 0.38), (0.04, 0.24, 0.5, 0.45)),
-         (1, (0.12,), (1.0,)),
-         (2, (0.8,), (1.0,)))
-DZP_H = ((0, (19.0, 2.9, 0.65), (0.035, 0.23, 0.82)),
-         (0, (0.16,), (1.0,)),
-         (1, (0.75,), (1.0,)))
-
-
-def _add_dzp_basis(b: Builder, atoms_z):
-    for atom, z in enumerate(atoms_z):
-        for l, e, c in (DZP_C if z == 6 else DZP_H):
-            b.add_shell(atom, l, np.array(e), np.array(c))
-
-
-def _build_ch(z, xyz_ang, rng, name, per_element=False, dzp=False, **meta):
+def _build_ch(z, xyz_ang, name, basis_seed=CH_BASIS_SEED, **meta):
     b = Builder()
     for zi, r in zip(z, xyz_ang):
         b.add_atom(zi, np.asarray(r) * ANG2BOHR)
-    if dzp:
-        _add_dzp_basis(b, z)
-    else:
-        _add_ch_basis(b, rng, z, per_element=per_element)
-    return b.build(name, **meta)
+    table = ch_basis(basis_seed)
+    for atom, zi in enumerate(z):
+        for l, e, c in table[zi]:
+            b.add_shell(atom, l, e, c)
+    return b.build(name, basis_seed=basis_seed, **meta)
 
 
-def hc_cluster(seed: int = 3, ncarbon: int = 34, aspect: float = 2.0) -> Molecule:
-    """54-atom C/H flake: the ``ncarbon`` honeycomb sites nearest the origin in
-    the metric sqrt(x^2 + (aspect*y)^2) (an elongated flake, so enough edge
-    sites carry H), C-C 1.40 A perturbed by +-0.05 A; one H on each carbon
-    with two carbon neighbours, two (tilted out of plane) on each carbon with
-    one.  34 C + 20 H (224 electrons), 610 cartesian AOs, the DZP-like set."""
-    rng = np.random.default_rng(seed)
-    a = 1.40
+def _honeycomb(a=1.40, n=10):
     pts = []
-    for i in range(-10, 11):
-        for j in range(-10, 11):
+    for i in range(-n, n + 1):
+        for j in range(-n, n + 1):
             o = np.array([i * 1.5 * a, (i + 2 * j) * math.sqrt(3) / 2 * a])
             pts.append(o + np.array([a / 2, 0.0]))
             pts.append(o + np.array([-a / 2, 0.0]))
-    pts = np.unique(np.round(np.array(pts), 6), axis=0)
-    d = np.sqrt(pts[:, 0] ** 2 + (aspect * pts[:, 1]) ** 2)
+    return np.unique(np.round(np.array(pts), 6), axis=0)
+
+
+def _flake(rng, ncarbon, aspect, theta_deg=0.0, shift=(0.0, 0.0)):
+    """C/H flake geometry (Angstrom): the ``ncarbon`` honeycomb sites
+    (C-C 1.40 A) nearest ``shift`` in the metric sqrt(x'^2 + (aspect y')^2)
+    of axes rotated by theta_deg (an elongated flake, so enough edge sites
+    carry H); one H at 1.09 A on each carbon with two carbon neighbours, two
+    (tilted out of plane) on each carbon with one; carbons perturbed by
+    +-0.05 A in bond length.  Returns (Z list, xyz)."""
+    a = 1.40
+    pts = _honeycomb(a)
+    t = math.radians(theta_deg)
+    rot = np.array([[math.cos(t), -math.sin(t)], [math.sin(t), math.cos(t)]])
+    q = (pts - np.asarray(shift)) @ rot.T
+    d = np.sqrt(q[:, 0] ** 2 + (aspect * q[:, 1]) ** 2)
     c2 = pts[np.argsort(d, kind="stable")[:ncarbon]]
     hs = []
     tilt = math.radians(54.75)
     for p in c2:
-        nb = [q for q in c2 if 0.1 < np.linalg.norm(q - p) < 1.1 * a]
+        nb = [x for x in c2 if 0.1 < np.linalg.norm(x - p) < 1.1 * a]
         if len(nb) >= 3 or not nb:
             continue
-        v = -sum((q - p) / np.linalg.norm(q - p) for q in nb)
+        v = -sum((x - p) / np.linalg.norm(x - p) for x in nb)
         v = np.append(v / np.linalg.norm(v), 0.0)
         p3 = np.append(p, 0.0)
         if len(nb) == 2:
@@ -222,9 +209,23 @@ def hc_cluster(seed: int = 3, ncarbon: int = 34, aspect: float = 2.0) -> Molecul
                 hs.append(p3 + 1.09 * (math.cos(tilt) * v + sz * math.sin(tilt) * np.array([0, 0, 1.0])))
     c3 = np.column_stack([c2, np.zeros(len(c2))])
     c3 += rng.uniform(-0.05, 0.05, size=c3.shape) / math.sqrt(3)
-    xyz = np.vstack([c3, np.array(hs)])
-    z = [6] * len(c3) + [1] * len(hs)
-    return _build_ch(z, xyz, rng, "hc_cluster", dzp=True, seed=seed)
+    return [6] * len(c3) + [1] * len(hs), np.vstack([c3, np.array(hs)])
+
+
+def c3_cluster(seed: int = 3) -> Molecule:
+    """The ~600-AO RHF system: 60-atom C/H flake, 36 C + 24 H (240
+    electrons), C on a perturbed hexagonal lattice (1.40 +- 0.05 A), H at
+    1.09 A on edge carbons, the seed-3 per-element basis (C 3s2p1d, H 2s1p,
+    K = 1..6, log-uniform exponents): 288 shells, 660 cartesian AOs."""
+    z, xyz = _flake(np.random.default_rng(seed), 36, 3.0, 10.0, (0.35, 0.0))
+    return _build_ch(z, xyz, "c3_cluster", seed=seed)
+
+
+def hc_cluster(seed: int = 3, ncarbon: int = 34, aspect: float = 2.0) -> Molecule:
+    """Flake of ``ncarbon`` carbons (``_flake`` with the metric unrotated),
+    the per-element basis."""
+    z, xyz = _flake(np.random.default_rng(seed), ncarbon, aspect)
+    return _build_ch(z, xyz, "hc_cluster", seed=seed)
 
 
 def flake_like(seed: int) -> Molecule:
@@ -243,7 +244,9 @@ def flake_like(seed: int) -> Molecule:
         nc += 1
 
 
-def hc_chain(seed: int = 4, ncarbon: int = 6) -> Molecule:
+def hc_chain(seed: int = 4, ncarbon: int = 6, basis_seed: int = CH_BASIS_SEED) -> Molecule:
+    """Zig-zag C_nH_(2n+2) chain (C-C 1.54 A, C-H 1.09 A, +-0.03 A noise on
+    every coordinate); n = 6 gives the 20-atom chain (160 cartesian AOs)."""
     rng = np.random.default_rng(seed)
     cc, ch = 1.54, 1.09
     ang = math.radians(109.47)
@@ -263,14 +266,13 @@ def hc_chain(seed: int = 4, ncarbon: int = 6) -> Molecule:
     xyz = np.vstack([cs, np.array(hs)])
     xyz += rng.uniform(-0.03, 0.03, size=xyz.shape)
     z = [6] * ncarbon + [1] * len(hs)
-    return _build_ch(z, xyz, rng, "hc_chain", seed=seed)
+    return _build_ch(z, xyz, "hc_chain", basis_seed=basis_seed, seed=seed)
 
 
-def benzene_like(seed: int = 5, basis_seed: int | None = None) -> Molecule:
-    """One C6H6-like ring; geometry from ``seed``.  Basis: the even-tempered
-    DZP-like set (``basis_seed=None``) or random shells drawn from
-    ``basis_seed``, one shell set per element either way (C 3s2p1d = 15,
-    H 2s1p = 5 cartesian AOs; 120 AOs in all)."""
+def benzene_like(seed: int = 5, basis_seed: int = CH_BASIS_SEED) -> Molecule:
+    """One C6H6-like ring; geometry from ``seed`` (bonds +-0.05 A, angles
+    +-3 deg); basis: the per-element set drawn from ``basis_seed`` (C
+    3s2p1d = 15, H 2s1p = 5 cartesian AOs; 120 AOs in all)."""
     rng = np.random.default_rng(seed)
     cc, ch = 1.40, 1.09
     cs, hs = [], []
@@ -281,7 +283,4 @@ def benzene_like(seed: int = 5, basis_seed: int | None = None) -> Molecule:
         rh = r + ch + rng.uniform(-0.05, 0.05)
         hs.append([rh * math.cos(t), rh * math.sin(t), 0.0])
     xyz = np.vstack([cs, hs])
-    if basis_seed is None:
-        return _build_ch([6] * 6 + [1] * 6, xyz, None, "benzene_like", dzp=True, seed=seed)
-    return _build_ch([6] * 6 + [1] * 6, xyz, np.random.default_rng(basis_seed), "benzene_like",
-                     per_element=True, seed=seed, basis_seed=basis_seed)
+    return _build_ch([6] * 6 + [1] * 6, xyz, "benzene_like", basis_seed=basis_seed, seed=seed)

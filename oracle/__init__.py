@@ -49,6 +49,12 @@ def lib():
         L.orc_energy.restype = _d
         L.orc_scf.argtypes = (_sz, _i, _d, _pi, _i, _pi, _i, _pd, _i)
         L.orc_scf.restype = _d
+        L.orc_fock_G_quartets.argtypes = (_pd, _pd, _pi, ctypes.c_long, _pi, _i, _pi, _i, _pd, _i)
+        L.orc_fock_G_blocks.argtypes = (_pd, _pd, _pi, _i, _pi, _i, _pi, _i, _pd, _i)
+        L.orc_energy2_sym.argtypes = (_pd, _pi, _i, _pi, _i, _pd, _i)
+        L.orc_energy2_sym.restype = _d
+        L.orc_energy1.argtypes = (_pd, _pi, _i, _pi, _i, _pd)
+        L.orc_energy1.restype = _d
         L.orc_nao.argtypes = (_i, _pi, _i)
         L.orc_nao.restype = _i
         _LIB = L
@@ -131,6 +137,46 @@ def fock_G(m, P, coord=0, nthreads=0):
     lib().orc_fock_G(_p(G, _pd), _p(P, _pd), coord, _p(atm, _pi), atm.size // 6, _p(bas, _pi),
                      bas.size // 8, _p(env, _pd), nthreads)
     return G.reshape(n, n)
+
+
+def fock_G_quartets(m, P, shls, nthreads=0):
+    """The reference's digestion over the listed quartets only ((nq, 4)
+    int32, each visited once as one slot of its nbas^4 loop)."""
+    atm, bas, env = _mol(m)
+    n = nao(m, 0)
+    P = np.ascontiguousarray(P, dtype=np.float64)
+    sh = np.ascontiguousarray(shls, dtype=np.int32)
+    G = np.zeros(n * n)
+    lib().orc_fock_G_quartets(_p(G, _pd), _p(P, _pd), _p(sh, _pi), sh.shape[0], _p(atm, _pi),
+                              atm.size // 6, _p(bas, _pi), bas.size // 8, _p(env, _pd), nthreads)
+    return G.reshape(n, n)
+
+
+def fock_G_blocks(m, P, pairs, nthreads=0):
+    """G(P) blocks for shell pairs [(X, Y), ...], exact (2 nbas^2 quartets per
+    block); returns a list of (nX, nY) arrays."""
+    atm, bas, env = _mol(m)
+    P = np.ascontiguousarray(P, dtype=np.float64)
+    pr = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+    b = bas.reshape(-1, 8)
+    dims = [(int((b[x, 1] + 1) * (b[x, 1] + 2) // 2), int((b[y, 1] + 1) * (b[y, 1] + 2) // 2))
+            for x, y in pr]
+    out = np.zeros(sum(a * c for a, c in dims))
+    lib().orc_fock_G_blocks(_p(out, _pd), _p(P, _pd), _p(pr, _pi), pr.shape[0], _p(atm, _pi),
+                            atm.size // 6, _p(bas, _pi), bas.size // 8, _p(env, _pd), nthreads)
+    res, o = [], 0
+    for a, c in dims:
+        res.append(out[o:o + a * c].reshape(a, c))
+        o += a * c
+    return res
+
+
+def energy_sym(m, P, nthreads=0):
+    """Energy functional through the unique-quartet two-electron sum."""
+    atm, bas, env = _mol(m)
+    P = np.ascontiguousarray(P, dtype=np.float64)
+    a = (_p(P, _pd), _p(atm, _pi), atm.size // 6, _p(bas, _pi), bas.size // 8, _p(env, _pd))
+    return lib().orc_energy1(*a) + lib().orc_energy2_sym(*a, nthreads)
 
 
 def density(m, nelec=None, imax=200, conv=1e-10, nthreads=0):

@@ -796,6 +796,158 @@ void orc_fock_G(double *G, const double *P, int coord, const int *atm, int, cons
   }
 }
 
+// One quartet's digestion, the reference's loop body (src/scf.rs:379-391):
+// slot (mu nu | sig lam): G[mu,nu] += P[lam,sig] v; G[mu,lam] -= P[nu,sig] v / 2.
+static void digest_quartet(double *G, const double *P, size_t n, const std::vector<int> &off,
+                           const int shls[4], const double *buf) {
+  const int i = shls[0], j = shls[1], k = shls[2], l = shls[3];
+  const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
+  const int dk = off[k + 1] - off[k], dl = off[l + 1] - off[l];
+  size_t c = 0;
+  for (int L = 0; L < dl; ++L)
+    for (int K = 0; K < dk; ++K)
+      for (int J = 0; J < dj; ++J)
+        for (int I = 0; I < di; ++I, ++c) {
+          const size_t mu = off[i] + I, nu = off[j] + J, sg = off[k] + K, lm = off[l] + L;
+          const double v = buf[c];
+          G[mu * n + nu] += P[lm * n + sg] * v;
+          G[mu * n + lm] += -0.5 * P[nu * n + sg] * v;
+        }
+}
+
+void orc_fock_G_quartets(double *G, const double *P, const int *shls, long nq, const int *atm,
+                         int, const int *bas, int nbas, const double *env, int nthreads) {
+  const std::vector<int> off = shell_offsets(0, bas, nbas);
+  const size_t n = off[nbas];
+  std::memset(G, 0, n * n * sizeof(double));
+  const int nt = threads_or_default(nthreads);
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<double> Gl(n * n, 0.0), buf;
+#pragma omp for schedule(dynamic, 64)
+    for (long q = 0; q < nq; ++q) {
+      const int *s4 = shls + 4 * q;
+      size_t d = 1;
+      for (int a = 0; a < 4; ++a) d *= off[s4[a] + 1] - off[s4[a]];
+      buf.resize(d);
+      quartet_block(buf.data(), 0, s4, atm, bas, env);
+      digest_quartet(Gl.data(), P, n, off, s4, buf.data());
+    }
+#pragma omp critical
+    for (size_t x = 0; x < n * n; ++x) G[x] += Gl[x];
+  }
+}
+
+void orc_fock_G_blocks(double *out, const double *P, const int *pairs, int npairs,
+                       const int *atm, int, const int *bas, int nbas, const double *env,
+                       int nthreads) {
+  const std::vector<int> off = shell_offsets(0, bas, nbas);
+  const size_t n = off[nbas];
+  std::vector<size_t> boff(npairs + 1, 0);
+  for (int p = 0; p < npairs; ++p)
+    boff[p + 1] = boff[p] + (size_t)(off[pairs[2 * p] + 1] - off[pairs[2 * p]]) *
+                                (off[pairs[2 * p + 1] + 1] - off[pairs[2 * p + 1]]);
+  std::memset(out, 0, boff[npairs] * sizeof(double));
+  const int nt = threads_or_default(nthreads);
+  // Block (X, Y): every quartet of the reference's nbas^4 loop whose digestion
+  // touches G[mu in X, nu in Y]: (X Y | K L) through the first update and
+  // (X J | K Y) through the second.
+  for (int p = 0; p < npairs; ++p) {
+    const int X = pairs[2 * p], Y = pairs[2 * p + 1];
+    const int dx = off[X + 1] - off[X], dy = off[Y + 1] - off[Y];
+#pragma omp parallel num_threads(nt)
+    {
+      std::vector<double> loc((size_t)dx * dy, 0.0), buf;
+#pragma omp for schedule(dynamic) collapse(2)
+      for (int a = 0; a < nbas; ++a)
+        for (int b = 0; b < nbas; ++b) {
+          for (int pass = 0; pass < 2; ++pass) {
+            // pass 0: (X Y | a b), G[mu,nu] += P[lam,sig] v
+            // pass 1: (X a | b Y), G[mu,lam] -= P[nu,sig] v / 2
+            const int s4[4] = {X, pass == 0 ? Y : a, pass == 0 ? a : b, pass == 0 ? b : Y};
+            const int d0 = off[s4[0] + 1] - off[s4[0]], d1 = off[s4[1] + 1] - off[s4[1]];
+            const int d2 = off[s4[2] + 1] - off[s4[2]], d3 = off[s4[3] + 1] - off[s4[3]];
+            buf.resize((size_t)d0 * d1 * d2 * d3);
+            quartet_block(buf.data(), 0, s4, atm, bas, env);
+            size_t c = 0;
+            for (int L = 0; L < d3; ++L)
+              for (int K = 0; K < d2; ++K)
+                for (int J = 0; J < d1; ++J)
+                  for (int I = 0; I < d0; ++I, ++c) {
+                    const size_t nu = off[s4[1]] + J, sg = off[s4[2]] + K, lm = off[s4[3]] + L;
+                    if (pass == 0)
+                      loc[(size_t)I * dy + J] += P[lm * n + sg] * buf[c];
+                    else
+                      loc[(size_t)I * dy + L] += -0.5 * P[nu * n + sg] * buf[c];
+                  }
+          }
+        }
+#pragma omp critical
+      for (size_t x = 0; x < (size_t)dx * dy; ++x) out[boff[p] + x] += loc[x];
+    }
+  }
+}
+
+double orc_energy2_sym(const double *P, const int *atm, int, const int *bas, int nbas,
+                       const double *env, int nthreads) {
+  // 1/2 sum P G(P) over unique quartets: with the 8-fold permutational
+  // symmetry of (ab|cd) and a symmetric P, 1/2 sum_{abcd} (ab|cd)
+  // [P_ab P_cd - 1/4 (P_ac P_bd + P_ad P_bc)] equals 1/2 tr(P G(P)) of the
+  // reference's digestion (src/scf.rs:379-391); each unique shell quartet
+  // carries its degeneracy weight.
+  const std::vector<int> off = shell_offsets(0, bas, nbas);
+  const size_t n = off[nbas];
+  const long npair = (long)nbas * (nbas + 1) / 2;
+  std::vector<int> pi(npair), pj(npair);
+  for (int i = 0, p = 0; i < nbas; ++i)
+    for (int j = 0; j <= i; ++j, ++p) { pi[p] = i; pj[p] = j; }
+  double total = 0.0;
+  const int nt = threads_or_default(nthreads);
+#pragma omp parallel num_threads(nt) reduction(+ : total)
+  {
+    std::vector<double> buf;
+#pragma omp for schedule(dynamic, 1)
+    for (long bra = npair - 1; bra >= 0; --bra) {
+      const int i = pi[bra], j = pj[bra];
+      double acc = 0.0;
+      for (long ket = 0; ket <= bra; ++ket) {
+        const int k = pi[ket], l = pj[ket];
+        const int s4[4] = {i, j, k, l};
+        const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
+        const int dk = off[k + 1] - off[k], dl = off[l + 1] - off[l];
+        buf.resize((size_t)di * dj * dk * dl);
+        if (!quartet_block(buf.data(), 0, s4, atm, bas, env)) continue;
+        const double w = (i != j ? 2.0 : 1.0) * (k != l ? 2.0 : 1.0) * (bra != ket ? 2.0 : 1.0);
+        double s = 0.0;
+        size_t c = 0;
+        for (int L = 0; L < dl; ++L)
+          for (int K = 0; K < dk; ++K)
+            for (int J = 0; J < dj; ++J)
+              for (int I = 0; I < di; ++I, ++c) {
+                const size_t a = off[i] + I, b = off[j] + J, cc = off[k] + K, d = off[l] + L;
+                s += buf[c] * (P[a * n + b] * P[cc * n + d] -
+                               0.25 * (P[a * n + cc] * P[b * n + d] + P[a * n + d] * P[b * n + cc]));
+              }
+        acc += w * s;
+      }
+      total += acc;
+    }
+  }
+  return 0.5 * total;
+}
+
+double orc_energy1(const double *P, const int *atm, int natm, const int *bas, int nbas,
+                   const double *env) {
+  const int n = orc_nao(0, bas, nbas);
+  const size_t nn = (size_t)n * n;
+  std::vector<double> T(nn), V(nn);
+  orc_int1e(T.data(), 0, 1, atm, natm, bas, nbas, env);
+  orc_int1e(V.data(), 0, 2, atm, natm, bas, nbas, env);
+  double e1 = 0.0;
+  for (size_t x = 0; x < nn; ++x) e1 += P[x] * (T[x] + V[x]);
+  return e1 + nuclear_repulsion(atm, natm, env);
+}
+
 int orc_density(double *Pout, size_t nelec, int imax, double conv, const int *atm, int natm,
                 const int *bas, int nbas, const double *env, int nthreads, int *iters) {
   const int n = orc_nao(0, bas, nbas);

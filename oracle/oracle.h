@@ -51,6 +51,29 @@ void orc_int1e(double *out, int coord, int typec, const int *atm, int natm,
 void orc_fock_G(double *G, const double *P, int coord, const int *atm, int natm,
                 const int *bas, int nbas, const double *env, int nthreads);
 
+/* The same digestion over a given list of shell quartets (shls[4*q..]),
+ * each visited once in the reference's slot order -- a bounded sample of
+ * the nbas^4 loop for timing. */
+void orc_fock_G_quartets(double *G, const double *P, const int *shls, long nq,
+                         const int *atm, int natm, const int *bas, int nbas,
+                         const double *env, int nthreads);
+
+/* G restricted to shell-pair blocks (X, Y) = pairs[2p], pairs[2p+1]: every
+ * term of the reference's nbas^4 digestion that lands in G[mu in X, nu in Y],
+ * summed exactly; blocks packed back to back, row-major (mu, nu).  Cost
+ * 2 nbas^2 quartets per block, so it checks large molecules block-wise. */
+void orc_fock_G_blocks(double *out, const double *P, const int *pairs, int npairs,
+                       const int *atm, int natm, const int *bas, int nbas,
+                       const double *env, int nthreads);
+
+/* 1/2 sum P G(P) over the unique quartets (8-fold symmetry, degeneracy
+ * weights), and the one-electron plus nuclear part sum P (T + V) + E_nn:
+ * their sum is the reference's energy functional (src/scf.rs:827-956). */
+double orc_energy2_sym(const double *P, const int *atm, int natm, const int *bas,
+                       int nbas, const double *env, int nthreads);
+double orc_energy1(const double *P, const int *atm, int natm, const int *bas, int nbas,
+                   const double *env);
+
 /* RHF in the cartesian basis (src/scf.rs:743-969).  density returns 0 on
  * success, 1 near-singular S, 2 not converged, 3 invalid density. */
 int orc_density(double *P, size_t nelec, int imax, double conv,

@@ -8,6 +8,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "reference_golden.npz")
+GOLDEN_FGC = os.path.join(ROOT, "tests", "golden", "reference_fgc.npz")
 
 # Per-integral tolerance used throughout: relative 1e-12 with an absolute floor
 # of 1e-15 Hartree.  Below ~1e-20 both the reference and the oracle lose
@@ -25,6 +26,25 @@ def pytest_configure(config):
 def golden():
     import numpy as np
     return np.load(GOLDEN)
+
+
+@pytest.fixture(scope="session")
+def golden_fgc():
+    """f-shell and general-contraction vectors from the reference's shipped
+    library (tests/golden/make_golden_fgc.py)."""
+    import numpy as np
+    return np.load(GOLDEN_FGC)
+
+
+def fgc_molecule(g, key):
+    from librint_b200.basis import Molecule
+    atm = g[key + "/atm"]
+    return Molecule(atm, g[key + "/bas"], g[key + "/env"], int(atm.reshape(-1, 6)[:, 0].sum()))
+
+
+def f_classes():
+    from librint_b200 import synthetic
+    return [c for c in synthetic.canonical_classes(3) if max(c) == 3]
 
 
 def assert_eri_close(got, ref, rtol=ERI_RTOL, atol=ERI_ATOL, what=""):
@@ -79,3 +99,61 @@ def assert_eri_close_or_exact(got, ref, m, shls, coord, gpu_cart, what="", max_q
         e_or, e_gpu = np.abs(o - ex).max(), np.abs(g - ex).max()
         assert e_gpu <= 4.0 * e_or + ERI_ATOL, \
             f"{what} quartet {q}: GPU error vs exact {e_gpu:.3e}, oracle's {e_or:.3e}"
+
+
+def segmented_copy(m):
+    """The molecule with every generally contracted shell split into its
+    contractions (consecutive segmented shells, same AO order) and, per AO,
+    its (segmented shell, cartesian component)."""
+    import numpy as np
+    from librint_b200.basis import Molecule
+    b = np.asarray(m.bas).reshape(-1, 8)
+    nb, ao = [], []
+    for row in b:
+        l, k, nc = int(row[1]), int(row[2]), int(row[3])
+        for c in range(nc):
+            nb.append([row[0], l, k, 1, 0, row[5], row[6] + c * k, 0])
+            ao += [(len(nb) - 1, comp) for comp in range((l + 1) * (l + 2) // 2)]
+    return Molecule(m.atm, np.array(nb, dtype=np.int32).ravel(), m.env, m.nelec), ao
+
+
+def assert_cart_elements_close_or_exact(got, ref, m, idx, what="", max_elements=64):
+    """Sampled elements (flat indices into the n^4 cartesian tensor) against
+    ref at the per-integral tolerance; where they differ, a 40-digit
+    evaluation (oracle/mp_exact.py, generally contracted shells split)
+    decides: got may not be further from it than 4x ref's error + 1e-15."""
+    import numpy as np
+    from oracle import mp_exact
+    got, ref = np.asarray(got), np.asarray(ref)
+    bad = np.nonzero(np.abs(got - ref) > ERI_RTOL * np.abs(ref) + ERI_ATOL)[0]
+    assert len(bad) <= max_elements, f"{what}: {len(bad)} elements outside tolerance"
+    if not len(bad):
+        return
+    ms, ao = segmented_copy(m)
+    n = len(ao)
+    bs = np.asarray(ms.bas).reshape(-1, 8)
+    for e in bad:
+        a, b, c, d = np.unravel_index(int(idx[e]), (n, n, n, n))
+        sh = [ao[a][0], ao[b][0], ao[c][0], ao[d][0]]
+        comp = [ao[a][1], ao[b][1], ao[c][1], ao[d][1]]
+        nf = [(bs[s, 1] + 1) * (bs[s, 1] + 2) // 2 for s in sh]
+        ex = mp_exact.eri_cart_exact(ms.atm, ms.bas, ms.env, sh)
+        v = ex[comp[0] + nf[0] * (comp[1] + nf[1] * (comp[2] + nf[2] * comp[3]))]
+        assert abs(got[e] - v) <= 4.0 * abs(ref[e] - v) + ERI_ATOL, \
+            f"{what} element {idx[e]}: error {abs(got[e] - v):.3e} vs exact, reference's {abs(ref[e] - v):.3e}"
+
+
+def assert_block_close_or_exact(got, ref, m, shls, what=""):
+    """One cartesian quartet block (libcint layout, i fastest, as an array
+    indexed [i, j, k, l]) against ref, arbitrated element-wise by the
+    40-digit evaluation where the two differ beyond the tolerance."""
+    import numpy as np
+    from oracle import mp_exact
+    got, ref = np.asarray(got), np.asarray(ref)
+    bad = np.abs(got - ref) > ERI_RTOL * np.abs(ref) + ERI_ATOL
+    if not bad.any():
+        return
+    ex = np.asarray(mp_exact.eri_cart_exact(m.atm, m.bas, m.env, list(shls))).reshape(
+        ref.shape[::-1]).transpose(3, 2, 1, 0)
+    assert (np.abs(got - ex)[bad] <= 4.0 * np.abs(ref - ex)[bad] + ERI_ATOL).all(), \
+        f"{what}: further from the 40-digit value than the reference"

@@ -1,0 +1,158 @@
+"""Parity on the measured configurations themselves, against the oracle:
+
+* the 60-atom, 660-AO C/H cluster: G(P) blocks at tau = 0 and the energy
+  functional at a converged density (the oracle's value of the same
+  functional is a committed fixture, ``tests/golden/make_c3_energy.py``);
+* the 20-atom C/H chain: nuclear, exponent and coefficient gradients of the
+  converged SCF energy against central differences with h = 1e-5;
+* the ERI sweep: 65,536 quartets of every class against the oracle, with the
+  number of quartets that need the 40-digit arbiter printed and bounded.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from librint_b200 import dscf, eri, scf, synthetic
+from librint_b200.basis import Molecule
+from tests.conftest import ERI_ATOL, ERI_RTOL, assert_eri_close_or_exact
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+C3_FIXTURE = os.path.join(HERE, "golden", "c3_energy.npz")
+
+
+def c3_density():
+    """The fixture's density: a converged FP64 RHF density of the C3 cluster
+    (stopped at ||dP||/2 <= 1e-8), rounded to float32 and symmetric, so the
+    GPU and the oracle evaluate exactly the same matrix."""
+    f = np.load(C3_FIXTURE)
+    n = int(f["n"])
+    P = np.zeros((n, n))
+    iu = np.triu_indices(n)
+    P[iu] = f["P"].astype(np.float64)
+    P = P + np.triu(P, 1).T
+    return P, f
+
+
+def _ao_offsets(m):
+    l = m.bas.reshape(-1, 8)[:, 1]
+    return np.concatenate([[0], np.cumsum((l + 1) * (l + 2) // 2)])
+
+
+def test_c3_fock_blocks_vs_oracle():
+    """G(P) of the whole 660-AO cluster at tau = 0 on the GPU; 24 shell-pair
+    blocks of every momentum pair, on and off the diagonal, near and far,
+    summed exactly by the oracle (2 nbas^2 quartets per block), agree to
+    1e-11 of the largest |G| element of the blocks."""
+    m = synthetic.c3_cluster()
+    P, _ = c3_density()
+    ctx = scf.MolContext(m)
+    G = ctx.fock_G(P, tau=0.0)
+    ctx.close()
+    b = m.bas.reshape(-1, 8)
+    rng = np.random.default_rng(33)
+    pairs = []
+    for lx in range(3):
+        for ly in range(3):
+            xs = np.nonzero(b[:, 1] == lx)[0]
+            ys = np.nonzero(b[:, 1] == ly)[0]
+            for _ in range(2 if lx == ly else 3):
+                pairs.append((int(rng.choice(xs)), int(rng.choice(ys))))
+    pairs = pairs[:24]
+    off = _ao_offsets(m)
+    ref = oracle.fock_G_blocks(m, P, pairs)
+    scale = max(np.abs(r).max() for r in ref)
+    worst = 0.0
+    for (x, y), r in zip(pairs, ref):
+        g = G[off[x]:off[x + 1], off[y]:off[y + 1]]
+        worst = max(worst, float(np.abs(g - r).max()))
+    print(f"C3 G blocks: max |dG| {worst:.3e} of max |G| {scale:.3e}")
+    assert worst <= 1e-11 * scale
+
+
+def test_c3_energy_vs_oracle():
+    """The energy functional sum P (T + V) + 1/2 sum P G(P) + E_nn at the
+    fixture density: GPU (tau = 0) against the oracle's unique-quartet sum,
+    1e-10 Eh; and the GPU's FP64 SCF reaches the energy recorded with that
+    density again."""
+    m = synthetic.c3_cluster()
+    P, f = c3_density()
+    ctx = scf.MolContext(m)
+    e_gpu = ctx.energy(P, tau=0.0)
+    print(f"C3 energy at the fixture density: GPU {e_gpu:.12f}, oracle {float(f['E_oracle']):.12f}")
+    assert abs(e_gpu - float(f["E_oracle"])) < 1e-10
+    r = ctx.scf(conv=1e-8, guess=1, diis=8, tau=1e-13, max_iter=300)
+    ctx.close()
+    assert abs(r.energy - float(f["E_scf"])) < 1e-8, (r.energy, float(f["E_scf"]))
+
+
+def _scf_energy(m, kw):
+    return dscf._energy_and_density(m, kw)[0]
+
+
+def test_c4_chain_gradients_vs_central_differences():
+    """20-atom C/H chain (160 AOs): dE/dR (lrb_grad_nuc) and dE/d(exponent,
+    coefficient) (danalytical) of the converged FP64 SCF energy against
+    central differences of converged SCF energies with h = 1e-5.  The
+    differences carry ~1e-12 Eh of SCF noise / 2h ~ 1e-7, hence the 1e-6
+    bound (relative above 1)."""
+    m = synthetic.hc_chain()
+    assert m.natm == 20
+    kw = dict(conv=1e-11)
+    _, P = dscf._energy_and_density(m, kw)
+    gn = dscf.nuclear_gradient(m, P)
+    ge = dscf.danalyticalf(m, P)
+    s1, _ = dscf.split(m.bas)
+    h = 1e-5
+    xyz = dscf.coordinates(m)
+    checks = []
+    for a, d in ((0, 0), (3, 1), (7, 2), (15, 0), (19, 1)):
+        es = []
+        for sgn in (1.0, -1.0):
+            x2 = xyz.copy()
+            x2[a, d] += sgn * h
+            es.append(_scf_energy(dscf.with_coordinates(m, x2), kw))
+        checks.append((f"R[{a},{d}]", (es[0] - es[1]) / (2 * h), gn[a, d]))
+    b = m.bas.reshape(-1, 8)
+    params = [int(b[0, 5]), int(b[3, 5]) + 1, int(b[5, 5]), int(b[20, 5]) + 2,
+              int(b[1, 6]), int(b[4, 6]) + 1, int(b[5, 6]) + 2, int(b[22, 6]) + 3]
+    for t in params:
+        es = []
+        for sgn in (1.0, -1.0):
+            e2 = m.env.copy()
+            e2[t] += sgn * h
+            es.append(_scf_energy(Molecule(m.atm, m.bas, e2, m.nelec), kw))
+        checks.append((f"env[{t}]", (es[0] - es[1]) / (2 * h), ge[t - s1]))
+    for name, fd, an in checks:
+        print(f"{name}: analytic {an:+.10f} fd {fd:+.10f} diff {an - fd:+.2e}")
+    for name, fd, an in checks:
+        assert abs(fd - an) < 1e-6 * max(1.0, abs(fd)), (name, fd, an)
+
+
+@pytest.mark.parametrize("cls", synthetic.canonical_classes(2), ids=lambda c: "%d%d%d%d" % c)
+def test_sweep_65536_per_class_vs_oracle(cls):
+    """65,536 quartets of the sweep distribution (K = 1..6, exponents
+    log-uniform in [0.05, 5000], centres in a 10 A cube, spherical) against
+    the oracle on all host threads.  Quartets outside 1e-12 relative (+1e-15)
+    go to the 40-digit arbiter; their count is printed and may not exceed
+    0.05 % of the class."""
+    nq = 65536
+    m, shls = synthetic.eri_sweep(cls, nq, seed=2)
+    got = eri.int2e_batch(m, shls, 1)
+    ref = oracle.int2e_batch(m, shls, 1)
+    err = np.abs(got - ref)
+    bad = err > ERI_RTOL * np.abs(ref) + ERI_ATOL
+    l = np.asarray(m.bas).reshape(-1, 8)[shls, 1]
+    off = np.concatenate([[0], np.cumsum((2 * l + 1).prod(axis=1))])
+    nbadq = len(np.unique(np.searchsorted(off, np.nonzero(bad)[0], side="right") - 1))
+    print(f"class {cls}: {bad.sum()} of {err.size} integrals in {nbadq} of {nq} quartets "
+          f"outside 1e-12 of the oracle")
+    limit = max(4, nq // 2000)
+    assert nbadq <= limit
+    if nbadq:
+        assert_eri_close_or_exact(got, ref, m, shls, 1,
+                                  lambda sh: eri.int2e_batch(m, sh, 0),
+                                  what=f"sweep {cls}", max_quartets=limit)

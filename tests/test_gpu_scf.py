@@ -149,3 +149,24 @@ def test_mixed_scf_matches_fp64(golden, which):
     assert abs(rmx.energy - r64.energy) < 1e-9, (rmx.energy, r64.energy)
     assert rlo.converged and rlo.quartets <= rmx.quartets
     assert abs(rlo.energy - r64.energy) < 1e-9, (rlo.energy, r64.energy)
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_fock_partition_shares_sum_to_G(golden, nranks):
+    """lrb_fock_G_part: the shares of ranks 0..N-1, computed one after the
+    other on this GPU (no rank waits for another), sum to the full G and
+    their quartet counts to its count, with and without screening."""
+    m = _ring()
+    n = m.nao(0)
+    rng = np.random.default_rng(4)
+    A = rng.standard_normal((n, n))
+    P = (A + A.T) / np.sqrt(n)
+    ctx = scf.MolContext(m)
+    for tau in (0.0, 1e-10):
+        G, nq, _ = ctx.fock_G_prec(P, 0, tau=tau)
+        parts = [ctx.fock_G_part(P, tau, r, nranks) for r in range(nranks)]
+        S = sum(p[0] for p in parts)
+        assert sum(p[1] for p in parts) == nq
+        assert min(p[1] for p in parts) > 0
+        np.testing.assert_allclose(S, G, rtol=1e-12, atol=1e-12 * np.abs(G).max())
+    ctx.close()

@@ -95,7 +95,9 @@ def test_guess_applies_only_to_matching_basis():
     pm = G.PairModel.from_molecule(synthetic.benzene_like(1))
     assert pm.applies(synthetic.benzene_like(2))
     assert not pm.applies(synthetic.water_like())
-    assert not pm.applies(synthetic.hc_chain())          # per-atom random shells
+    assert pm.applies(synthetic.c3_cluster())            # same per-element basis
+    assert pm.applies(synthetic.hc_chain())
+    assert not pm.applies(synthetic.hc_chain(basis_seed=7))   # another basis draw
 
 
 def test_mlp_oracle_gradients_vs_finite_differences():

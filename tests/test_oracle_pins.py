@@ -165,3 +165,55 @@ def test_truth_jacobians_vs_oracle_differences(op, typec):
               oracle.int1e(Molecule(m.atm, m.bas, em), typec)) / (2 * h)
         np.testing.assert_allclose(J[:, l].reshape(fd.shape).T, fd,
                                    atol=1e-7 * max(1.0, np.abs(fd).max()))
+
+
+# ---- f shells and general contraction (tests/golden/make_golden_fgc.py) ----
+from tests.conftest import (assert_block_close_or_exact, assert_cart_elements_close_or_exact,  # noqa: E402
+                            f_classes, fgc_molecule)
+
+# The reference's spherical blocks carry its own rounding on small elements
+# of large blocks and on generally contracted shells (measured against the
+# 40-digit evaluation: up to 4e-15 absolute in (ff|fp), 2.3e-15 on 2e-4
+# elements of the contracted water); where the cartesian values are
+# arbitrated exactly, the spherical ones are compared at 1e-12 relative plus
+# 1e-12 of the largest cartesian magnitude they are combined from (in one
+# (ff|fp) block the spherical values are 150x smaller than the cartesian
+# ones; the reference's error there is 5e-13 of the cartesian scale).
+
+
+def _sph_close(got, ref, what, scale=None):
+    scale = np.abs(ref).max() if scale is None else scale
+    bad = np.abs(got - ref) > 1e-12 * np.abs(ref) + 1e-12 * scale + 1e-15
+    assert not bad.any(), f"{what}: {bad.sum()} outside; worst {np.abs(got - ref).max():.3e}"
+
+
+@pytest.mark.parametrize("cls", f_classes(), ids=lambda c: "%d%d%d%d" % c)
+def test_f_class_quartets_vs_reference(golden_fgc, cls):
+    for q in range(3):
+        key = "f/%d%d%d%d/%d" % (cls + (q,))
+        m = fgc_molecule(golden_fgc, key)
+        got, _ = oracle.int2e_block(m, [0, 1, 2, 3], 0)
+        assert_block_close_or_exact(got, golden_fgc[f"{key}/cart"], m, [0, 1, 2, 3], what=key)
+        got, _ = oracle.int2e_block(m, [0, 1, 2, 3], 1)
+        _sph_close(got, golden_fgc[f"{key}/sph"], key + " sph",
+                   np.abs(golden_fgc[f"{key}/cart"]).max())
+
+
+@pytest.mark.parametrize("key", ["gc", "fpol"])
+def test_gc_and_f_molecules_vs_reference(golden_fgc, key):
+    """Generally contracted shells (O s x2, p x3, H s x2) and f polarisation:
+    int1e, sampled int2e_c tensors, and the energy functional at the
+    reference's converged density."""
+    g = golden_fgc
+    m = fgc_molecule(g, key)
+    for coord in (0, 1):
+        for typec in (0, 1, 2):
+            np.testing.assert_allclose(oracle.int1e(m, typec, coord), g[f"{key}/int1e_{coord}{typec}"],
+                                       rtol=1e-12, atol=1e-12)
+        t = oracle.int2e_tensor(m, coord).ravel()
+        idx = g[f"{key}/int2e_{coord}_idx"]
+        if coord == 0:
+            assert_cart_elements_close_or_exact(t[idx], g[f"{key}/int2e_0_val"], m, idx, what=key)
+        else:
+            _sph_close(t[idx], g[f"{key}/int2e_1_val"], key + " sph")
+    assert abs(oracle.energy(m, g[f"{key}/scf_P"]) - float(g[f"{key}/scf"])) < 1e-10
