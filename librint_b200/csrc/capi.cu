@@ -77,9 +77,6 @@ int check_common(const int *atm, int natm, const int *bas, int nbas, const doubl
                  long long nenv) {
   if (!atm || !bas || !env || natm <= 0 || nbas <= 0 || nenv <= 0)
     return set_error("empty or NULL atm/bas/env"), LRB_ERR_INPUT;
-  if (nenv > 8 && env[8] != 0.0)
-    return set_error("range-separated integrals (env[8] != 0) are not supported"),
-           LRB_ERR_UNSUPPORTED;
   return LRB_OK;
 }
 

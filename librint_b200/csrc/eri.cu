@@ -491,6 +491,10 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   ++eng.launches;
   long long cls_begin[NCLASS + 1];
   LRB_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * (NCLASS + 1), cudaMemcpyDeviceToHost, st));
+  // env[0] (screening cutoff) and env[8] (range-separation omega)
+  double henv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  LRB_CK(cudaMemcpyAsync(henv, d_env, sizeof(double) * (size_t)std::min(nenv, 9LL),
+                         cudaMemcpyDeviceToHost, st));
   LRB_CK(cudaStreamSynchronize(st));
   if (herr == 2) return set_error("shell index out of range"), LRB_ERR_INPUT;
   if (herr) return set_error("shell with l > 3, nprim > 31 or nctr != 1"), LRB_ERR_UNSUPPORTED;
@@ -514,7 +518,8 @@ int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, lon
   prm.pp = pp;
   prm.centers = cen;
   prm.out = out;
-  prm.expcutoff = eng.expcutoff;
+  prm.expcutoff = henv[0] == 0.0 ? eng.expcutoff : std::max(40.0, henv[0]) + 1.0;
+  prm.omega = henv[8];
   prm.sph = coord;
   for (int c = 0; c < NCLASS; ++c) {
     const long long end = cls_begin[c + 1];

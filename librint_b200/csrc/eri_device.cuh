@@ -149,7 +149,8 @@ struct EriParams {
   const PrimPair *pp;
   const double *centers;  // 3 doubles per shell
   double *out;
-  double expcutoff;
+  double expcutoff;       // env[0] == 0 ? 60 : max(40, env[0]) + 1 (reference src/g2e.rs:83-92)
+  double omega;           // env[8]: 0 Coulomb, > 0 long range (erf), < 0 short range (erfc)
   int sph;                // 1: spherical output, 0: cartesian
 };
 

@@ -233,12 +233,21 @@ k_eri_gen(EriParams prm, FockParams fk, GenClass g, const double *__restrict__ r
         if (bra.cce > cut - ket.cce) continue;
         nprim += tid == 0;
         const double aij = bra.a, akl = ket.a, inv = 1.0 / (aij + akl);
-        const double fac1 = sqrt(inv) * bra.facia * ket.facia;
+        const double fac0 = sqrt(inv) * bra.facia * ket.facia;
         const double pq[3] = {bra.px - ket.px, bra.py - ket.py, bra.pz - ket.pz};
-        const double x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
+        const double x0 = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
+        // range separation as in the templated kernels (omega = env[8])
+        const double omega = prm.omega;
+        const double theta = omega != 0.0 ? omega * omega / (omega * omega + aij * akl * inv) : 0.0;
+        if (omega < 0.0 && theta * x0 > fmin(40.0, cut - bra.cce - ket.cce)) continue;
+        for (int part = 0; part < (omega < 0.0 ? 2 : 1); ++part) {
+        const bool attenuate = omega > 0.0 || part == 1;
+        const double x = attenuate ? x0 * theta : x0;
+        const double fac1 = attenuate ? fac0 * (omega > 0.0 ? sqrt(theta) : -sqrt(theta)) : fac0;
         __syncthreads();                      // previous primitive's G fully read
         if (tid < 2 * nr) {
-          const double v = rys_function_rt(rys_tab_n, nr, x, tid);
+          double v = rys_function_rt(rys_tab_n, nr, x, tid);
+          if (attenuate && tid < nr) v = v * theta / (v + 1.0 - v * theta);
           RW[tid] = v;
           if (tid < nr) RW[2 * nr + tid] = 1.0 / (1.0 + v);
         }
@@ -267,6 +276,7 @@ k_eri_gen(EriParams prm, FockParams fk, GenClass g, const double *__restrict__ r
           }
           acc[e] = s;
         }
+        }   // parts
       }
     }
     __syncthreads();

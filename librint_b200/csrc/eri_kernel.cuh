@@ -448,10 +448,22 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
         while (nbk > 0 && !(prm.pp[job.pij_off + nbk - 1].cce <= cut - kc)) --nbk;
       }
     }
-    for (int p = 0; p < npmax; ++p) {
-      bool run = p < np;
-      PrimPair bra, ket;
-      if (run) {
+    // Range separation (omega = env[8], reference src/g2e.rs:5564-5612):
+    // omega > 0 (long range, erf) scales x by theta = omega^2/(omega^2 + a0),
+    // the prefactor by sqrt(theta) and maps each node u -> u theta / (u + 1 -
+    // u theta); omega < 0 (short range, erfc) visits every primitive quartet
+    // twice, as the full operator and as the long-range one with weights
+    // times -sqrt(theta), and skips it when theta x exceeds 40 or the
+    // screening budget left.
+    const double omega = prm.omega;
+    const int reps = omega < 0.0 ? 2 : 1;
+    bool run = false;
+    PrimPair bra, ket;
+    for (int it = 0; it < npmax * reps; ++it) {
+      const bool lr_part = reps == 2 && (it & 1);
+      const int p = reps == 2 ? (it >> 1) : it;
+      if (!lr_part) run = p < np;
+      if (run && !lr_part) {
         ket = prm.pp[job.pkl_off + kl];
         bra = prm.pp[job.pij_off + ij];
         if constexpr (MODE == 0) {
@@ -480,10 +492,24 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
         fac1 = sqrt(inv) * bra.facia * ket.facia;
         pq[0] = bra.px - ket.px; pq[1] = bra.py - ket.py; pq[2] = bra.pz - ket.pz;
         x = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
-        for (int f = rho; f < 2 * C::NR; f += C::LANES) {
-          const double v = rys_function<C::NR>(tab, x, f);
-          RW[f] = v;
-          if (f < C::NR) RW[2 * C::NR + f] = 1.0 / (1.0 + v);   // t^2 complement 1/(1+u)
+        double theta = 0.0;
+        if (omega != 0.0) {
+          theta = omega * omega / (omega * omega + aij * akl * inv);
+          if (omega < 0.0 && !lr_part && theta * x > fmin(40.0, cut - bra.cce - ket.cce))
+            run = false;                        // both parts of this primitive quartet
+        }
+        const bool attenuate = omega > 0.0 || lr_part;
+        if (attenuate) {
+          x *= theta;
+          fac1 *= omega > 0.0 ? sqrt(theta) : -sqrt(theta);
+        }
+        if (run) {
+          for (int f = rho; f < 2 * C::NR; f += C::LANES) {
+            double v = rys_function<C::NR>(tab, x, f);
+            if (attenuate && f < C::NR) v = v * theta / (v + 1.0 - v * theta);
+            RW[f] = v;
+            if (f < C::NR) RW[2 * C::NR + f] = 1.0 / (1.0 + v);   // t^2 complement 1/(1+u)
+          }
         }
       }
       __syncwarp();

@@ -282,9 +282,6 @@ static int mol_create_segmented(MolCtx &m, const int *atm, int natm, const int *
   for (int a = 0; a < natm; ++a)
     if (atm[6 * a + 1] < 0 || (long long)atm[6 * a + 1] + 3 > nenv)
       return set_error("molecule: atm coordinate pointer out of range"), LRB_ERR_INPUT;
-  if (nenv > 8 && env[8] != 0.0)
-    return set_error("range-separated integrals (env[8] != 0) are not supported"),
-           LRB_ERR_UNSUPPORTED;
   m.h_aooff.assign(nbas + 1, 0);
   for (int s = 0; s < nbas; ++s) m.h_aooff[s + 1] = m.h_aooff[s] + ncart(bas[8 * s + 1]);
   m.nao = m.h_aooff[nbas];
@@ -476,7 +473,8 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     EriParams prm{};
     prm.pp = m.pp;
     prm.centers = m.centers;
-    prm.expcutoff = eng.expcutoff;
+    prm.expcutoff = m.h_env[0] == 0.0 ? eng.expcutoff : std::max(40.0, m.h_env[0]) + 1.0;
+    prm.omega = m.nenv > 8 ? m.h_env[8] : 0.0;
     prm.sph = 0;
     FockParams fk;
     fk.jobs = jobs;

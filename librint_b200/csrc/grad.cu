@@ -40,6 +40,9 @@ GradEntry g_grad_classes[NGRADCLS][NGRADMODE];
 static int grad_shells_supported(const MolCtx &m) {
   if (m.gc) return set_error("gradients: generally contracted shells are not supported"),
             LRB_ERR_UNSUPPORTED;
+  if (m.nenv > 8 && m.h_env[8] != 0.0)
+    return set_error("gradients: range-separated integrals (env[8] != 0) are not supported"),
+           LRB_ERR_UNSUPPORTED;
   for (int s = 0; s < m.nbas; ++s)
     if (m.h_bas[8 * s + 1] > 2)
       return set_error("gradients: shells up to l = 2 are supported"), LRB_ERR_UNSUPPORTED;

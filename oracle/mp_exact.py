@@ -40,6 +40,7 @@ def _fac_sp(l):
 
 def eri_cart_exact(atm, bas, env, shls):
     mp.dps = DPS
+    omega = mpf(float(env[8])) if len(env) > 8 else mpf(0)
     atm = np.asarray(atm).reshape(-1, 6)
     bas = np.asarray(bas).reshape(-1, 8)
     sh = []
@@ -76,9 +77,23 @@ def eri_cart_exact(atm, bas, env, shls):
                     fac1 = sqrt(a0 / (a1 ** 3)) * fac
                     pq = [rij[d] - rkl[d] for d in range(3)]
                     x = a0 * sum(v * v for v in pq)
-                    us, ws = gen_rys_tables.rys_rule(nroots, x)
+                    # range separation: erf (omega > 0) as nodes at theta x,
+                    # erfc (omega < 0) as full minus erf; exact at DPS digits
+                    nodes = []
+                    if omega == 0:
+                        us, ws = gen_rys_tables.rys_rule(nroots, x)
+                        nodes = list(zip(us, ws))
+                    else:
+                        theta = omega * omega / (omega * omega + a0)
+                        if omega < 0:
+                            us, ws = gen_rys_tables.rys_rule(nroots, x)
+                            nodes = list(zip(us, ws))
+                        us, ws = gen_rys_tables.rys_rule(nroots, x * theta)
+                        sgn = 1 if omega > 0 else -1
+                        nodes += [(u * theta / (u + 1 - u * theta), sgn * w * sqrt(theta))
+                                  for u, w in zip(us, ws)]
                     mp.dps = DPS
-                    for u, w in zip(us, ws):
+                    for u, w in nodes:
                         u2 = a0 * u
                         t4 = mpf(1) / 2 / (u2 * (aij + akl) + a1)
                         t5 = u2 * t4

@@ -121,6 +121,7 @@ struct Quartet {
   int lA, lB, lC, lD, nab, ncd;
   const double *rA, *rB, *rC, *rD;
   double common_factor, expcutoff;
+  double omega;   // env[8]: range separation (0 Coulomb, > 0 erf, < 0 erfc)
   double rirj[3], rkrl[3], rr_ij, rr_kl;
   double AB[3], CD[3];
   int sB, sC, sA;   // strides of G: index = ((a*(lB+1) + b)*(ncd+1) + c)*(lD+1) + d
@@ -151,6 +152,7 @@ Quartet make_quartet(const int *shls, const int *atm, const int *bas, const doub
                     common_fac_sp(q.lk) * common_fac_sp(q.ll);
   // src/g2e.rs:83-92 (the no-optimizer loop reads envs.expcutoff)
   q.expcutoff = env[0] == 0.0 ? 60.0 : std::max(40.0, env[0]) + 1.0;
+  q.omega = env[8];
   for (int d = 0; d < 3; ++d) {
     q.rirj[d] = q.si.r[d] - q.sj.r[d];
     q.rkrl[d] = q.sk.r[d] - q.sl.r[d];
@@ -261,7 +263,7 @@ int eri_cart(double *out, const Quartet &q) {
   const int nc = si.nctr * sj.nctr * sk.nctr * sl.nctr;
   std::vector<double> gbuf(3 * GSIZE), prim(nf);
   double *g[3] = {gbuf.data(), gbuf.data() + GSIZE, gbuf.data() + 2 * GSIZE};
-  double u[NROOT_MAX], w[NROOT_MAX];
+  double u[2 * NROOT_MAX], w[2 * NROOT_MAX];
   int any = 0;
 
   for (int lp = 0; lp < sl.nprim; ++lp) {
@@ -291,10 +293,38 @@ int eri_cart(double *out, const Quartet &q) {
           for (int d = 0; d < 3; ++d) rijrkl[d] = pij[d] - rkl[d];
           const double x = a0 * (rijrkl[0] * rijrkl[0] + rijrkl[1] * rijrkl[1] +
                                  rijrkl[2] * rijrkl[2]);
-          rys_roots(q.nroots, x, u, w);
+          // range separation (src/g2e.rs:5564-5612): erf(omega r)/r for
+          // omega > 0 through nodes at theta x mapped u -> u theta/(u + 1 -
+          // u theta) and sqrt(theta) on the prefactor; erfc for omega < 0 as
+          // the full operator minus the long-range one (second node set,
+          // weights times -sqrt(theta)), skipped when theta x > 40 or beyond
+          // the screening budget.  (The reference solves dedicated
+          // short-range nodes for Rys orders >= 4; the two forms are the same
+          // quadrature and differ by rounding.)
+          int nr = q.nroots;
+          double fac1r = fac1;
+          if (q.omega == 0.0) {
+            rys_roots(nr, x, u, w);
+          } else {
+            const double theta = q.omega * q.omega / (q.omega * q.omega + a0);
+            if (q.omega > 0.0) {
+              rys_roots(nr, x * theta, u, w);
+              for (int r = 0; r < nr; ++r) u[r] = u[r] * theta / (u[r] + 1.0 - u[r] * theta);
+              fac1r *= std::sqrt(theta);
+            } else {
+              if (theta * x > eijcutoff - cceij[n] || theta * x > 40.0) continue;
+              rys_roots(nr, x, u, w);
+              rys_roots(nr, x * theta, u + nr, w + nr);
+              for (int r = nr; r < 2 * nr; ++r) {
+                u[r] = u[r] * theta / (u[r] + 1.0 - u[r] * theta);
+                w[r] *= -std::sqrt(theta);
+              }
+              nr *= 2;
+            }
+          }
           std::fill(prim.begin(), prim.end(), 0.0);
-          for (int r = 0; r < q.nroots; ++r) {
-            g_one_root(g, q, aij, akl, a0, fac1, u[r], w[r], pij, rkl, rijrkl);
+          for (int r = 0; r < nr; ++r) {
+            g_one_root(g, q, aij, akl, a0, fac1r, u[r], w[r], pij, rkl, rijrkl);
             int idx = 0;
             for (int lf = 0; lf < nfl; ++lf)
               for (int kf = 0; kf < nfk; ++kf)

@@ -217,3 +217,43 @@ def test_gc_and_f_molecules_vs_reference(golden_fgc, key):
         else:
             _sph_close(t[idx], g[f"{key}/int2e_1_val"], key + " sph")
     assert abs(oracle.energy(m, g[f"{key}/scf_P"]) - float(g[f"{key}/scf"])) < 1e-10
+
+
+RS_KEYS = ["rs/water_like/+0.3", "rs/water_like/-0.3", "rs/h2o_def2svp/+0.3",
+           "rs/h2o_def2svp/-0.3"]
+
+
+@pytest.mark.parametrize("key", RS_KEYS)
+def test_range_separated_vs_reference(golden_fgc, key):
+    """env[8] = omega: long range everywhere, short range where the reference
+    uses its doubled-node form (Rys order <= 3; the fixture holds only those
+    elements for omega < 0)."""
+    g = golden_fgc
+    m = fgc_molecule(g, key)
+    for coord in (0, 1):
+        t = oracle.int2e_tensor(m, coord).ravel()
+        idx = g[f"{key}/int2e_{coord}_idx"]
+        if coord == 0:
+            assert_cart_elements_close_or_exact(t[idx], g[f"{key}/int2e_0_val"], m, idx, what=key)
+        else:
+            _sph_close(t[idx], g[f"{key}/int2e_1_val"], key + " sph")
+
+
+@pytest.mark.parametrize("omega", [-0.3, -2.0])
+def test_short_range_high_order_vs_exact(golden, omega):
+    """Short range at Rys orders 4-5 ((dd|dd), (dd|dp), (dp|dp) of
+    h2o/def2svp), where the reference's shipped nodes are wrong or abort:
+    the oracle against the 40-digit evaluation of the same operator."""
+    from oracle import mp_exact
+    m = mol(golden, "mol/h2o/def2svp")
+    env = m.env.copy()
+    env[8] = omega
+    m = Molecule(m.atm, m.bas, env, 10)
+    l = m.bas.reshape(-1, 8)[:, 1]
+    d = int(np.nonzero(l == 2)[0][0])
+    p = int(np.nonzero(l == 1)[0][0])
+    for shls in ([d, d, d, d], [d, d, d, p], [d, p, d, p]):
+        got, _ = oracle.int2e_block(m, shls, 0)
+        ex = np.asarray(mp_exact.eri_cart_exact(m.atm, m.bas, m.env, shls)).reshape(
+            got.shape[::-1]).transpose(3, 2, 1, 0)
+        assert_eri_close(got, ex, what=f"omega {omega} {shls}")
