@@ -44,6 +44,14 @@ struct DevMol {
     CK(cudaMemcpyAsync(env, e, sizeof(double) * (size_t)ne, cudaMemcpyHostToDevice, st));
     return LRB_OK;
   }
+  // device arrays only; the caller fills them
+  int alloc(cudaStream_t st, int na, int nb, long long ne) {
+    natm = na; nbas = nb; nenv = ne;
+    CK(cudaMallocAsync((void **)&atm, sizeof(int) * 6 * (size_t)std::max(na, 1), st));
+    CK(cudaMallocAsync((void **)&bas, sizeof(int) * 8 * (size_t)std::max(nb, 1), st));
+    CK(cudaMallocAsync((void **)&env, sizeof(double) * (size_t)std::max(ne, 1LL), st));
+    return LRB_OK;
+  }
   void release(cudaStream_t st) {
     if (atm) cudaFreeAsync(atm, st);
     if (bas) cudaFreeAsync(bas, st);
@@ -139,6 +147,53 @@ int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq
 // non-blocking streams: chunk c's output copy to the host overlaps chunk
 // c+1's preparation and kernels.  A chunk starts only after the previous
 // chunk's kernels (event), because both share the engine's workspace.
+// Shells, atoms and env entries (half-open ranges) that one chunk's quartets
+// can reach: every shell between the lowest and highest index it names,
+// their atoms, and the env entries of those shells and atoms.
+struct ChunkRange {
+  int s0, s1, a0, a1;
+  long long e0, e1;
+};
+
+// Ranges of every chunk; false (upload everything up front) unless they are
+// valid and each chunk's ranges lie after the previous chunk's, so a chunk can
+// upload its own part of the molecule while earlier chunks compute.
+static bool chunk_ranges(const int *shls, const std::vector<long long> &qb, const int *atm,
+                         int natm, const int *bas, int nbas, long long nenv, long long head,
+                         std::vector<ChunkRange> &rg) {
+  const int nchunk = (int)qb.size() - 1;
+  if (nchunk < 2) return false;
+  rg.resize(nchunk);
+  for (int c = 0; c < nchunk; ++c) {
+    ChunkRange r{nbas, -1, natm, -1, nenv, -1};
+    for (long long q = 4 * qb[c]; q < 4 * qb[c + 1]; ++q) {
+      r.s0 = std::min(r.s0, shls[q]);
+      r.s1 = std::max(r.s1, shls[q] + 1);
+    }
+    for (int sh = r.s0; sh < r.s1; ++sh) {
+      const int *b = bas + 8 * sh;
+      if (b[0] < 0 || b[0] >= natm || b[2] < 1 || b[3] < 1 || b[5] < 0 || b[6] < 0 ||
+          (long long)b[5] + b[2] > nenv || (long long)b[6] + (long long)b[2] * b[3] > nenv)
+        return false;
+      r.a0 = std::min(r.a0, b[0]);
+      r.a1 = std::max(r.a1, b[0] + 1);
+      r.e0 = std::min({r.e0, (long long)b[5], (long long)b[6]});
+      r.e1 = std::max({r.e1, (long long)b[5] + b[2], (long long)b[6] + (long long)b[2] * b[3]});
+    }
+    for (int a = r.a0; a < r.a1; ++a) {
+      const long long pc = atm[6 * a + 1];
+      if (pc < 0 || pc + 3 > nenv) return false;
+      r.e0 = std::min(r.e0, pc);
+      r.e1 = std::max(r.e1, pc + 3);
+    }
+    const ChunkRange *prev = c > 0 ? &rg[c - 1] : nullptr;
+    if (r.e0 < head || (prev && (r.s0 < prev->s1 || r.a0 < prev->a1 || r.e0 < prev->e1)))
+      return false;
+    rg[c] = r;
+  }
+  return true;
+}
+
 static int batch_host(double *out, int coord, const int *shls, long long nq, const int *atm,
                       int natm, const int *bas, int nbas, const double *env, long long nenv,
                       int gc_screen) {
@@ -170,23 +225,31 @@ static int batch_host(double *out, int coord, const int *shls, long long nq, con
     if (!eng.done[i] && cudaEventCreateWithFlags(&eng.done[i], cudaEventDisableTiming) != cudaSuccess)
       return set_error("event creation failed"), LRB_ERR_CUDA;
   }
+  // env[0..head) holds the settings every chunk reads (cutoff, omega)
+  const long long head = std::min(nenv, 20LL);
+  std::vector<ChunkRange> rg;
+  const bool streamed = chunk_ranges(shls, qb, atm, natm, bas, nbas, nenv, head, rg);
   DevMol m;
-  rc = m.upload(eng.pipe[0], atm, natm, bas, nbas, env, nenv);
-  // shell centres once per call (chunk 0's kernels, and through its event
-  // every later chunk, are ordered after them on stream 0)
   double *cen = (double *)eng.pipe_centers.get(eng.pipe[0], sizeof(double) * 3 * (size_t)nbas + 256);
-  if (!rc && !cen) rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
-  if (!rc)
-    rc = eri_centers(m.atm, natm, m.bas, nbas, m.env, nenv, cen,
-                     reinterpret_cast<int *>(cen + 3 * (size_t)nbas), eng.pipe[0]);
+  if (!cen) rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
+  int *d_err = reinterpret_cast<int *>(cen + 3 * (size_t)nbas);
+  if (!rc && !streamed) {
+    // the whole molecule, and shell centres once per call (chunk 0's kernels,
+    // and through its event every later chunk, are ordered after them)
+    rc = m.upload(eng.pipe[0], atm, natm, bas, nbas, env, nenv);
+    if (!rc) rc = eri_centers(m.atm, natm, m.bas, nbas, m.env, nenv, cen, d_err, eng.pipe[0]);
+  } else if (!rc) {
+    // device arrays of full size; each chunk fills its own ranges
+    rc = m.alloc(eng.pipe[0], natm, nbas, nenv);
+    if (!rc && (cudaMemcpyAsync(m.env, env, sizeof(double) * head, cudaMemcpyHostToDevice,
+                                eng.pipe[0]) != cudaSuccess ||
+                cudaStreamSynchronize(eng.pipe[0]) != cudaSuccess))
+      rc = (set_error("copy failed"), LRB_ERR_CUDA);
+  }
   const int nchunk = (int)qb.size() - 1;
   for (int c = 0; c < nchunk && !rc; ++c) {
     const int X = c & 1;
     cudaStream_t st = eng.pipe[X];
-    if (c > 0 && cudaStreamWaitEvent(st, eng.done[1 - X], 0) != cudaSuccess) {
-      rc = (set_error("stream wait failed"), LRB_ERR_CUDA);
-      break;
-    }
     const long long nqc = qb[c + 1] - qb[c], len = ob[c + 1] - ob[c];
     int *d_sh = (int *)eng.pipe_in[X].get(st, sizeof(int) * 4 * (size_t)nqc);
     double *d_o = (double *)eng.pipe_out[X].get(st, sizeof(double) * (size_t)std::max(len, 1LL));
@@ -194,11 +257,32 @@ static int batch_host(double *out, int coord, const int *shls, long long nq, con
       rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
       break;
     }
-    if (cudaMemcpyAsync(d_sh, shls + 4 * qb[c], sizeof(int) * 4 * (size_t)nqc,
-                        cudaMemcpyHostToDevice, st) != cudaSuccess) {
+    // this chunk's inputs go up before it waits for the previous chunk, so
+    // they overlap that chunk's kernels
+    bool ok = cudaMemcpyAsync(d_sh, shls + 4 * qb[c], sizeof(int) * 4 * (size_t)nqc,
+                              cudaMemcpyHostToDevice, st) == cudaSuccess;
+    if (streamed) {
+      const ChunkRange &r = rg[c];
+      ok = ok && cudaMemcpyAsync(m.bas + 8 * (size_t)r.s0, bas + 8 * (size_t)r.s0,
+                                 sizeof(int) * 8 * (size_t)(r.s1 - r.s0), cudaMemcpyHostToDevice,
+                                 st) == cudaSuccess;
+      ok = ok && cudaMemcpyAsync(m.atm + 6 * (size_t)r.a0, atm + 6 * (size_t)r.a0,
+                                 sizeof(int) * 6 * (size_t)(r.a1 - r.a0), cudaMemcpyHostToDevice,
+                                 st) == cudaSuccess;
+      ok = ok && cudaMemcpyAsync(m.env + r.e0, env + r.e0, sizeof(double) * (size_t)(r.e1 - r.e0),
+                                 cudaMemcpyHostToDevice, st) == cudaSuccess;
+    }
+    if (!ok) {
       rc = (set_error("copy failed"), LRB_ERR_CUDA);
       break;
     }
+    if (c > 0 && cudaStreamWaitEvent(st, eng.done[1 - X], 0) != cudaSuccess) {
+      rc = (set_error("stream wait failed"), LRB_ERR_CUDA);
+      break;
+    }
+    if (streamed)
+      eri_centers_async(m.atm, natm, m.bas + 8 * (size_t)rg[c].s0, rg[c].s1 - rg[c].s0, m.env,
+                        nenv, cen + 3 * (size_t)rg[c].s0, d_err, st);
     rc = eri_batch_device(eng, d_o, coord, d_sh, nqc, m.atm, natm, m.bas, nbas, m.env, nenv, st,
                           nullptr, cen, gc_screen);
     if (rc) break;

@@ -105,5 +105,10 @@ int gc_expand(const int *bas, int nbas, const double *env, long long nenv, GcExp
 int eri_centers(const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
                 long long nenv, double *centers, int *d_err, cudaStream_t st);
 long long eri_batch_out_len(int coord, const int *shls, long long nq, const int *bas);
+// k_centers over nbas shells starting at d_bas (centres written from
+// `centers`), queued on st without reading the error flag back: for shells
+// whose indices the caller has checked on the host.
+void eri_centers_async(const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
+                       long long nenv, double *centers, int *d_err, cudaStream_t st);
 
 }  // namespace lrb

@@ -425,6 +425,14 @@ int eri_centers(const int *d_atm, int natm, const int *d_bas, int nbas, const do
   return LRB_OK;
 }
 
+void eri_centers_async(const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
+                       long long nenv, double *centers, int *d_err, cudaStream_t st) {
+  if (nbas <= 0) return;
+  const int T = 256;
+  k_centers<<<(nbas + T - 1) / T, T, 0, st>>>(d_atm, natm, d_bas, nbas, d_env, nenv, centers, d_err);
+  ++engine().launches;
+}
+
 int eri_batch_device(Engine &eng, double *out, int coord, const int *d_shls, long long nq,
                      const int *d_atm, int natm, const int *d_bas, int nbas, const double *d_env,
                      long long nenv, cudaStream_t st, EriBatchStats *stats,

@@ -109,6 +109,15 @@ struct EriClass {
   }
 };
 
+// Density sub-blocks a quartet's digestion reads, staged once per quartet in
+// the slot's shared memory (the digestion reads each of them NI..NL times):
+// P_cd, P_ab, P_bd, P_ad, P_bc, P_ac, each row-major in (first, second).
+template <int NI, int NJ, int NK, int NL>
+struct FockStage {
+  static constexpr int CD = 0, AB = CD + NK * NL, BD = AB + NI * NJ, AD = BD + NJ * NL,
+                       BC = AD + NI * NL, AC = BC + NJ * NK, SIZE = AC + NI * NK;
+};
+
 template <class C, int MODE = 0, typename R = double>
 struct EriLayout {
   static constexpr int NKO_MAX = C::NKET;   // cartesian >= spherical
@@ -118,7 +127,10 @@ struct EriLayout {
   // (NBRA*NKO, output mode only) in the epilogue.  FP32 halves the R parts.
   static constexpr int RD(int n) { return (int)((n * sizeof(R) + 7) / 8); }
   static constexpr int LOOP = 3 * C::NR + RD(C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ);
-  static constexpr int EPI = RD(C::NBRA * C::NKET) + (MODE == 0 ? C::NBRA * NKO_MAX : 0);
+  // Fock mode stages the quartet's density blocks after the block
+  static constexpr int EPI = RD(C::NBRA * C::NKET) +
+                             (MODE == 0 ? C::NBRA * NKO_MAX
+                                        : RD(FockStage<C::NI, C::NJ, C::NK, C::NL>::SIZE) + 1);
   static constexpr int SLOT = LOOP > EPI ? LOOP : EPI;
   static constexpr int WARP = C::SLOTS * SLOT;
   static constexpr int TAB = (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR]);
@@ -213,61 +225,84 @@ __device__ __forceinline__ void gout_cols(R (&acc)[C::NCOLS], const R (&x)[C::CW
   }
 }
 
+// doubles needed for `bytes` bytes
+__host__ __device__ constexpr int RD_(size_t bytes) { return (int)((bytes + 7) / 8); }
+
 // ---------------------------------------------------------------- digestion
+template <int NI, int NJ, int NK, int NL, typename R>
+__device__ __forceinline__ void fock_stage(R *Ps, const QuartetJob &q, const FockParams &fk,
+                                           int rho, int nlanes) {
+  using S = FockStage<NI, NJ, NK, NL>;
+  const int n = fk.n;
+  const int oi = fk.aooff[q.ish], oj = fk.aooff[q.jsh], ok = fk.aooff[q.ksh], ol = fk.aooff[q.lsh];
+  const double *P = fk.P;
+  for (int t = rho; t < S::SIZE; t += nlanes) {
+    int r0, c0, nc, e;
+    if (t < S::AB) { e = t - S::CD; r0 = ok; c0 = ol; nc = NL; }
+    else if (t < S::BD) { e = t - S::AB; r0 = oi; c0 = oj; nc = NJ; }
+    else if (t < S::AD) { e = t - S::BD; r0 = oj; c0 = ol; nc = NL; }
+    else if (t < S::BC) { e = t - S::AD; r0 = oi; c0 = ol; nc = NL; }
+    else if (t < S::AC) { e = t - S::BC; r0 = oj; c0 = ok; nc = NK; }
+    else { e = t - S::AC; r0 = oi; c0 = ok; nc = NK; }
+    Ps[t] = (R)P[(long long)(r0 + e / nc) * n + c0 + e % nc];
+  }
+}
+
 // J/K digestion of one cartesian block B[a + NI*(b + NJ*(c + NK*d))] with
-// the degeneracy weight w of its canonical shell quartet:
+// the degeneracy weight w of its canonical shell quartet, against the staged
+// density blocks Ps:
 //   Jacc[ab] += 2w sum_cd B P[cd],  Jacc[cd] += 2w sum_ab B P[ab],
 //   Kacc[ac] += w sum_bd B P[bd],   Kacc[bc] += w sum_ad B P[ad],
 //   Kacc[ad] += w sum_bc B P[bc],   Kacc[bd] += w sum_ac B P[ac];
 // G = (Jacc + Jacc^T) - (Kacc + Kacc^T)/2 then equals the reference's
 // G[mu nu] = sum P[ls](mu nu|s l) - 1/2 sum P[ns](mu l|s n) (src/scf.rs:379-391).
 template <int NI, int NJ, int NK, int NL, typename R>
-__device__ __forceinline__ void fock_digest(const R *B, const QuartetJob &q, double w,
+__device__ __forceinline__ void fock_digest(const R *B, const R *Ps, const QuartetJob &q, double w,
                                             const FockParams &fk, int rho, int nlanes) {
+  using S = FockStage<NI, NJ, NK, NL>;
   const int n = fk.n;
   const int oi = fk.aooff[q.ish], oj = fk.aooff[q.jsh], ok = fk.aooff[q.ksh], ol = fk.aooff[q.lsh];
-  const double *P = fk.P;
   auto blk = [&](int a, int b, int c, int d) { return B[a + NI * (b + NJ * (c + NK * d))]; };
   for (int t = rho; t < NI * NJ; t += nlanes) {          // J[ab]
     const int a = t % NI, b = t / NI;
     R s = 0;
     for (int d = 0; d < NL; ++d)
-      for (int c = 0; c < NK; ++c) s = fma(blk(a, b, c, d), (R)P[(long long)(ok + c) * n + ol + d], s);
+      for (int c = 0; c < NK; ++c) s = fma(blk(a, b, c, d), Ps[S::CD + c * NL + d], s);
     atomicAdd(&fk.J[(long long)(oi + a) * n + oj + b], 2.0 * w * (double)s);
   }
   for (int t = rho; t < NK * NL; t += nlanes) {          // J[cd]
     const int c = t % NK, d = t / NK;
     R s = 0;
     for (int b = 0; b < NJ; ++b)
-      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), (R)P[(long long)(oi + a) * n + oj + b], s);
+      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), Ps[S::AB + a * NJ + b], s);
     atomicAdd(&fk.J[(long long)(ok + c) * n + ol + d], 2.0 * w * (double)s);
   }
   for (int t = rho; t < NI * NK; t += nlanes) {          // K[ac]
     const int a = t % NI, c = t / NI;
     R s = 0;
     for (int d = 0; d < NL; ++d)
-      for (int b = 0; b < NJ; ++b) s = fma(blk(a, b, c, d), (R)P[(long long)(oj + b) * n + ol + d], s);
+      for (int b = 0; b < NJ; ++b) s = fma(blk(a, b, c, d), Ps[S::BD + b * NL + d], s);
     atomicAdd(&fk.K[(long long)(oi + a) * n + ok + c], w * (double)s);
   }
   for (int t = rho; t < NJ * NK; t += nlanes) {          // K[bc]
     const int b = t % NJ, c = t / NJ;
     R s = 0;
     for (int d = 0; d < NL; ++d)
-      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), (R)P[(long long)(oi + a) * n + ol + d], s);
+      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), Ps[S::AD + a * NL + d], s);
     atomicAdd(&fk.K[(long long)(oj + b) * n + ok + c], w * (double)s);
   }
   for (int t = rho; t < NI * NL; t += nlanes) {          // K[ad]
     const int a = t % NI, d = t / NI;
     R s = 0;
     for (int c = 0; c < NK; ++c)
-      for (int b = 0; b < NJ; ++b) s = fma(blk(a, b, c, d), (R)P[(long long)(oj + b) * n + ok + c], s);
+      for (int b = 0; b < NJ; ++b) s = fma(blk(a, b, c, d), Ps[S::BC + b * NK + c], s);
     atomicAdd(&fk.K[(long long)(oi + a) * n + ol + d], w * (double)s);
   }
   for (int t = rho; t < NJ * NL; t += nlanes) {          // K[bd]
     const int b = t % NJ, d = t / NJ;
     R s = 0;
     for (int c = 0; c < NK; ++c)
-      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), (R)P[(long long)(oi + a) * n + ok + c], s);
+      for (int a = 0; a < NI; ++a) s = fma(blk(a, b, c, d), Ps[S::AC + a * NK + c], s);
     atomicAdd(&fk.K[(long long)(oj + b) * n + ol + d], w * (double)s);
   }
 }
@@ -632,7 +667,13 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
                 (long long)ko * job.s_k + (long long)lo * job.s_l] = (double)v;
       }
     }
-    if (MODE == 1 && have) fock_digest<C::NI, C::NJ, C::NK, C::NL, R>(Bk, job, wdeg, fk, rho, C::LANES);
+    if constexpr (MODE == 1) {
+      // staged density blocks start on an 8-byte boundary after the block
+      R *Ps = reinterpret_cast<R *>(sb + RD_(C::NBRA * C::NKET * sizeof(R)));
+      if (have) fock_stage<C::NI, C::NJ, C::NK, C::NL, R>(Ps, job, fk, rho, C::LANES);
+      __syncwarp();
+      if (have) fock_digest<C::NI, C::NJ, C::NK, C::NL, R>(Bk, Ps, job, wdeg, fk, rho, C::LANES);
+    }
     __syncwarp();
   }
   if (MODE == 1 && fk.prim_count) {
