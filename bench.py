@@ -218,6 +218,28 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def link_bandwidth(dev, nbytes=1 << 30, reps=3):
+    """Pinned host <-> device copy bandwidth (GB/s per direction), measured
+    with CUDA events on one stream: the ceiling of the end-to-end path."""
+    import torch
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = {}
+    for name, fn in (("h2d_gbs", lambda: d.copy_(h, non_blocking=True)),
+                     ("d2h_gbs", lambda: h.copy_(d, non_blocking=True))):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = nbytes * reps / (a.elapsed_time(b) * 1e-3) / 1e9
+    del h, d
+    return out
+
+
 # ------------------------------------------------------------ CPU arms
 def _prefix_molecule(atm, bas, env, nshell):
     """The first nshell shells of a sweep (one atom per shell, env laid out
@@ -415,9 +437,17 @@ def main():
             e2e_step()
         torch.cuda.synchronize()
         te = shard.max_over_ranks(time.perf_counter() - t0, dev)
+        bw = link_bandwidth(dev)
+        step_s = te / args.e2e_steps
+        bound = {"h2d": h2d / bw["h2d_gbs"] / 1e9, "d2h": d2h / bw["d2h_gbs"] / 1e9,
+                 "device": elapsed / args.steps}
         e2e = {"value": world * len(CLASSES) * args.nq * args.e2e_steps / te, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "note": "lrb_int2e_batch with pinned host buffers; all %d classes per step"
+               "step_s": step_s, "link": bw, "bound_s": bound,
+               "frac_of_overlapped_bound": max(bound.values()) / step_s,
+               "note": "lrb_int2e_batch with pinned host buffers; all %d classes per step; "
+                       "bound_s = bytes / measured pinned copy bandwidth per direction, and the "
+                       "device-resident step time; a fully overlapped pipeline takes the largest"
                        % len(CLASSES)}
 
     cpu = None

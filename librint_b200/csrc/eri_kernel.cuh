@@ -494,13 +494,20 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
     const int reps = omega < 0.0 ? 2 : 1;
     bool run = false;
     PrimPair bra, ket;
+    // pair data of the next primitive quartet, loaded one iteration ahead so
+    // the L2 latency overlaps the current iteration's arithmetic
+    PrimPair nbra, nket;
+    if (np > 0) {
+      nket = prm.pp[job.pkl_off + kl];
+      nbra = prm.pp[job.pij_off + ij];
+    }
     for (int it = 0; it < npmax * reps; ++it) {
       const bool lr_part = reps == 2 && (it & 1);
       const int p = reps == 2 ? (it >> 1) : it;
       if (!lr_part) run = p < np;
       if (run && !lr_part) {
-        ket = prm.pp[job.pkl_off + kl];
-        bra = prm.pp[job.pij_off + ij];
+        ket = nket;
+        bra = nbra;
         if constexpr (MODE == 0) {
           if (++ij == nbk) {
             ij = 0;
@@ -515,6 +522,10 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
           run = !(ket.cce > cut) && !(bra.cce > cut - ket.cce);
           if (++ij == job.nij) { ij = 0; ++kl; }
           nprim += run && rho == 0;
+        }
+        if (p + 1 < np) {
+          nket = prm.pp[job.pkl_off + kl];
+          nbra = prm.pp[job.pij_off + ij];
         }
       }
       // Roots, weights, prefactors and the per-unit coefficients are FP64 in
