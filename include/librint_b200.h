@@ -46,8 +46,13 @@ LRB_API const char *lrb_last_error(void);
  * shls holds nq quartets (4 shell indices each).  Every quartet's block is
  * written in libcint layout (out[i + ni*(j + nj*(k + nk*l))]) and the blocks
  * are packed back to back in quartet order; lrb_int2e_batch_len gives the
- * total length in doubles.  Shells: l <= 3, 1..31 primitives, nctr == 1.
- * Screening is the reference's (expcutoff 60, src/cint2e.rs:367-393).
+ * total length in doubles.  Shells: l <= 3 with 1..31 primitives.
+ * Generally contracted shells (nctr > 1; blocks of nf * nctr rows per shell,
+ * contraction-major as libcint) are accepted by lrb_int2e_batch, which splits
+ * them into segmented sub-shells on the host; the device-pointer entry points
+ * take segmented shells only.  Screening is the reference's (expcutoff from
+ * env[0], 60 by default, src/cint2e.rs:367-393); env[8] = omega selects the
+ * range-separated operator (src/g2e.rs:5564-5612).
  * -------------------------------------------------------------------*/
 LRB_API long long lrb_int2e_batch_len(int coord, const int *shls, long long nq, const int *bas, int nbas);
 

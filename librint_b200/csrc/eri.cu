@@ -580,8 +580,9 @@ long long eri_batch_out_len(int coord, const int *shls, long long nq, const int 
   for (long long q = 0; q < nq; ++q) {
     long long b = 1;
     for (int a = 0; a < 4; ++a) {
-      const int l = bas[8 * shls[4 * q + a] + 1];
-      b *= coord == 0 ? ncart(l) : nsph(l);
+      const int *bs = bas + 8 * shls[4 * q + a];
+      const int l = bs[1], nctr = bs[3] > 1 ? bs[3] : 1;   // contractions are rows too
+      b *= (long long)(coord == 0 ? ncart(l) : nsph(l)) * nctr;
     }
     n += b;
   }

@@ -14,7 +14,8 @@ contraction coefficients are positive and PySCF-normalised
   exponents log-uniform in [0.05, 5000].
 * ``ch_basis``       -- the C/H basis every C/H system below uses: one shell
   set per element drawn from seed 3 (C 3s2p1d, H 2s1p, K uniform in 1..6,
-  exponents log-uniform in [0.1, 5000] for C and [0.1, 50] for H).
+  exponents log-uniform within each shell's core / valence / diffuse /
+  polarisation range, together C [0.1, 5000] and H [0.1, 50]).
 * ``c3_cluster``     -- the 60-atom RHF system: 36 C on a perturbed hexagonal
   lattice (C-C 1.40 +- 0.05 A) and 24 H at 1.09 A on edge carbons,
   660 cartesian AOs.
@@ -133,17 +134,28 @@ def _normalise_many(ls, e, c, mask):
 
 
 # ------------------------------------------------------------------ C/H sets
-C_SHELLS = (0, 0, 0, 1, 1, 2)       # 3s2p1d
-H_SHELLS = (0, 0, 1)                # 2s1p
-C_RANGE = (0.1, 5000.0)
-H_RANGE = (0.1, 50.0)
-CH_BASIS_SEED = 3                   # the one basis every C/H system here uses
+# A split-valence set with polarisation ("DZP-like"): C 3s2p1d, H 2s1p.  Each
+# shell has a role -- core, valence, diffuse or polarisation -- and draws K
+# uniform in 1..6 and its exponents log-uniform within its role's range; the
+# ranges span C [0.1, 5000] and H [0.1, 50].  Drawing every shell over the
+# whole range instead makes every contracted function tight (the smallest
+# kinetic-energy diagonal of the 120-AO ring was 7.8 Eh and its
+# core-Hamiltonian HOMO +11.5 Eh) and no SCF converges on such a set.
+C_ROLES = ((0, 3.0, 5000.0),    # s core
+           (0, 0.25, 5.0),      # s valence
+           (0, 0.1, 0.3),       # s diffuse
+           (1, 0.3, 30.0),      # p valence
+           (1, 0.1, 0.4),       # p diffuse
+           (2, 0.3, 2.0))       # d polarisation
+H_ROLES = ((0, 0.3, 50.0),      # s valence
+           (0, 0.1, 0.3),       # s diffuse
+           (1, 0.3, 2.0))       # p polarisation
+CH_BASIS_SEED = 3               # the one basis every C/H system here uses
 
 
 def _draw_shells(rng, z, kmax):
-    shells, (lo, hi) = (C_SHELLS, C_RANGE) if z == 6 else (H_SHELLS, H_RANGE)
     out = []
-    for l in shells:
+    for l, lo, hi in (C_ROLES if z == 6 else H_ROLES):
         k = int(rng.integers(1, kmax + 1))
         out.append((l, _exps(rng, k, lo, hi), _coefs(rng, k)))
     return out
@@ -151,9 +163,10 @@ def _draw_shells(rng, z, kmax):
 
 def ch_basis(seed: int = CH_BASIS_SEED, kmax: int = 6) -> dict:
     """One shell set per element, like a named basis: C 3s2p1d, H 2s1p, K
-    uniform in 1..kmax per shell, exponents log-uniform in [0.1, 5000] (C)
-    or [0.1, 50] (H), coefficients uniform in [0.2, 1] (normalised when the
-    shell is added).  C is drawn first, then H, from default_rng(seed)."""
+    uniform in 1..kmax per shell, exponents log-uniform within each shell's
+    role range (C_ROLES, H_ROLES), coefficients uniform in [0.2, 1]
+    (normalised when the shell is added).  C is drawn first, then H, from
+    default_rng(seed)."""
     rng = np.random.default_rng(seed)
     return {z: _draw_shells(rng, z, kmax) for z in (6, 1)}
 
@@ -216,7 +229,8 @@ def c3_cluster(seed: int = 3) -> Molecule:
     """The ~600-AO RHF system: 60-atom C/H flake, 36 C + 24 H (240
     electrons), C on a perturbed hexagonal lattice (1.40 +- 0.05 A), H at
     1.09 A on edge carbons, the seed-3 per-element basis (C 3s2p1d, H 2s1p,
-    K = 1..6, log-uniform exponents): 288 shells, 660 cartesian AOs."""
+    K = 1..6, log-uniform exponents per shell role): 288 shells, 660
+    cartesian AOs."""
     z, xyz = _flake(np.random.default_rng(seed), 36, 3.0, 10.0, (0.35, 0.0))
     return _build_ch(z, xyz, "c3_cluster", seed=seed)
 

@@ -157,3 +157,29 @@ def assert_block_close_or_exact(got, ref, m, shls, what=""):
         ref.shape[::-1]).transpose(3, 2, 1, 0)
     assert (np.abs(got - ex)[bad] <= 4.0 * np.abs(ref - ex)[bad] + ERI_ATOL).all(), \
         f"{what}: further from the 40-digit value than the reference"
+
+
+def block_scale(m, shls, coord, values):
+    """Per element, the largest |value| of the quartet block it belongs to
+    (packed libcint blocks of the quartet list ``shls``)."""
+    import numpy as np
+    off = np.concatenate([[0], np.cumsum(_block_sizes(m, shls, coord))])
+    v = np.abs(np.asarray(values))
+    mx = np.maximum.reduceat(v, off[:-1]) if v.size else v
+    return np.repeat(mx, np.diff(off))
+
+
+def assert_close_block_scale(got, ref, m, shls, coord, scale_values=None, rel_block=1e-12,
+                             what=""):
+    """Per integral 1e-12 relative plus ``rel_block`` of the largest |value| of
+    its quartet block (of ``scale_values``, default ref) plus 1e-15: the
+    bar for blocks whose small elements come out of cancellation between
+    much larger terms (high-momentum blocks; short range as full minus long
+    range), where both double-precision paths carry ~1e-16 of the block's
+    scale."""
+    import numpy as np
+    got, ref = np.asarray(got), np.asarray(ref)
+    scale = block_scale(m, shls, coord, ref if scale_values is None else scale_values)
+    bad = np.abs(got - ref) > ERI_RTOL * np.abs(ref) + rel_block * scale + ERI_ATOL
+    assert not bad.any(), (f"{what}: {bad.sum()} of {bad.size} outside; worst relative to the "
+                           f"block scale {(np.abs(got - ref) / np.maximum(scale, 1e-300)).max():.3e}")

@@ -101,15 +101,18 @@ def test_errors_are_reported_not_fatal():
     bad[0, 0] = m.nbas + 7
     with pytest.raises(B.LibrintError):
         eri.int2e_batch(m, bad)
-    # f shell: not compiled (l <= 2)
+    # g shell: no kernel (l <= 3)
     m2 = Molecule(m.atm.copy(), m.bas.copy(), m.env.copy())
-    m2.bas.reshape(-1, 8)[0, 1] = 3
+    m2.bas.reshape(-1, 8)[0, 1] = 4
     with pytest.raises(B.LibrintError):
         eri.int2e_batch(m2, shls[:1], 0)
-    # range separation (env[8] != 0) is out of scope
-    m3 = Molecule(m.atm.copy(), m.bas.copy(), m.env.copy())
-    m3.env[8] = 0.3
+    # more than 31 primitives in a shell
+    m3 = Molecule(m.atm.copy(), m.bas.copy(), np.concatenate([m.env, np.ones(80)]))
+    b3 = m3.bas.reshape(-1, 8)
+    b3[0, 2] = 40
+    b3[0, 5] = m.env.size
+    b3[0, 6] = m.env.size + 40
     with pytest.raises(B.LibrintError):
-        eri.int2e_batch(m3, shls)
+        eri.int2e_batch(m3, shls[:1], 0)
     # the library still works afterwards
     assert_eri_close(eri.int2e_batch(m, shls), oracle.int2e_batch(m, shls, 1))
