@@ -317,6 +317,8 @@ def main():
                          "single-GPU runs only")
     ap.add_argument("--guess", default=os.path.join(ROOT, "librint_b200", "data", "guess_ch.npz"),
                     help="learned-guess network for the --rhf runs")
+    ap.add_argument("--rhf-ablations", action="store_true",
+                    help="also run the mixed (core-H start) and learned FP64 RHF legs")
     ap.add_argument("--classes", default="",
                     help="comma list of classes to run, e.g. 2222,2221 (default: all 21)")
     args = ap.parse_args()
@@ -458,7 +460,8 @@ def main():
                          f"workload, 1 untimed + 3 timed passes ({3 * len(CLASSES) * s} quartets, "
                          f"{tcpu:.1f} s), oracle/ C++ restatement, OpenMP over quartets"}
 
-    rhf = run_rhf(args.guess, threads, fp64_peak, cpu=not args.no_cpu) \
+    rhf = run_rhf(args.guess, threads, fp64_peak, cpu=not args.no_cpu,
+                  ablations=args.rhf_ablations) \
         if (args.rhf and world == 1) else None
 
     if rank == 0:
@@ -500,6 +503,7 @@ def main():
 # operator's.
 TAU_FP32 = 1e-11
 TAU = 1e-13
+TAU_PRIM = 1e-15        # primitive-quartet screening of every leg's Fock builds
 RHF_TARGET_EH = 1e-6     # |E - E_FP64| a leg must reach to count
 
 
@@ -517,7 +521,7 @@ def fock_flops(cls, prim_quartets, quartets):
     return float(prim_quartets) * per_prim + 8.0 * nf * float(quartets)
 
 
-def fock_measure(ctx, P, fp64_peak, builds=3):
+def fock_measure(ctx, P, fp64_peak, builds=1):
     """Fock builds G(P) of the cluster at its converged density: FP64 and
     all-FP32 builds per second (host wall clock around lrb_fock_G_prec,
     copies of P and G included), per-class kernel times (CUDA events) and
@@ -526,7 +530,8 @@ def fock_measure(ctx, P, fp64_peak, builds=3):
     import torch
     from librint_b200 import _bindings as B
     L = B.lib()
-    out = {}
+    out = {"tau": TAU, "tau_prim": TAU_PRIM}
+    ctx.set_tau_prim(TAU_PRIM)
     for prec, name in ((0, "fp64"), (1, "fp32")):
         ctx.fock_G_prec(P, prec, tau=TAU)          # warm
         torch.cuda.synchronize()
@@ -597,21 +602,23 @@ def rhf_cpu_baseline(mol, P, threads, iterations, budget_s=10.0, seed=7):
                       f"reference's own P = I Roothaan loop needs more)"}
 
 
-def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True):
+def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True, ablations=False):
     """RHF wall time on the 60-atom C/H cluster (synthetic.c3_cluster: 36 C +
     24 H, 660 cartesian AOs, the seed-3 per-element C 3s2p1d / H 2s1p basis
     with K = 1..6).
 
-    reference: FP64, core-H guess, DIIS(8), Schwarz x density tau = 1e-13,
-               ||dP||/2 <= 1e-8: the FP64 energy every leg is judged against;
-    plain:     the same FP64 GPU schedule stopped at 1e-5;
-    mixed:     incremental Fock builds with FP32 quartets, same stop (FP32
-               phases screen at tau_fp32 = 1e-11, the FP64 finish at 1e-13
-               after a full rebuild);
-    learned_*: started from the learned guess (when its network applies to
-               this basis), FP64 or mixed; the host prediction is timed in.
-    chosen = the fastest leg within 1e-6 Eh of the FP64 energy.  Times
-    exclude the one-off pair table / Schwarz set-up (setup_s)."""
+    plain:     FP64 GPU path: core-H guess, DIIS(8), full Fock builds with
+               Schwarz x density screening at tau = 1e-13 and primitive
+               screening at TAU_PRIM, stopped at ||dP||/2 <= 1e-5;
+    reference: the FP64 energy every leg is judged against: the plain run
+               continued from its density to ||dP||/2 <= 1e-8;
+    learned_mixed (the chosen form): the learned guess (when its network
+               applies to this basis; the host prediction is timed in) and
+               incremental Fock builds with FP32 quartets, FP32 phases
+               screened at tau_fp32 = 1e-11, FP64 finish at 1e-13;
+    with ablations also mixed (core-H start) and learned_fp64.
+    chosen = the fastest leg within 1e-6 Eh of the reference.  Times exclude
+    the one-off pair table / Schwarz set-up (setup_s)."""
     import torch
     from librint_b200 import scf as S
     mol = synthetic.c3_cluster()
@@ -619,7 +626,7 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True):
     ctx = S.MolContext(mol)
     torch.cuda.synchronize()
     setup = time.perf_counter() - t0
-    base = dict(guess=1, diis=8, tau=TAU, max_iter=300, check=False)
+    base = dict(guess=1, diis=8, tau=TAU, max_iter=300, check=False, tau_prim=TAU_PRIM)
 
     def run(conv, P0=None, extra_ms=0.0, density=False, **kw):
         t0 = time.perf_counter()
@@ -632,10 +639,14 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True):
 
     out = {"system": "c3_cluster seed 3: %d atoms, %d cartesian AOs, %d shells, %d electrons"
                      % (mol.natm, ctx.nao, mol.nbas, mol.nelec), "setup_s": setup,
-           "target_eh": RHF_TARGET_EH}
-    out["reference"], P_ref = run(1e-8, density=True)
-    out["plain"] = run(1e-5)
-    out["mixed"] = run(1e-5, mixed=1, tau_fp32=TAU_FP32)
+           "target_eh": RHF_TARGET_EH, "tau": TAU, "tau_prim": TAU_PRIM, "tau_fp32": TAU_FP32}
+    out["plain"], P_plain = run(1e-5, density=True)
+    out["reference"], P_ref = run(1e-8, P0=P_plain, density=True)
+    out["reference"]["note"] = "plain FP64 continued from the plain run's density to 1e-8"
+    legs = ["plain"]
+    if ablations:
+        out["mixed"] = run(1e-5, mixed=1, tau_fp32=TAU_FP32)
+        legs.append("mixed")
     if guess_file and os.path.exists(guess_file):
         from librint_b200.guess import LearnedGuess
         g = LearnedGuess.load(guess_file)
@@ -644,13 +655,18 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True):
             tp = time.perf_counter()
             P0 = g.predict(mol, S=S_ov)
             t_pred = (time.perf_counter() - tp) * 1e3
-            out["learned_fp64"] = run(1e-5, P0=P0, extra_ms=t_pred)
+            if ablations:
+                out["learned_fp64"] = run(1e-5, P0=P0, extra_ms=t_pred)
+                legs.append("learned_fp64")
             out["learned_mixed"] = run(1e-5, P0=P0, extra_ms=t_pred, mixed=1, tau_fp32=TAU_FP32)
+            legs.append("learned_mixed")
             out["predict_ms"] = t_pred
         else:
             out["learned"] = "network does not apply to this basis"
+    if "learned_mixed" not in out and not ablations:
+        out["mixed"] = run(1e-5, mixed=1, tau_fp32=TAU_FP32)
+        legs.append("mixed")
     e_ref = out["reference"]["energy"]
-    legs = [k for k in ("plain", "mixed", "learned_fp64", "learned_mixed") if k in out]
     for k in legs:
         out[k]["dE_vs_reference"] = out[k]["energy"] - e_ref
         out[k]["speedup_vs_plain"] = out["plain"]["wall_s"] / out[k]["wall_s"]

@@ -179,6 +179,8 @@ typedef struct {
   int rebuild_every;  /* full (non-incremental) Fock build period */
   double tau_fp32;    /* screening threshold of the FP32 and split builds
                          (0: tau); the FP64 phase always screens at tau */
+  double tau_prim;    /* primitive-quartet screening of the Fock builds (0: off;
+                         see lrb_mol_set_tau_prim) */
 } LrbScfOptions;
 
 typedef struct {
@@ -186,6 +188,15 @@ typedef struct {
   int iterations, converged;
   long long quartets, fp32_quartets;
 } LrbScfResult;
+
+/* Primitive-quartet screening of a context's Fock builds (no reference
+ * counterpart; the reference screens primitives only by its exponent test,
+ * src/cint2e.rs:367-393): a primitive quartet of a kept shell quartet is
+ * skipped when Q_ij Q_kl d < tau_prim, Q the primitive pairs' Schwarz factors
+ * sqrt(max |(ij|ij)|) and d the shell quartet's density factor.  FP32 quartets
+ * use the larger of tau_prim and the build's quartet threshold.  0 (the
+ * default) keeps every primitive quartet the reference keeps. */
+LRB_API int lrb_mol_set_tau_prim(LrbMol *m, double tau_prim);
 
 /* RHF (src/scf.rs:743-969).  P_out (n*n host) and P0 (initial density,
  * overrides guess) may be NULL. */

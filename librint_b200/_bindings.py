@@ -67,7 +67,8 @@ class ScfOptions(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv", ctypes.c_double), ("guess", ctypes.c_int),
                 ("diis", ctypes.c_int), ("tau", ctypes.c_double), ("mixed", ctypes.c_int),
                 ("fp32_until", ctypes.c_double), ("tau32", ctypes.c_double),
-                ("rebuild_every", ctypes.c_int), ("tau_fp32", ctypes.c_double)]
+                ("rebuild_every", ctypes.c_int), ("tau_fp32", ctypes.c_double),
+                ("tau_prim", ctypes.c_double)]
 
 
 class ScfResult(ctypes.Structure):
@@ -88,6 +89,7 @@ def _optional(L):
         "lrb_mol_create": (c_int, (ctypes.POINTER(c_vp), P_i, c_int, P_i, c_int, P_d, c_ll)),
         "lrb_mol_destroy": (None, (c_vp,)),
         "lrb_mol_nao": (c_int, (c_vp,)),
+        "lrb_mol_set_tau_prim": (c_int, (c_vp, c_d)),
         "lrb_fock_G": (c_int, (c_vp, P_d, P_d, c_d, ctypes.POINTER(c_ll))),
         "lrb_fock_G_device": (c_int, (c_vp, c_vp, c_vp, c_d, c_vp)),
         "lrb_fock_G_part": (c_int, (c_vp, P_d, P_d, c_d, c_int, c_int, ctypes.POINTER(c_ll))),

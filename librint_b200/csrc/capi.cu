@@ -666,15 +666,26 @@ LRB_API int lrb_scf(LrbMol *m, long long nelec, const LrbScfOptions *opt, LrbScf
     o.tau = opt->tau; o.mixed = opt->mixed; o.fp32_until = opt->fp32_until;
     o.tau32 = opt->tau32; o.rebuild_every = opt->rebuild_every > 0 ? opt->rebuild_every : 6;
     o.tau_fp32 = opt->tau_fp32;
+    o.tau_prim = opt->tau_prim;
   }
   ScfResult r;
+  // the SCF's Fock builds screen primitive quartets at tau_prim (when > 0)
+  const double keep_prim = m->ctx.tau_prim;
+  if (o.tau_prim > 0.0) m->ctx.tau_prim = o.tau_prim;
   const int rc = scf_run(m->ctx, (size_t)nelec, o, &r, P_out, P0, nullptr);
+  m->ctx.tau_prim = keep_prim;
   if (res) {
     res->energy = r.energy; res->e_nuc = r.e_nuc; res->delta = r.delta; res->fock_ms = r.fock_ms;
     res->wall_ms = r.wall_ms; res->iterations = r.iterations; res->converged = r.converged;
     res->quartets = r.quartets; res->fp32_quartets = r.fp32_quartets;
   }
   return rc;
+}
+
+LRB_API int lrb_mol_set_tau_prim(LrbMol *m, double tau_prim) {
+  if (!m || !(tau_prim >= 0.0)) return set_error("need a molecule and tau_prim >= 0"), LRB_ERR_INPUT;
+  m->ctx.tau_prim = tau_prim;
+  return LRB_OK;
 }
 
 LRB_API int lrb_energy(LrbMol *m, const double *P, double tau, double *E) {

@@ -140,6 +140,13 @@ struct FockParams {
   // measurement only: when not NULL, the launch adds the number of primitive
   // quartets that passed screening (one atomic per warp at its end)
   unsigned long long *prim_count;
+  // primitive screening (when lq is not NULL): a primitive quartet is skipped
+  // when Q_bra Q_ket d < tau_prim, with Q the primitive pairs' Schwarz
+  // factors (log, float) and d the quartet's density factor from Dsh
+  const float *lq;
+  double tau_prim;
+  const double *Dsh;      // shell-block maxima of |P|, nbas x nbas
+  int nbas;
 };
 
 struct EriParams {

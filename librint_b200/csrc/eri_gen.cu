@@ -225,12 +225,23 @@ k_eri_gen(EriParams prm, FockParams fk, GenClass g, const double *__restrict__ r
     }
     for (int e = tid; e < ne; e += nt) acc[e] = 0.0;
     const double cut = prm.expcutoff;
+    // Fock mode, primitive screening (as the templated kernels)
+    float lthr = -INFINITY;
+    if (MODE == 1 && fk.lq) {
+      const int nb = fk.nbas;
+      const double *D = fk.Dsh;
+      const int I = job.ish, J = job.jsh, K = job.ksh, L = job.lsh;
+      const double dd = fmax(fmax(2.0 * D[I * nb + J], 2.0 * D[K * nb + L]),
+                             fmax(fmax(D[I * nb + K], D[I * nb + L]), fmax(D[J * nb + K], D[J * nb + L])));
+      lthr = dd > 0.0 ? (float)log(fk.tau_prim / dd) : INFINITY;
+    }
     for (int kl = 0; kl < job.nkl; ++kl) {
       const PrimPair ket = prm.pp[job.pkl_off + kl];
       if (ket.cce > cut) continue;           // uniform over the CTA
       for (int ij = 0; ij < job.nij; ++ij) {
         const PrimPair bra = prm.pp[job.pij_off + ij];
         if (bra.cce > cut - ket.cce) continue;
+        if (MODE == 1 && fk.lq && fk.lq[job.pij_off + ij] + fk.lq[job.pkl_off + kl] < lthr) continue;
         nprim += tid == 0;
         const double aij = bra.a, akl = ket.a, inv = 1.0 / (aij + akl);
         const double fac0 = sqrt(inv) * bra.facia * ket.facia;

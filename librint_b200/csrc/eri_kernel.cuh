@@ -501,6 +501,22 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
       nket = prm.pp[job.pkl_off + kl];
       nbra = prm.pp[job.pij_off + ij];
     }
+    // Fock mode, primitive screening: log(tau_prim / d) with d the quartet's
+    // density factor (the same maximum the quartet screening uses)
+    const bool pscreen = MODE == 1 && fk.lq != nullptr;
+    float lthr = 0.f, nlqb = 0.f, nlqk = 0.f;
+    if (MODE == 1 && pscreen && have) {
+      const int nb = fk.nbas;
+      const double *D = fk.Dsh;
+      const int I = job.ish, J = job.jsh, K = job.ksh, L = job.lsh;
+      const double dd = fmax(fmax(2.0 * D[I * nb + J], 2.0 * D[K * nb + L]),
+                             fmax(fmax(D[I * nb + K], D[I * nb + L]), fmax(D[J * nb + K], D[J * nb + L])));
+      lthr = dd > 0.0 ? (float)log(fk.tau_prim / dd) : INFINITY;
+      if (np > 0) {
+        nlqb = fk.lq[job.pij_off + ij];
+        nlqk = fk.lq[job.pkl_off + kl];
+      }
+    }
     for (int it = 0; it < npmax * reps; ++it) {
       const bool lr_part = reps == 2 && (it & 1);
       const int p = reps == 2 ? (it >> 1) : it;
@@ -518,14 +534,20 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
             }
           }
         } else {
-          // screening (reference src/cint2e.rs:367-393)
+          // screening (reference src/cint2e.rs:367-393), then the primitive
+          // Schwarz x density test
           run = !(ket.cce > cut) && !(bra.cce > cut - ket.cce);
+          if (pscreen) run = run && nlqb + nlqk >= lthr;
           if (++ij == job.nij) { ij = 0; ++kl; }
           nprim += run && rho == 0;
         }
         if (p + 1 < np) {
           nket = prm.pp[job.pkl_off + kl];
           nbra = prm.pp[job.pij_off + ij];
+          if (pscreen) {
+            nlqb = fk.lq[job.pij_off + ij];
+            nlqk = fk.lq[job.pkl_off + kl];
+          }
         }
       }
       // Roots, weights, prefactors and the per-unit coefficients are FP64 in

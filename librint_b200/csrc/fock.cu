@@ -100,6 +100,23 @@ __global__ void k_schwarz(const double *__restrict__ blocks, const long long *__
   Q[p] = sqrt(m);
 }
 
+// log of each primitive pair's Schwarz factor, sqrt(max |(ab|ab)|) over the
+// cartesian components of its (ij|ij) block (float; -inf when zero).
+__global__ void k_prim_schwarz(const double *__restrict__ blocks, const long long *__restrict__ roff,
+                               const int *__restrict__ rdim, int nrec, float *lq) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrec) return;
+  const int ni = rdim[2 * r], nj = rdim[2 * r + 1];
+  const double *b = blocks + roff[r];
+  double m = 0.0;
+  for (int a = 0; a < ni; ++a)
+    for (int c = 0; c < nj; ++c) {
+      const long long e = a + (long long)ni * (c + (long long)nj * (a + (long long)ni * c));
+      m = fmax(m, fabs(b[e]));
+    }
+  lq[r] = m > 0.0 ? (float)(0.5 * log(m)) : -INFINITY;
+}
+
 // Shell-block maxima of |P|.
 __global__ void k_dens_max(const double *__restrict__ P, int n, const int *__restrict__ aooff,
                            int nbas, double *Dsh) {
@@ -361,6 +378,75 @@ static int mol_create_segmented(MolCtx &m, const int *atm, int natm, const int *
   cudaFreeAsync(d_boff, st);
   cudaFreeAsync(d_blk, st);
   FK_CK(cudaStreamSynchronize(st));
+  // Schwarz factor of every primitive pair (the Fock builds' primitive
+  // screening): (ij|ij) of single-primitive shells, in chunks of records
+  // whose blocks take at most 256 MB
+  {
+    std::vector<int> pfirst(nbas + 1, 0);
+    for (int sh = 0; sh < nbas; ++sh) pfirst[sh + 1] = pfirst[sh] + bas[8 * sh + 2];
+    const int nps = pfirst[nbas];
+    std::vector<int> pbas(8 * (size_t)nps);
+    for (int sh = 0; sh < nbas; ++sh)
+      for (int q = 0; q < bas[8 * sh + 2]; ++q) {
+        int *r = &pbas[8 * (size_t)(pfirst[sh] + q)];
+        const int *b = bas + 8 * sh;
+        r[0] = b[0]; r[1] = b[1]; r[2] = 1; r[3] = 1; r[4] = b[4];
+        r[5] = b[5] + q; r[6] = b[6] + q; r[7] = b[7] > 0 ? b[7] + q : 0;
+      }
+    std::vector<int> rq(4 * (size_t)npp), rdim(2 * (size_t)npp);
+    for (int q = 0; q < m.npairs; ++q) {
+      const int I = pr[q].ish, J = pr[q].jsh, ki = bas[8 * I + 2];
+      for (int e = 0; e < pr[q].npp; ++e) {
+        const int r = pr[q].pp_off + e;
+        const int a = pfirst[I] + e % ki, b = pfirst[J] + e / ki;
+        rq[4 * (size_t)r] = a; rq[4 * (size_t)r + 1] = b;
+        rq[4 * (size_t)r + 2] = a; rq[4 * (size_t)r + 3] = b;
+        rdim[2 * (size_t)r] = ncart(bas[8 * I + 1]);
+        rdim[2 * (size_t)r + 1] = ncart(bas[8 * J + 1]);
+      }
+    }
+    int *d_pbas = nullptr, *d_rq = nullptr, *d_rdim = nullptr;
+    if (!al((void **)&m.lq, sizeof(float) * (size_t)npp) ||
+        !al((void **)&d_pbas, sizeof(int) * pbas.size()) || !al((void **)&d_rq, sizeof(int) * rq.size()) ||
+        !al((void **)&d_rdim, sizeof(int) * rdim.size()))
+      return set_error("molecule: device allocation failed"), LRB_ERR_ALLOC;
+    FK_CK(cudaMemcpyAsync(d_pbas, pbas.data(), sizeof(int) * pbas.size(), cudaMemcpyHostToDevice, st));
+    FK_CK(cudaMemcpyAsync(d_rq, rq.data(), sizeof(int) * rq.size(), cudaMemcpyHostToDevice, st));
+    FK_CK(cudaMemcpyAsync(d_rdim, rdim.data(), sizeof(int) * rdim.size(), cudaMemcpyHostToDevice, st));
+    const long long cap = 256LL << 17;   // doubles of blocks per chunk (256 MB)
+    for (int r0 = 0; r0 < npp;) {
+      std::vector<long long> roff{0};
+      int r1 = r0;
+      while (r1 < npp) {
+        const long long sz = (long long)rdim[2 * (size_t)r1] * rdim[2 * (size_t)r1 + 1];
+        if (r1 > r0 && roff.back() + sz * sz > cap) break;
+        roff.push_back(roff.back() + sz * sz);
+        ++r1;
+      }
+      long long *d_roff = nullptr;
+      double *d_pb = nullptr;
+      if (!al((void **)&d_roff, sizeof(long long) * roff.size()) ||
+          !al((void **)&d_pb, sizeof(double) * (size_t)roff.back()))
+        return set_error("molecule: device allocation failed"), LRB_ERR_ALLOC;
+      FK_CK(cudaMemcpyAsync(d_roff, roff.data(), sizeof(long long) * roff.size(),
+                            cudaMemcpyHostToDevice, st));
+      int rc2 = eri_batch_device(engine(), d_pb, 0, d_rq + 4 * (size_t)r0, r1 - r0, m.atm, natm,
+                                 d_pbas, nps, m.env, nenv, st, nullptr, nullptr, m.gc);
+      if (rc2) return rc2;
+      k_prim_schwarz<<<(r1 - r0 + 255) / 256, 256, 0, st>>>(d_pb, d_roff, d_rdim + 2 * (size_t)r0,
+                                                             r1 - r0, m.lq + r0);
+      engine().launches++;
+      FK_CK(cudaGetLastError());
+      cudaFreeAsync(d_roff, st);
+      cudaFreeAsync(d_pb, st);
+      FK_CK(cudaStreamSynchronize(st));   // roff goes out of scope
+      r0 = r1;
+    }
+    cudaFreeAsync(d_pbas, st);
+    cudaFreeAsync(d_rq, st);
+    cudaFreeAsync(d_rdim, st);
+    FK_CK(cudaStreamSynchronize(st));
+  }
   // pairs by descending Schwarz factor, for the candidate enumeration
   {
     std::vector<double> q(m.npairs);
@@ -384,7 +470,8 @@ static int mol_create_segmented(MolCtx &m, const int *atm, int natm, const int *
 void mol_destroy(MolCtx &m, cudaStream_t st) {
   for (void *p : {(void *)m.atm, (void *)m.bas, (void *)m.env, (void *)m.aooff, (void *)m.pairs,
                   (void *)m.pcls, (void *)m.pp, (void *)m.Q, (void *)m.Dsh, (void *)m.centers,
-                  (void *)m.qorder, (void *)m.Qs, (void *)m.qcnt, (void *)m.qoff, (void *)m.dmax})
+                  (void *)m.qorder, (void *)m.Qs, (void *)m.qcnt, (void *)m.qoff, (void *)m.dmax,
+                  (void *)m.lq})
     if (p) cudaFreeAsync(p, st);
   cudaStreamSynchronize(st);
 }
@@ -485,6 +572,13 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     fk.K = K;
     fk.n = n;
     fk.prim_count = nullptr;
+    // primitive screening: the FP64 quartets at the context's threshold, the
+    // FP32 ones at the larger of it and the build's quartet threshold
+    const double tprim = m.tau_prim > 0.0 ? (prec == 1 ? std::max(m.tau_prim, tau) : m.tau_prim) : 0.0;
+    fk.lq = tprim > 0.0 ? m.lq : nullptr;
+    fk.tau_prim = tprim;
+    fk.Dsh = m.Dsh;
+    fk.nbas = nbas;
     if (eng.profile && !eng.fock_prim) {
       if (cudaMalloc((void **)&eng.fock_prim, 128 * sizeof(unsigned long long)) != cudaSuccess)
         return set_error("fock: counter allocation failed"), LRB_ERR_ALLOC;

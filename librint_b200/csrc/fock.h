@@ -24,6 +24,11 @@ struct MolCtx {
   int *qorder = nullptr, *qcnt = nullptr;
   double *Qs = nullptr, *dmax = nullptr;
   long long *qoff = nullptr;
+  // log Schwarz factor of every primitive pair (same order as pp), and the
+  // primitive-quartet screening threshold of this context's Fock builds
+  // (0: only the reference's exponent screening)
+  float *lq = nullptr;
+  double tau_prim = 0.0;
 };
 
 struct FockStats {
@@ -41,6 +46,7 @@ struct ScfOptions {
   double tau32 = 1e-7;     // afterwards FP32 only for bounds below this
   int rebuild_every = 6;   // full (non-incremental) build period
   double tau_fp32 = 0.0;   // screening of the FP32 / split builds (0: tau)
+  double tau_prim = 0.0;   // primitive-quartet screening of the Fock builds (0: off)
 };
 
 struct ScfResult {

@@ -52,6 +52,11 @@ class MolContext:
         B.check(rc, "lrb_fock_G")
         return G
 
+    def set_tau_prim(self, tau_prim: float):
+        """Primitive-quartet screening threshold of this context's Fock
+        builds (lrb_mol_set_tau_prim; 0 keeps every primitive quartet)."""
+        B.check(B.lib().lrb_mol_set_tau_prim(self.h, tau_prim), "lrb_mol_set_tau_prim")
+
     def fock_G_part(self, P, tau: float, rank: int, nranks: int):
         """This rank's share of G(P) (lrb_fock_G_part); the shares of ranks
         0..nranks-1 sum to fock_G(P, tau).  Returns (G share, quartets)."""
@@ -95,17 +100,19 @@ class MolContext:
 
     def scf(self, nelec=None, max_iter=100, conv=1e-10, guess=0, diis=0, tau=0.0, P0=None,
             return_density=False, mixed=0, fp32_until=1e-3, tau32=1e-7, rebuild_every=6,
-            check=True, tau_fp32=0.0):
+            check=True, tau_fp32=0.0, tau_prim=0.0):
         """RHF.  Defaults are the reference's algorithm (P0 = I, plain
         Roothaan, FP64, no screening); guess=1 / diis / tau / mixed select
         the faster schedules, which change iterations and time, not the
         converged energy (mixed: within the tolerance stated in the tests).
         check=False returns a non-converged result (``r.converged`` 0)
         instead of raising.  tau_fp32 (mixed only) is the screening threshold
-        of the FP32 and split builds; the FP64 phase screens at tau."""
+        of the FP32 and split builds; the FP64 phase screens at tau.
+        tau_prim > 0 also skips primitive quartets whose Schwarz x density
+        bound is below it (lrb_mol_set_tau_prim) for this SCF's builds."""
         nelec = self.m.nelec if nelec is None else nelec
         o = B.ScfOptions(max_iter, conv, guess, diis, tau, mixed, fp32_until, tau32, rebuild_every,
-                         tau_fp32)
+                         tau_fp32, tau_prim)
         r = B.ScfResult()
         P = np.empty((self.nao, self.nao))
         p0 = None if P0 is None else np.ascontiguousarray(P0, dtype=np.float64).ctypes.data_as(B.P_d)
