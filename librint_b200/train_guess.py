@@ -1,21 +1,23 @@
 """Train the learned initial guess on densities the GPU SCF generates.
 
-    python -m librint_b200.train_guess --train 2000 --test 200 --flakes 100 \
-        --test-flakes 10 --out librint_b200/data/guess_ch.npz --summary summary.json
+    python -m librint_b200.train_guess --train 2000 --test 200 --flakes 60 \
+        --test-flakes 8 --gen-conv 1e-6 --gen-mixed --tau-prim 1e-15 \
+        --out librint_b200/data/guess_ch.npz --summary summary.json
 
 Data: seeded C6H6-like rings (``synthetic.benzene_like``: bonds +-0.05 A,
-angles +-3 deg, the even-tempered DZP-like C 3s2p1d / H 2s1p set, 120
-cartesian AOs), geometry seeds 10000 + i; optionally (``--flakes``) small
-C/H flakes of the same lattice construction as the 610-AO cluster
+angles +-3 deg, the seed-3 per-element C 3s2p1d / H 2s1p basis with K =
+1..6, 120 cartesian AOs), geometry seeds 10000 + i; optionally (``--flakes``)
+small C/H flakes of the same lattice construction as the 660-AO cluster
 (``synthetic.flake_like``, seeds 20000 + i), so that the network also sees
 interior carbons.  Each density comes from this library's RHF
-(core-Hamiltonian guess, DIIS, FP64, density change <= conv).  After the
-first ``--bootstrap`` ring geometries a provisional network is trained and
-used as the starting density for the rest, which only shortens data
-generation (the converged densities do not depend on the start).  The final
-network is trained on the GPU with this library's MLP kernels, then judged
-on held-out geometries by SCF: energies against the core-Hamiltonian start,
-iterations and wall time.
+(core-Hamiltonian guess, DIIS, density change <= --gen-conv; with
+--gen-mixed the mixed-precision schedule, which ends with FP64 builds).
+After the first ``--bootstrap`` ring geometries a provisional network is
+trained and used as the starting density for the rest, which only shortens
+data generation (the converged densities do not depend on the start).  The
+final network is trained on the GPU with this library's MLP kernels, then
+judged on held-out geometries by FP64 SCF to --conv: energies against the
+core-Hamiltonian start, iterations and wall time.
 """
 from __future__ import annotations
 
@@ -31,6 +33,9 @@ from .guess import LearnedGuess, PairModel, lowdin
 from .scf import MolContext
 
 SCF_OPTS = dict(guess=1, diis=8, tau=1e-12, max_iter=100)
+# extra options of the SCFs that generate the training densities (--gen-mixed,
+# --tau-prim); the held-out evaluation runs SCF_OPTS plus --tau-prim
+GEN_OPTS: dict = {}
 
 
 def geometry(i: int, family: str = "rings"):
@@ -51,10 +56,10 @@ def run_scf(m, conv, guess=None):
         r = None
         if guess is not None:
             r, P = ctx.scf(conv=conv, P0=guess.predict(m, S=S), return_density=True, check=False,
-                           **SCF_OPTS)
+                           **dict(SCF_OPTS, **GEN_OPTS))
         if r is None or not r.converged:
             r, P = ctx.scf(conv=conv, return_density=True, check=False,
-                           **dict(SCF_OPTS, max_iter=300))
+                           **dict(SCF_OPTS, max_iter=300, **GEN_OPTS))
     finally:
         ctx.close()
     if not r.converged:          # no usable target (e.g. a near-degenerate flake)
@@ -152,7 +157,14 @@ def main(argv=None):
     ap.add_argument("--flakes", type=int, default=0, help="flake geometries for training")
     ap.add_argument("--test-flakes", type=int, default=0, help="held-out flake geometries")
     ap.add_argument("--bootstrap", type=int, default=200)
-    ap.add_argument("--conv", type=float, default=1e-8)
+    ap.add_argument("--conv", type=float, default=1e-8,
+                    help="density convergence of the held-out evaluation SCFs")
+    ap.add_argument("--gen-conv", type=float, default=None,
+                    help="density convergence of the training SCFs (default: --conv)")
+    ap.add_argument("--gen-mixed", action="store_true",
+                    help="training SCFs with the mixed-precision incremental schedule")
+    ap.add_argument("--tau-prim", type=float, default=0.0,
+                    help="primitive-quartet screening of every SCF (0: off)")
     ap.add_argument("--hidden", type=int, nargs="+", default=[256, 256, 256])
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--batch", type=int, default=2048)
@@ -163,6 +175,12 @@ def main(argv=None):
     ap.add_argument("--densities", default=None, help="cache file for the training densities")
     a = ap.parse_args(argv)
 
+    gen_conv = a.gen_conv if a.gen_conv else a.conv
+    if a.gen_mixed:
+        GEN_OPTS.update(mixed=1, tau_fp32=1e-11)
+    if a.tau_prim > 0:
+        GEN_OPTS["tau_prim"] = a.tau_prim
+        SCF_OPTS["tau_prim"] = a.tau_prim
     model = PairModel.from_molecule(geometry(0))
     train_ids = [("rings", i) for i in range(a.train)] + [("flakes", i) for i in range(a.flakes)]
     test_ids = [("rings", i) for i in range(a.train, a.train + a.test)] + \
@@ -177,12 +195,12 @@ def main(argv=None):
     else:
         nb = min(a.bootstrap, a.train)
         print(f"generating {nb} densities from the core-Hamiltonian start")
-        kept, dens, stats = generate(train_ids[:nb], a.conv)
+        kept, dens, stats = generate(train_ids[:nb], gen_conv)
         if nb < len(train_ids):
             g0 = fit(model, kept, dens, a.hidden, max(40, a.epochs // 5),
                      a.batch, a.lr, a.seed, log=None)[0] if kept else None
             print(f"generating {len(train_ids) - nb} more from the provisional network")
-            k2, d2, s2 = generate(train_ids[nb:], a.conv, guess=g0)
+            k2, d2, s2 = generate(train_ids[nb:], gen_conv, guess=g0)
             kept += k2
             dens += d2
             stats += s2
@@ -203,7 +221,8 @@ def main(argv=None):
     summary = dict(train=a.train, flakes=a.flakes, test=a.test, test_flakes=a.test_flakes,
                    train_converged=len(train_ids),
                    samples=nsamp, hidden=a.hidden, epochs=a.epochs, batch=a.batch, lr=a.lr,
-                   conv=a.conv, scf_options=SCF_OPTS, gen_seconds=t_gen,
+                   conv=a.conv, gen_conv=gen_conv, scf_options=SCF_OPTS, gen_options=GEN_OPTS,
+                   gen_seconds=t_gen,
                    gen_iterations_mean=float(st[:, 0].mean()), gen_ms_mean=float(st[:, 1].mean()),
                    train_seconds=t_train, loss_first=hist[0], loss_last=hist[-1],
                    heldout=ev, heldout_rows=rows[:40])

@@ -181,5 +181,8 @@ def assert_close_block_scale(got, ref, m, shls, coord, scale_values=None, rel_bl
     got, ref = np.asarray(got), np.asarray(ref)
     scale = block_scale(m, shls, coord, ref if scale_values is None else scale_values)
     bad = np.abs(got - ref) > ERI_RTOL * np.abs(ref) + rel_block * scale + ERI_ATOL
-    assert not bad.any(), (f"{what}: {bad.sum()} of {bad.size} outside; worst relative to the "
-                           f"block scale {(np.abs(got - ref) / np.maximum(scale, 1e-300)).max():.3e}")
+    if bad.any():
+        rel = (np.abs(got - ref) / np.maximum(scale, 1e-300))[bad]
+        raise AssertionError(f"{what}: {bad.sum()} of {bad.size} outside; flagged elements: largest "
+                             f"|diff| {np.abs(got - ref)[bad].max():.3e}, largest |diff| / block "
+                             f"scale {rel.max():.3e}")

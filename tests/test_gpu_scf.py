@@ -171,3 +171,35 @@ def test_fock_partition_shares_sum_to_G(golden, nranks):
         assert min(p[1] for p in parts) > 0
         np.testing.assert_allclose(S, G, rtol=1e-12, atol=1e-12 * np.abs(G).max())
     ctx.close()
+
+
+def test_primitive_screening_error():
+    """Primitive-quartet screening (lrb_mol_set_tau_prim) at 1e-15 changes
+    G(P) at a converged density by far less than 1e-9 per element, skips
+    primitive quartets, and leaves the converged SCF energy within 1e-9 Eh;
+    0 restores the reference's primitive set."""
+    import ctypes
+    from librint_b200 import _bindings as B
+    m = _ring()
+    ctx = scf.MolContext(m)
+    r0, P = ctx.scf(conv=1e-9, guess=1, diis=8, tau=1e-13, return_density=True)
+    L = B.lib()
+    counts = []
+    for tp in (0.0, 1e-15, 0.0):
+        ctx.set_tau_prim(tp)
+        L.lrb_fock_class_counts((ctypes.c_longlong * 128)(), (ctypes.c_longlong * 128)(), 128)
+        L.lrb_profile_enable(1)
+        G = ctx.fock_G(P, 1e-13)
+        L.lrb_profile_enable(0)
+        L.lrb_profile_read((ctypes.c_double * 128)(), 128)
+        q, p = (ctypes.c_longlong * 128)(), (ctypes.c_longlong * 128)()
+        L.lrb_fock_class_counts(q, p, 128)
+        counts.append((G, sum(p)))
+    (G0, p0), (G1, p1), (G2, p2) = counts
+    print(f"primitive quartets {p0} -> {p1}; max |dG| {np.abs(G1 - G0).max():.3e}")
+    assert p1 < p0 and p2 == p0
+    assert np.abs(G1 - G0).max() < 1e-9
+    assert np.abs(G2 - G0).max() < 1e-12      # atomics order only
+    r1 = ctx.scf(conv=1e-9, guess=1, diis=8, tau=1e-13, tau_prim=1e-15)
+    ctx.close()
+    assert abs(r1.energy - r0.energy) < 1e-9, (r1.energy, r0.energy)
