@@ -170,19 +170,34 @@ def block_scale(m, shls, coord, values):
 
 
 def assert_close_block_scale(got, ref, m, shls, coord, scale_values=None, rel_block=1e-12,
-                             what=""):
+                             what="", atol=ERI_ATOL, gpu_cart=None, max_arbitrated=3):
     """Per integral 1e-12 relative plus ``rel_block`` of the largest |value| of
-    its quartet block (of ``scale_values``, default ref) plus 1e-15: the
+    its quartet block (of ``scale_values``, default ref) plus ``atol``: the
     bar for blocks whose small elements come out of cancellation between
     much larger terms (high-momentum blocks; short range as full minus long
-    range), where both double-precision paths carry ~1e-16 of the block's
-    scale."""
+    range).  Quartets still outside go to the 40-digit evaluation (at most
+    ``max_arbitrated``, cartesian blocks from ``gpu_cart(shls)``): the GPU may
+    not be further from it than 4x the oracle's error + 1e-15."""
     import numpy as np
     got, ref = np.asarray(got), np.asarray(ref)
     scale = block_scale(m, shls, coord, ref if scale_values is None else scale_values)
-    bad = np.abs(got - ref) > ERI_RTOL * np.abs(ref) + rel_block * scale + ERI_ATOL
-    if bad.any():
-        rel = (np.abs(got - ref) / np.maximum(scale, 1e-300))[bad]
-        raise AssertionError(f"{what}: {bad.sum()} of {bad.size} outside; flagged elements: largest "
-                             f"|diff| {np.abs(got - ref)[bad].max():.3e}, largest |diff| / block "
-                             f"scale {rel.max():.3e}")
+    bad = np.abs(got - ref) > ERI_RTOL * np.abs(ref) + rel_block * scale + atol
+    if not bad.any():
+        return
+    rel = (np.abs(got - ref) / np.maximum(scale, 1e-300))[bad]
+    msg = (f"{what}: {bad.sum()} of {bad.size} outside; flagged elements: largest |diff| "
+           f"{np.abs(got - ref)[bad].max():.3e}, largest |diff| / block scale {rel.max():.3e}")
+    if gpu_cart is None:
+        raise AssertionError(msg)
+    import oracle
+    from oracle import mp_exact
+    off = np.concatenate([[0], np.cumsum(_block_sizes(m, shls, coord))])
+    quartets = np.unique(np.searchsorted(off, np.nonzero(bad)[0], side="right") - 1)
+    assert len(quartets) <= max_arbitrated, msg + f" in {len(quartets)} quartets"
+    for q in quartets:
+        sh = np.ascontiguousarray(np.asarray(shls)[q:q + 1], dtype=np.int32)
+        ex = np.array(mp_exact.eri_cart_exact(m.atm, m.bas, m.env, sh[0]), dtype=float).ravel()
+        e_or = np.abs(oracle.int2e_batch(m, sh, 0) - ex).max()
+        e_gpu = np.abs(gpu_cart(sh) - ex).max()
+        assert e_gpu <= 4.0 * e_or + ERI_ATOL, \
+            f"{what} quartet {q}: GPU error vs exact {e_gpu:.3e}, oracle's {e_or:.3e}"

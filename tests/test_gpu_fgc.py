@@ -46,16 +46,23 @@ def test_f_class_samples(golden_fgc, cls):
 def test_f_sweep_vs_oracle(cls):
     """300 quartets per f class, compact sweep distribution (centres in a
     2.5 A cube, K = 1..4, exponents log-uniform in [0.1, 50]), cartesian and
-    spherical, against the oracle: 1e-12 relative per integral plus 1e-13 of
-    its block's largest element (the small elements of (fd|fd)-size blocks
-    come out of cancellation; the reference's own error there reaches 6e-13
-    of the block scale)."""
+    spherical, against the oracle: 1e-12 relative per integral plus 2e-11 of
+    its block's largest element.  The small elements of these blocks come
+    out of cancellation in the horizontal recurrences: against 40-digit
+    values both paths err by up to ~2e-11 of the block scale (measured: an
+    (ff|ss) quartet, GPU 3.0e-16 and oracle 2.3e-15 on a scale of 1.5e-4;
+    another, GPU 1.7e-14 and oracle 2.9e-15 on 3.5e-3; (fd|dd), GPU 7.4e-15
+    and oracle 1.5e-14 on 7.3e-3), and the reference differs from the oracle
+    by 3.7e-11 of the block scale on these quartets.  The few quartets beyond
+    that go to the 40-digit arbiter (an (ff|dd) quartet: GPU 9.7e-13, oracle
+    4.3e-13 on a block scale of 0.018)."""
     m, shls = synthetic.eri_sweep(cls, 300, seed=31, kmax=4, cube_ang=2.5, elo=0.1, ehi=50.0)
     for coord in (0, 1):
         got = eri.int2e_batch(m, shls, coord)
         ref = oracle.int2e_batch(m, shls, coord)
-        assert_close_block_scale(got, ref, m, shls, coord, rel_block=1e-13,
-                                 what=f"f sweep {cls} coord {coord}")
+        assert_close_block_scale(got, ref, m, shls, coord, rel_block=2e-11,
+                                 what=f"f sweep {cls} coord {coord}",
+                                 gpu_cart=lambda sh: eri.int2e_batch(m, sh, 0))
 
 
 @pytest.mark.parametrize("key", ["gc", "fpol"])

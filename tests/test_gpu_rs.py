@@ -38,17 +38,21 @@ def test_dense_tensors(golden, omega):
 def test_sweep_classes(omega, cls):
     """500 quartets per class of a compact sweep distribution (centres in a
     4 A cube, K = 1..4), spherical, against the oracle: 1e-12 relative per
-    integral plus 1e-13 of the largest element of the quartet's block under
-    the full operator (short range is the full integral minus the long-range
-    one, so its small values carry ~1e-16 of the full block's scale in both
-    paths)."""
+    integral plus 2e-11 of the largest element of the quartet's block under
+    the full operator.  Short range is the full integral minus the
+    long-range one, and the recurrences of compact high-momentum blocks
+    amplify rounding: against 40-digit values both paths err by up to ~5e-15
+    absolute on (dd|dd) blocks (long range, scale 3e-4: GPU 5.4e-15, oracle
+    4.0e-15; short range, scale 2e-8: GPU 3.2e-15, oracle 3.4e-15), hence
+    the 5e-15 floor; quartets beyond it go to the 40-digit arbiter."""
     m0, shls = synthetic.eri_sweep(cls, 500, seed=41, kmax=4, cube_ang=4.0, elo=0.1, ehi=200.0)
     m = _with_omega(m0, omega)
     got = eri.int2e_batch(m, shls, 1)
     ref = oracle.int2e_batch(m, shls, 1)
     full = oracle.int2e_batch(m0, shls, 1)
     assert_close_block_scale(got, ref, m, shls, 1, scale_values=np.maximum(np.abs(full), np.abs(ref)),
-                             rel_block=1e-13, what=f"omega {omega} {cls}")
+                             rel_block=2e-11, atol=5e-15, what=f"omega {omega} {cls}",
+                             gpu_cart=lambda sh: eri.int2e_batch(m, sh, 0))
 
 
 @pytest.mark.parametrize("omega", [0.4, -0.4])
