@@ -99,6 +99,12 @@ LRB_API int lrb_profile_read(double *ms, int n);
  * plus 55 for the FP32 kernels) the shell quartets and the primitive
  * quartets that passed screening, since the last read (which clears them). */
 LRB_API int lrb_fock_class_counts(long long *quartets, long long *prim_quartets, int n);
+/* Fock builds: shell quartets of the small classes ((ss|ss) ... (dp|ss), at
+ * most 27 cartesian elements) with at least kmin primitive quartets run one
+ * lane per primitive quartet instead of one slot per shell quartet.  kmin > 0
+ * sets the bound for the process (default 32, or LRB_FOCK_LP_MIN; 1048576
+ * disables those kernels); every call returns the bound in force. */
+LRB_API int lrb_fock_lane_min(int kmin);
 LRB_API long long lrb_launch_count(void);
 LRB_API double lrb_fp64_peak_probe(int ms);
 

@@ -85,6 +85,7 @@ def _optional(L):
         "lrb_profile_read": (c_int, (P_d, c_int)),
         "lrb_launch_count": (c_ll, ()),
         "lrb_fock_class_counts": (c_int, (ctypes.POINTER(c_ll), ctypes.POINTER(c_ll), c_int)),
+        "lrb_fock_lane_min": (c_int, (c_int,)),
         "lrb_fp64_peak_probe": (c_d, (c_int,)),
         "lrb_mol_create": (c_int, (ctypes.POINTER(c_vp), P_i, c_int, P_i, c_int, P_d, c_ll)),
         "lrb_mol_destroy": (None, (c_vp,)),

@@ -383,6 +383,11 @@ const ClassEntry *class_table() {
       if (!g_classes[c].gen)
         e = cudaFuncSetAttribute(g_classes[c].fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)g_classes[c].smem[m]);
+  for (int c = 0; c < NCLASS && e == cudaSuccess && filled; ++c)
+    for (int m = 0; m < 2 && e == cudaSuccess; ++m)
+      if (!g_classes[c].gen && g_classes[c].lp[m])
+        e = cudaFuncSetAttribute(g_classes[c].lp[m], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)g_classes[c].lp_smem[m]);
   if (e != cudaSuccess) {
     char msg[160];
     snprintf(msg, sizeof msg, "ERI kernel table set-up on device %d failed: %s", dev,

@@ -38,6 +38,8 @@ cudaError_t eri_register_gen(const double *c2s_host);   // per device
 struct ClassEntry {
   EriKernelFn fn[3];     // output (FP64), Fock digestion FP64, Fock digestion FP32
   size_t smem[3];
+  EriKernelFn lp[2];     // Fock lane-per-primitive kernels (FP64, FP32) or NULL
+  size_t lp_smem[2];
   int slots, nr;
   int gen;               // 1: k_eri_gen with `g` (fn unused)
   GenClass g;
@@ -56,6 +58,14 @@ ClassEntry make_entry() {
   e.slots = C::SLOTS;
   e.nr = C::NR;
   e.gen = 0;
+  e.lp[0] = e.lp[1] = nullptr;
+  e.lp_smem[0] = e.lp_smem[1] = 0;
+  if constexpr (lp_class<LI, LJ, LK, LL>()) {
+    e.lp[0] = k_fock_lp<LI, LJ, LK, LL, double>;
+    e.lp[1] = k_fock_lp<LI, LJ, LK, LL, float>;
+    e.lp_smem[0] = LpLayout<LI, LJ, LK, LL, double>::SMEM;
+    e.lp_smem[1] = LpLayout<LI, LJ, LK, LL, float>::SMEM;
+  }
   return e;
 }
 

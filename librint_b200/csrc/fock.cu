@@ -11,6 +11,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <vector>
 
@@ -33,6 +34,22 @@ const double *rys_table_device();
   } while (0)
 
 namespace {
+
+// Quartets with at least this many primitive quartets run one lane per
+// primitive quartet where the class has that kernel (LRB_FOCK_LP_MIN or
+// lrb_fock_lane_min override it; 0x100000 turns the lane kernels off).
+std::atomic<int> g_lp_min{0};
+int fock_lp_min() {
+  int v = g_lp_min.load();
+  if (v == 0) {
+    const char *e = getenv("LRB_FOCK_LP_MIN");
+    const long x = e ? strtol(e, nullptr, 10) : LP_MIN_PRIM;
+    v = (int)std::min(std::max(x, 1L), 0x100000L);
+    int z = 0;
+    if (!g_lp_min.compare_exchange_strong(z, v)) v = z;
+  }
+  return v;
+}
 
 __device__ inline double fac_sp_d(int l) {
   return l == 0 ? 0.28209479177387814 : (l == 1 ? 0.48860251190291992 : 1.0);
@@ -234,12 +251,15 @@ __global__ void k_screen_sorted(const PairInfo *__restrict__ pairs, const int *_
   }
 }
 
+// starts[c] = first sorted position whose key is >= (c << 20) + add: add = 0
+// gives the class boundaries, add = 0x100000 - kmin the first quartet of
+// class c with fewer than kmin primitive quartets
 __global__ void k_class_starts_f(const unsigned *__restrict__ keys, long long n, int ncls,
-                                 long long *starts) {
+                                 unsigned add, long long *starts) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c > ncls) return;
   long long lo = 0, hi = n;
-  const unsigned key = (unsigned)c << 20;
+  const unsigned key = ((unsigned)c << 20) + add;
   while (lo < hi) {
     const long long mid = (lo + hi) >> 1;
     if (keys[mid] < key) lo = mid + 1; else hi = mid;
@@ -512,8 +532,8 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
   const size_t cap = (size_t)std::max(ncand, 1LL);
   const size_t need = carve_size(sizeof(int2) * cap) + 2 * carve_size(sizeof(unsigned) * cap) +
                       2 * carve_size(sizeof(int) * cap) + 2 * carve_size(sizeof(double) * (size_t)n * n) +
-                      carve_size(sizeof(long long) * 128) + carve_size(sizeof(unsigned long long)) +
-                      carve_size(sizeof(int) * 128);
+                      carve_size(sizeof(long long) * 256) + carve_size(sizeof(unsigned long long)) +
+                      carve_size(sizeof(int) * 256);
   char *base = eng.ws.reserve_extra(st, need) ? (char *)eng.ws.extra.ptr : nullptr;
   if (!base) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
   Carver cv(base);
@@ -521,13 +541,13 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
   unsigned *keys = cv.take<unsigned>(cap), *keys2 = cv.take<unsigned>(cap);
   int *idx = cv.take<int>(cap), *idx2 = cv.take<int>(cap);
   double *J = cv.take<double>((size_t)n * n), *K = cv.take<double>((size_t)n * n);
-  long long *starts = cv.take<long long>(128);
+  long long *starts = cv.take<long long>(256);
   unsigned long long *count = cv.take<unsigned long long>(1);
-  int *counters = cv.take<int>(128);
+  int *counters = cv.take<int>(256);   // task counters: slot kernels, then lane kernels
   FK_CK(cudaMemsetAsync(J, 0, sizeof(double) * (size_t)n * n, st));
   FK_CK(cudaMemsetAsync(K, 0, sizeof(double) * (size_t)n * n, st));
   FK_CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
-  FK_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 128, st));
+  FK_CK(cudaMemsetAsync(counters, 0, sizeof(int) * 256, st));
   if (ncand > 0) {
     k_screen_sorted<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(
         m.pairs, m.pcls, m.Q, m.qorder, m.qoff, m.npairs, m.Dsh, nbas, ncand, tau, prec, tau32,
@@ -547,11 +567,16 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
     if (!tmp) return set_error("fock: workspace allocation failed"), LRB_ERR_ALLOC;
     FK_CK(cub::DeviceRadixSort::SortPairs(tmp, tmpb, keys, keys2, idx, idx2, (int)nj, 0, 32, st));
     static_assert(2 * NCLASS + 1 <= 128, "class starts launch covers 128 ids");
-    k_class_starts_f<<<1, 128, 0, st>>>(keys2, (long long)nj, 2 * NCLASS, starts);
-    eng.launches++;
-    long long cls_begin[2 * NCLASS + 1];
-    FK_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * (2 * NCLASS + 1),
-                          cudaMemcpyDeviceToHost, st));
+    k_class_starts_f<<<1, 128, 0, st>>>(keys2, (long long)nj, 2 * NCLASS, 0u, starts);
+    // within a class the keys run by decreasing primitive-quartet count: the
+    // quartets with at least lp_min of them come first and go to the
+    // lane-per-primitive kernel where the class has one
+    const int lp_min = fock_lp_min();
+    k_class_starts_f<<<1, 128, 0, st>>>(keys2, (long long)nj, 2 * NCLASS,
+                                        0x100000u - (unsigned)lp_min, starts + 128);
+    eng.launches += 2;
+    long long cls_begin[256];
+    FK_CK(cudaMemcpyAsync(cls_begin, starts, sizeof(long long) * 256, cudaMemcpyDeviceToHost, st));
     FK_CK(cudaStreamSynchronize(st));
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -585,23 +610,12 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
       FK_CK(cudaMemset(eng.fock_prim, 0, 128 * sizeof(unsigned long long)));
     }
     for (int cc = 0; cc < 2 * NCLASS; ++cc) {
-      const long long b0 = cls_begin[cc], b1 = cls_begin[cc + 1];
+      long long b0 = cls_begin[cc];
+      const long long b1 = cls_begin[cc + 1];
       if (b1 <= b0) continue;
       const int c = cc % NCLASS, fi = cc < NCLASS ? 1 : 2;
       if (fi == 2) n32 += b1 - b0;
       const ClassEntry &ce = tab[c];
-      prm.order = idx2 + b0;
-      prm.njobs = (int)(b1 - b0);
-      int per_sm = 0;
-      if (ce.gen)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gen_kernel(1), GEN_THREADS, ce.smem[1]);
-      else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[fi], ERI_THREADS, ce.smem[fi]);
-      if (per_sm < 1) per_sm = 1;
-      const long long tasks = (prm.njobs + ce.slots - 1) / ce.slots;
-      long long grid = (long long)nsm * per_sm;
-      const long long needg = ce.gen ? tasks : (tasks + ERI_WARPS - 1) / ERI_WARPS;
-      if (grid > needg) grid = needg;
       ProfRecord rec{cc, nullptr, nullptr};
       if (eng.profile) {
         cudaEventCreate(&rec.start);
@@ -612,14 +626,46 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
       } else {
         fk.prim_count = nullptr;
       }
-      if (ce.gen)
-        gen_kernel(1)<<<(unsigned)grid, GEN_THREADS, ce.smem[1], st>>>(
-            prm, fk, ce.g, rys + RYS_TAB_OFFSET[ce.nr], counters + cc);
-      else
-        ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(
-            prm, fk, rys + RYS_TAB_OFFSET[ce.nr], counters + cc);
-      FK_CK(cudaGetLastError());
-      eng.launches++;
+      const long long split = std::min(std::max(cls_begin[128 + cc], b0), b1);
+      if (ce.lp[fi - 1] && split > b0) {
+        // one warp per shell quartet, one lane per primitive quartet
+        const EriKernelFn lp = ce.lp[fi - 1];
+        prm.order = idx2 + b0;
+        prm.njobs = (int)(split - b0);
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lp, ERI_THREADS, ce.lp_smem[fi - 1]);
+        if (per_sm < 1) per_sm = 1;
+        long long grid = (long long)nsm * per_sm;
+        const long long needg = (prm.njobs + ERI_WARPS - 1) / ERI_WARPS;
+        if (grid > needg) grid = needg;
+        lp<<<(unsigned)grid, ERI_THREADS, ce.lp_smem[fi - 1], st>>>(
+            prm, fk, rys + RYS_TAB_OFFSET[ce.nr], counters + 128 + cc);
+        FK_CK(cudaGetLastError());
+        eng.launches++;
+        b0 = split;
+      }
+      if (b1 > b0) {
+        prm.order = idx2 + b0;
+        prm.njobs = (int)(b1 - b0);
+        int per_sm = 0;
+        if (ce.gen)
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gen_kernel(1), GEN_THREADS, ce.smem[1]);
+        else
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ce.fn[fi], ERI_THREADS, ce.smem[fi]);
+        if (per_sm < 1) per_sm = 1;
+        const long long tasks = (prm.njobs + ce.slots - 1) / ce.slots;
+        long long grid = (long long)nsm * per_sm;
+        const long long needg = ce.gen ? tasks : (tasks + ERI_WARPS - 1) / ERI_WARPS;
+        if (grid > needg) grid = needg;
+        if (ce.gen)
+          gen_kernel(1)<<<(unsigned)grid, GEN_THREADS, ce.smem[1], st>>>(
+              prm, fk, ce.g, rys + RYS_TAB_OFFSET[ce.nr], counters + cc);
+        else
+          ce.fn[fi]<<<(unsigned)grid, ERI_THREADS, ce.smem[fi], st>>>(
+              prm, fk, rys + RYS_TAB_OFFSET[ce.nr], counters + cc);
+        FK_CK(cudaGetLastError());
+        eng.launches++;
+      }
       if (eng.profile) {
         cudaEventRecord(rec.stop, st);
         eng.prof.push_back(rec);
@@ -638,3 +684,10 @@ int fock_build(MolCtx &m, const double *dP, double *dG, double tau, cudaStream_t
 }
 
 }  // namespace lrb
+
+// Minimum primitive-quartet count of the lane-per-primitive Fock kernels;
+// kmin > 0 sets it (0x100000 or more: never), kmin <= 0 only reads it.
+LRB_API int lrb_fock_lane_min(int kmin) {
+  if (kmin > 0) lrb::g_lp_min.store(std::min(kmin, 0x100000));
+  return lrb::fock_lp_min();
+}

@@ -130,6 +130,13 @@ class MolContext:
 
 
 # --- reference python/librint/scf.py shapes (arrays in, arrays out) -------
+def fock_lane_min(kmin: int = 0) -> int:
+    """Primitive-quartet count from which the small Fock classes run one lane
+    per primitive quartet (lrb_fock_lane_min): kmin > 0 sets it for the
+    process, 1 << 20 turns those kernels off; returns the value in force."""
+    return int(B.lib().lrb_fock_lane_min(int(kmin)))
+
+
 def _p2c(m: Molecule):
     atm, bas, env = _arr(m)
     return (atm.ctypes.data_as(B.P_i), atm.size, bas.ctypes.data_as(B.P_i), bas.size,

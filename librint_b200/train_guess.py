@@ -173,6 +173,8 @@ def main(argv=None):
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "data", "guess_ch.npz"))
     ap.add_argument("--summary", default=None)
     ap.add_argument("--densities", default=None, help="cache file for the training densities")
+    ap.add_argument("--evaluate-only", action="store_true",
+                    help="load the network at --out and only run the held-out evaluation")
     a = ap.parse_args(argv)
 
     gen_conv = a.gen_conv if a.gen_conv else a.conv
@@ -182,6 +184,19 @@ def main(argv=None):
         GEN_OPTS["tau_prim"] = a.tau_prim
         SCF_OPTS["tau_prim"] = a.tau_prim
     model = PairModel.from_molecule(geometry(0))
+    if a.evaluate_only:
+        from .guess import LearnedGuess
+        test_ids = [("rings", i) for i in range(a.train, a.train + a.test)] + \
+                   [("flakes", i) for i in range(a.flakes, a.flakes + a.test_flakes)]
+        ev, rows = evaluate(LearnedGuess.load(a.out), test_ids, a.conv)
+        summary = dict(network=os.path.basename(a.out), test=a.test, test_flakes=a.test_flakes,
+                       first_test_ring=a.train, first_test_flake=a.flakes, conv=a.conv,
+                       scf_options=SCF_OPTS, heldout=ev, heldout_rows=rows[:40])
+        if a.summary:
+            with open(a.summary, "w") as fh:
+                json.dump(summary, fh, indent=1)
+        print(json.dumps({k: v for k, v in summary.items() if k != "heldout_rows"}))
+        return
     train_ids = [("rings", i) for i in range(a.train)] + [("flakes", i) for i in range(a.flakes)]
     test_ids = [("rings", i) for i in range(a.train, a.train + a.test)] + \
                [("flakes", i) for i in range(a.flakes, a.flakes + a.test_flakes)]

@@ -203,3 +203,37 @@ def test_primitive_screening_error():
     r1 = ctx.scf(conv=1e-9, guess=1, diis=8, tau=1e-13, tau_prim=1e-15)
     ctx.close()
     assert abs(r1.energy - r0.energy) < 1e-9, (r1.energy, r0.energy)
+
+
+def test_lane_per_primitive_kernels():
+    """The lane-per-primitive Fock kernels of the small classes (every such
+    quartet routed to them, bound 1) against the slot kernels (bound 1 << 20)
+    at tau = 0 (FP64, 1e-12 of max |G|), and both against the oracle's exact
+    sums of 12 shell-pair blocks of G (FP64 1e-11; FP32 within the all-FP32
+    bound of test_fp32_fock_build_error)."""
+    m = _ring()
+    ctx = scf.MolContext(m)
+    _, P = ctx.scf(conv=1e-8, guess=1, diis=8, return_density=True)
+    old = scf.fock_lane_min()
+    try:
+        res = {}
+        for kmin in (1, 1 << 20, 32):
+            assert scf.fock_lane_min(kmin) == kmin
+            res[kmin] = (ctx.fock_G_prec(P, 0)[0], ctx.fock_G_prec(P, 1)[0])
+    finally:
+        scf.fock_lane_min(old)
+    ctx.close()
+    b = m.bas.reshape(-1, 8)
+    rng = np.random.default_rng(12)
+    pairs = [(int(x), int(y)) for x, y in rng.integers(0, m.nbas, size=(12, 2))]
+    ref = oracle.fock_G_blocks(m, P, pairs)
+    off = np.concatenate([[0], np.cumsum((b[:, 1] + 1) * (b[:, 1] + 2) // 2)])
+    scale = np.abs(res[1 << 20][0]).max()
+    bscale = max(np.abs(r).max() for r in ref)
+    for kmin, (g64, g32) in res.items():
+        e64 = max(np.abs(g64[off[x]:off[x + 1], off[y]:off[y + 1]] - r).max()
+                  for (x, y), r in zip(pairs, ref))
+        e32 = np.abs(g32 - res[1 << 20][0]).max()
+        print(f"lane bound {kmin}: FP64 blocks {e64:.3e} of {bscale:.3e}, FP32 {e32:.3e} of {scale:.3e}")
+        assert e64 < 1e-11 * bscale and e32 < 4e-6 * scale
+        assert np.abs(g64 - res[1 << 20][0]).max() < 1e-12 * scale
