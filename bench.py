@@ -524,6 +524,26 @@ def fock_flops(cls, prim_quartets, quartets):
     return float(prim_quartets) * per_prim + 8.0 * nf * float(quartets)
 
 
+NCLASS_FOCK = 55        # Fock class ids: canonical class id, + 55 for the FP32 kernels
+
+
+def lane_class(c):
+    """Classes with the lane-per-primitive Fock kernel (csrc/eri_kernel.cuh
+    lp_passes): at most 27 cartesian elements, or momentum sum 4 with a bra
+    of at most (dp|."""
+    nf = ncart(c[0]) * ncart(c[1]) * ncart(c[2]) * ncart(c[3])
+    return nf <= 27 or (sum(c) == 4 and c[0] + c[1] <= 3)
+
+
+def fock_kernel_name(c, prec):
+    r = "double" if prec == 0 else "float"
+    slot = "k_eri<%d,%d,%d,%d,1,%s>" % (tuple(c) + (r,))
+    if lane_class(c):
+        return "k_fock_lp<%d,%d,%d,%d,%s> (quartets with >= 32 primitive quartets) + %s" % (
+            tuple(c) + (r, slot))
+    return slot
+
+
 def fock_measure(ctx, P, fp64_peak, builds=1):
     """Fock builds G(P) of the cluster at its converged density: FP64 and
     all-FP32 builds per second (host wall clock around lrb_fock_G_prec,
@@ -538,19 +558,19 @@ def fock_measure(ctx, P, fp64_peak, builds=1):
     for prec, name in ((0, "fp64"), (1, "fp32")):
         ctx.fock_G_prec(P, prec, tau=TAU)          # warm
         torch.cuda.synchronize()
-        L.lrb_profile_read((ctypes.c_double * 64)(), 64)
-        L.lrb_fock_class_counts((ctypes.c_longlong * 64)(), (ctypes.c_longlong * 64)(), 64)
+        L.lrb_profile_read((ctypes.c_double * 128)(), 128)
+        L.lrb_fock_class_counts((ctypes.c_longlong * 128)(), (ctypes.c_longlong * 128)(), 128)
         L.lrb_profile_enable(1)
         t0 = time.perf_counter()
         for _ in range(builds):
             _, nq, _ = ctx.fock_G_prec(P, prec, tau=TAU)
         dt = (time.perf_counter() - t0) / builds
         L.lrb_profile_enable(0)
-        ms = (ctypes.c_double * 64)()
-        L.lrb_profile_read(ms, 64)
-        qn, pn = (ctypes.c_longlong * 64)(), (ctypes.c_longlong * 64)()
-        L.lrb_fock_class_counts(qn, pn, 64)
-        off = 0 if prec == 0 else len(CLASSES)
+        ms = (ctypes.c_double * 128)()
+        L.lrb_profile_read(ms, 128)
+        qn, pn = (ctypes.c_longlong * 128)(), (ctypes.c_longlong * 128)()
+        L.lrb_fock_class_counts(qn, pn, 128)
+        off = 0 if prec == 0 else NCLASS_FOCK
         cls_rows = {}
         for c in CLASSES:
             i = class_id(c) + off
@@ -567,7 +587,7 @@ def fock_measure(ctx, P, fp64_peak, builds=1):
         if prec == 0:
             top = max(cls_rows, key=lambda k: cls_rows[k]["ms"])
             r = cls_rows[top]
-            out["roofline"] = {"bound": "fp64", "kernel": "k_eri<%s,%s,%s,%s,1,double>" % tuple(top),
+            out["roofline"] = {"bound": "fp64", "kernel": fock_kernel_name(tuple(int(x) for x in top), 0),
                                "achieved": r["tflops"], "peak": fp64_peak, "unit": "TFLOP/s",
                                "frac": r["tflops"] / fp64_peak if fp64_peak > 0 else None,
                                "kernel_ms": r["ms"], "kernel_share": r["ms"] / kern,

@@ -177,7 +177,7 @@ typedef struct {
   int max_iter;       /* reference imax */
   double conv;        /* reference conv: ||P - P_old||_F / 2 */
   int guess;          /* 0: P0 = I (reference), 1: core Hamiltonian */
-  int diis;           /* DIIS subspace (0 = plain Roothaan, as the reference) */
+  int diis;           /* DIIS subspace, at most 20 (0 = plain Roothaan, as the reference) */
   double tau;         /* quartet screening threshold */
   int mixed;          /* 1: incremental Fock builds, FP32 for small quartets */
   double fp32_until;  /* all-FP32 builds while ||dP|| is above this */

@@ -717,20 +717,27 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
 }
 
 // ---------------------------------------------------------------- lane per primitive quartet
-// Fock-mode kernel for the small classes (at most LP_MAX_ELEMENTS cartesian
-// elements: (ss|ss), (ps|ss), (ps|ps), (pp|ss), (pp|ps), (ds|ss), (ds|ps),
-// (dp|ss)) and shell quartets with at least LP_MIN_PRIM primitive quartets:
-// one warp takes one shell quartet and each lane runs whole primitive
-// quartets -- nodes, the recurrences of every (root, axis) and the block
-// products -- in its own registers, with no shared memory or warp barrier
-// per primitive quartet.  The block is summed across the lanes with
-// shuffles once per shell quartet and digested like the slot kernels do.
-constexpr int LP_MAX_ELEMENTS = 27;
+// Fock-mode kernel for the small classes and shell quartets with at least
+// LP_MIN_PRIM primitive quartets: one warp takes one shell quartet and each
+// lane runs whole primitive quartets -- nodes, the recurrences of every
+// (root, axis) and the block products -- in its own registers, with no
+// shared memory or warp barrier per primitive quartet.  The block is summed
+// across the lanes with shuffles once per shell quartet and digested like
+// the slot kernels do.  Blocks of more than LP_CHUNK elements are made in
+// passes of at most LP_CHUNK accumulators each, every pass recomputing the
+// recurrences (registers bound the accumulators).  The classes: at most 27
+// cartesian elements ((ss|ss) .. (dp|ss), one pass), and the momentum-sum-4
+// classes with a bra of at most (dp|: (pp|pp) in 3 passes, (ds|pp), (dp|ps)
+// and (ds|ds) in 2.
+constexpr int LP_CHUNK = 27;
 constexpr int LP_MIN_PRIM = 32;
 
 template <int LI, int LJ, int LK, int LL>
-constexpr bool lp_class() {
-  return ncart(LI) * ncart(LJ) * ncart(LK) * ncart(LL) <= LP_MAX_ELEMENTS;
+constexpr int lp_passes() {
+  constexpr int ne = ncart(LI) * ncart(LJ) * ncart(LK) * ncart(LL);
+  if (ne <= LP_CHUNK) return 1;
+  if (LI + LJ + LK + LL == 4 && LI + LJ <= 3) return (ne + LP_CHUNK - 1) / LP_CHUNK;
+  return 0;
 }
 
 // offset of element (i, j, k, l) in one axis' G block (vrr_hrr_unit layout)
@@ -740,26 +747,18 @@ constexpr int lp_off(int i, int j, int k, int l, int ax) {
                    : C::bra_off(i, j, ax) * C::KSZ + C::ket_off(k, l, ax);
 }
 
-// acc[e] += x y z over the canonical block, e = i + NI (j + NJ (k + NK l))
-template <class C, typename R, int E>
-__device__ __forceinline__ void lp_gout(R (&acc)[C::NBRA * C::NKET], const R (&gx)[C::GSZ],
-                                        const R (&gy)[C::GSZ], const R (&gz)[C::GSZ]) {
-  if constexpr (E < C::NBRA * C::NKET) {
+// acc[E - E0] += x y z for the elements E0 <= E < E1 of the canonical block,
+// E = i + NI (j + NJ (k + NK l))
+template <class C, typename R, int E0, int E1, int E, int NA>
+__device__ __forceinline__ void lp_gout(R (&acc)[NA], const R (&gx)[C::GSZ], const R (&gy)[C::GSZ],
+                                        const R (&gz)[C::GSZ]) {
+  if constexpr (E < E1) {
     constexpr int i = E % C::NI, j = (E / C::NI) % C::NJ, k = (E / C::NBRA) % C::NK;
     constexpr int l = E / (C::NBRA * C::NK);
     constexpr int X = lp_off<C>(i, j, k, l, 0), Y = lp_off<C>(i, j, k, l, 1);
     constexpr int Z = lp_off<C>(i, j, k, l, 2);
-    acc[E] = fma(gx[X] * gy[Y], gz[Z], acc[E]);
-    lp_gout<C, R, E + 1>(acc, gx, gy, gz);
-  }
-}
-
-// element E of the lane-summed block to shared memory by its owner lane
-template <class C, typename R, int E>
-__device__ __forceinline__ void lp_store(R *Bk, const R (&acc)[C::NBRA * C::NKET], int lane) {
-  if constexpr (E < C::NBRA * C::NKET) {
-    if ((E & 31) == lane) Bk[E] = acc[E];
-    lp_store<C, R, E + 1>(Bk, acc, lane);
+    acc[E - E0] = fma(gx[X] * gy[Y], gz[Z], acc[E - E0]);
+    lp_gout<C, R, E0, E1, E + 1, NA>(acc, gx, gy, gz);
   }
 }
 
@@ -768,17 +767,97 @@ struct LpLayout {
   using C = EriClass<LI, LJ, LK, LL, true>;
   using S = FockStage<C::NI, C::NJ, C::NK, C::NL>;
   static constexpr int NE = C::NBRA * C::NKET;
+  static constexpr int NPASS = lp_passes<LI, LJ, LK, LL>();
+  static constexpr int CH = (NE + NPASS - 1) / NPASS;   // accumulators per pass
   static constexpr int TAB = RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR];
   static constexpr int WAREA = RD_(NE * sizeof(R)) + RD_(S::SIZE * sizeof(R)) + 1;   // doubles
   static constexpr size_t SMEM = sizeof(double) * (size_t)(TAB + ERI_WARPS * WAREA);
 };
+
+// Per-quartet constants of the lane kernel.
+struct LpQuartet {
+  QuartetJob job;
+  double rA[3], rB[3], rC[3], rD[3];
+  float lthr;
+  int np;
+};
+
+// One pass: elements [PASS * CH, min(NE, (PASS + 1) * CH)) of the block,
+// summed over this lane's primitive quartets, then over the warp, into Bk.
+template <class C, class Lay, typename R, int PASS>
+__device__ __forceinline__ void lp_pass(const EriParams &prm, const FockParams &fk, const double *tab,
+                                        const LpQuartet &q, R *Bk, int lane, unsigned long long &nprim) {
+  constexpr int NE = Lay::NE, NR = C::NR, CH = Lay::CH;
+  constexpr int E0 = PASS * CH, E1 = (PASS + 1) * CH < NE ? (PASS + 1) * CH : NE;
+  const double cut = prm.expcutoff, omega = prm.omega;
+  const int reps = omega < 0.0 ? 2 : 1;
+  const QuartetJob &job = q.job;
+  R acc[CH];
+#pragma unroll
+  for (int e = 0; e < CH; ++e) acc[e] = 0;
+  for (int p = lane; p < q.np; p += 32) {
+    const int ij = p % job.nij, kl = p / job.nij;
+    const PrimPair ket = prm.pp[job.pkl_off + kl];
+    const PrimPair bra = prm.pp[job.pij_off + ij];
+    // screening (reference src/cint2e.rs:367-393), then the primitive
+    // Schwarz x density test
+    if (ket.cce > cut || bra.cce > cut - ket.cce) continue;
+    if (fk.lq && fk.lq[job.pij_off + ij] + fk.lq[job.pkl_off + kl] < q.lthr) continue;
+    const double aij = bra.a, akl = ket.a, inv = 1.0 / (aij + akl);
+    const double fac0 = sqrt(inv) * bra.facia * ket.facia;
+    const double pq[3] = {bra.px - ket.px, bra.py - ket.py, bra.pz - ket.pz};
+    const double x0 = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
+    const double theta = omega != 0.0 ? omega * omega / (omega * omega + aij * akl * inv) : 0.0;
+    if (omega < 0.0 && theta * x0 > fmin(40.0, cut - bra.cce - ket.cce)) continue;
+    if (PASS == 0) ++nprim;
+    const double pa[3] = {bra.px - q.rA[0], bra.py - q.rA[1], bra.pz - q.rA[2]};
+    const double qc[3] = {ket.px - q.rC[0], ket.py - q.rC[1], ket.pz - q.rC[2]};
+    for (int part = 0; part < reps; ++part) {
+      // range separation as in k_eri (omega = env[8])
+      const bool attenuate = omega > 0.0 || part == 1;
+      const double x = attenuate ? x0 * theta : x0;
+      const double fac1 = attenuate ? fac0 * (omega > 0.0 ? sqrt(theta) : -sqrt(theta)) : fac0;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        double u = rys_function<NR>(tab, x, r);
+        const double w = rys_function<NR>(tab, x, NR + r);
+        if (attenuate) u = u * theta / (u + 1.0 - u * theta);
+        const double d = 1.0 / (1.0 + u);
+        const double tmp5 = 0.5 * inv * u * d;
+        const double b10 = tmp5 + 0.5 * bra.ia * d;
+        const double b01 = tmp5 + 0.5 * ket.ia * d;
+        R g[3][C::GSZ];
+        R tsc[C::TSZ > 0 ? C::TSZ : 1];
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          const double cn = pa[ax] - 2.0 * tmp5 * akl * pq[ax];
+          const double cm = qc[ax] + 2.0 * tmp5 * aij * pq[ax];
+          const double v00 = ax == 2 ? w * fac1 : 1.0;
+          vrr_hrr_unit<C, R>(g[ax], tsc, (R)v00, (R)cn, (R)cm, (R)b10, (R)b01, (R)tmp5,
+                             (R)(q.rA[ax] - q.rB[ax]), (R)(q.rC[ax] - q.rD[ax]));
+        }
+        lp_gout<C, R, E0, E1, E0, CH>(acc, g[0], g[1], g[2]);
+      }
+    }
+  }
+  // sum over the lanes; lane e % 32 stores element E0 + e
+#pragma unroll
+  for (int e = 0; e < E1 - E0; ++e) {
+    R v = acc[e];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((e & 31) == lane) Bk[E0 + e] = v;
+  }
+  if constexpr (PASS + 1 < Lay::NPASS) lp_pass<C, Lay, R, PASS + 1>(prm, fk, tab, q, Bk, lane, nprim);
+}
 
 template <int LI, int LJ, int LK, int LL, typename R>
 __global__ void __launch_bounds__(ERI_THREADS)
 k_fock_lp(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *counter) {
   using Lay = LpLayout<LI, LJ, LK, LL, R>;
   using C = typename Lay::C;
-  constexpr int NE = Lay::NE, NR = C::NR;
+  constexpr int NE = Lay::NE;
+  static_assert(Lay::NPASS > 0, "not a lane-kernel class");
   extern __shared__ double smem[];
   double *tab = smem;
   for (int i = threadIdx.x; i < Lay::TAB; i += blockDim.x) tab[i] = rys_tab_n[i];
@@ -787,8 +866,6 @@ k_fock_lp(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, in
   double *wa = smem + Lay::TAB + warp * Lay::WAREA;
   R *Bk = reinterpret_cast<R *>(wa);
   R *Ps = reinterpret_cast<R *>(wa + RD_(NE * sizeof(R)));
-  const double cut = prm.expcutoff, omega = prm.omega;
-  const int reps = omega < 0.0 ? 2 : 1;
   unsigned long long nprim = 0;
   for (;;) {
     int task = 0;
@@ -797,90 +874,35 @@ k_fock_lp(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, in
     if (task >= prm.njobs) break;
     const int2 jb = fk.jobs[prm.order[task]];
     const PairInfo pb = fk.pairs[jb.x], pk = fk.pairs[jb.y];
-    QuartetJob job;
+    LpQuartet q;
+    QuartetJob &job = q.job;
     job.ish = pb.ish; job.jsh = pb.jsh; job.pij_off = pb.pp_off; job.nij = pb.npp;
     job.ksh = pk.ish; job.lsh = pk.jsh; job.pkl_off = pk.pp_off; job.nkl = pk.npp;
     job.out_off = 0; job.s_i = job.s_j = job.s_k = job.s_l = 0;
+    q.np = job.nij * job.nkl;
     double wdeg = 1.0;
     if (pb.ish == pb.jsh) wdeg *= 0.5;
     if (pk.ish == pk.jsh) wdeg *= 0.5;
     if (jb.x == jb.y) wdeg *= 0.5;
-    double rA[3], rB[3], rC[3], rD[3];
     {
       const int a = C::IB ? job.ish : job.jsh, b = C::IB ? job.jsh : job.ish;
       const int c = C::KB ? job.ksh : job.lsh, d = C::KB ? job.lsh : job.ksh;
 #pragma unroll
       for (int x = 0; x < 3; ++x) {
-        rA[x] = prm.centers[3 * a + x]; rB[x] = prm.centers[3 * b + x];
-        rC[x] = prm.centers[3 * c + x]; rD[x] = prm.centers[3 * d + x];
+        q.rA[x] = prm.centers[3 * a + x]; q.rB[x] = prm.centers[3 * b + x];
+        q.rC[x] = prm.centers[3 * c + x]; q.rD[x] = prm.centers[3 * d + x];
       }
     }
-    float lthr = 0.f;
+    q.lthr = 0.f;
     if (fk.lq) {
       const int nb = fk.nbas;
       const double *D = fk.Dsh;
       const int I = job.ish, J = job.jsh, K = job.ksh, L = job.lsh;
       const double dd = fmax(fmax(2.0 * D[I * nb + J], 2.0 * D[K * nb + L]),
                              fmax(fmax(D[I * nb + K], D[I * nb + L]), fmax(D[J * nb + K], D[J * nb + L])));
-      lthr = dd > 0.0 ? (float)log(fk.tau_prim / dd) : INFINITY;
+      q.lthr = dd > 0.0 ? (float)log(fk.tau_prim / dd) : INFINITY;
     }
-    R acc[NE];
-#pragma unroll
-    for (int e = 0; e < NE; ++e) acc[e] = 0;
-    const int np = job.nij * job.nkl;
-    for (int p = lane; p < np; p += 32) {
-      const int ij = p % job.nij, kl = p / job.nij;
-      const PrimPair ket = prm.pp[job.pkl_off + kl];
-      const PrimPair bra = prm.pp[job.pij_off + ij];
-      // screening (reference src/cint2e.rs:367-393), then the primitive
-      // Schwarz x density test
-      if (ket.cce > cut || bra.cce > cut - ket.cce) continue;
-      if (fk.lq && fk.lq[job.pij_off + ij] + fk.lq[job.pkl_off + kl] < lthr) continue;
-      const double aij = bra.a, akl = ket.a, inv = 1.0 / (aij + akl);
-      const double fac0 = sqrt(inv) * bra.facia * ket.facia;
-      const double pq[3] = {bra.px - ket.px, bra.py - ket.py, bra.pz - ket.pz};
-      const double x0 = aij * akl * inv * (pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2]);
-      const double theta = omega != 0.0 ? omega * omega / (omega * omega + aij * akl * inv) : 0.0;
-      if (omega < 0.0 && theta * x0 > fmin(40.0, cut - bra.cce - ket.cce)) continue;
-      ++nprim;
-      const double pa[3] = {bra.px - rA[0], bra.py - rA[1], bra.pz - rA[2]};
-      const double qc[3] = {ket.px - rC[0], ket.py - rC[1], ket.pz - rC[2]};
-      const double ab[3] = {rA[0] - rB[0], rA[1] - rB[1], rA[2] - rB[2]};
-      const double cd[3] = {rC[0] - rD[0], rC[1] - rD[1], rC[2] - rD[2]};
-      for (int part = 0; part < reps; ++part) {
-        // range separation as in k_eri (omega = env[8])
-        const bool attenuate = omega > 0.0 || part == 1;
-        const double x = attenuate ? x0 * theta : x0;
-        const double fac1 = attenuate ? fac0 * (omega > 0.0 ? sqrt(theta) : -sqrt(theta)) : fac0;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          double u = rys_function<NR>(tab, x, r);
-          const double w = rys_function<NR>(tab, x, NR + r);
-          if (attenuate) u = u * theta / (u + 1.0 - u * theta);
-          const double d = 1.0 / (1.0 + u);
-          const double tmp5 = 0.5 * inv * u * d;
-          const double b10 = tmp5 + 0.5 * bra.ia * d;
-          const double b01 = tmp5 + 0.5 * ket.ia * d;
-          R g[3][C::GSZ];
-          R tsc[C::TSZ > 0 ? C::TSZ : 1];
-#pragma unroll
-          for (int ax = 0; ax < 3; ++ax) {
-            const double cn = pa[ax] - 2.0 * tmp5 * akl * pq[ax];
-            const double cm = qc[ax] + 2.0 * tmp5 * aij * pq[ax];
-            const double v00 = ax == 2 ? w * fac1 : 1.0;
-            vrr_hrr_unit<C, R>(g[ax], tsc, (R)v00, (R)cn, (R)cm, (R)b10, (R)b01, (R)tmp5,
-                               (R)ab[ax], (R)cd[ax]);
-          }
-          lp_gout<C, R, 0>(acc, g[0], g[1], g[2]);
-        }
-      }
-    }
-    // sum over the lanes (every lane ends with the totals)
-#pragma unroll
-    for (int e = 0; e < NE; ++e)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], o);
-    lp_store<C, R, 0>(Bk, acc, lane);
+    lp_pass<C, Lay, R, 0>(prm, fk, tab, q, Bk, lane, nprim);
     fock_stage<C::NI, C::NJ, C::NK, C::NL, R>(Ps, job, fk, lane, 32);
     __syncwarp();
     fock_digest<C::NI, C::NJ, C::NK, C::NL, R>(Bk, Ps, job, wdeg, fk, lane, 32);

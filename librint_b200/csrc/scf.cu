@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -207,7 +209,7 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
   double *Pold = dv.alloc<double>(nn), *G = dv.alloc<double>(nn), *F = dv.alloc<double>(nn);
   double *W1 = dv.alloc<double>(nn), *W2 = dv.alloc<double>(nn), *C = dv.alloc<double>(nn);
   double *ev = dv.alloc<double>(n), *scr = dv.alloc<double>(2);
-  const int ndiis = o.diis > 0 ? std::min(o.diis, 8) : 0;
+  const int ndiis = o.diis > 0 ? std::min(o.diis, 20) : 0;
   double *Fh = ndiis ? dv.alloc<double>(nn * ndiis) : nullptr;
   double *Eh = ndiis ? dv.alloc<double>(nn * ndiis) : nullptr;
   if (!dv.ok) return set_error("scf: device allocation failed"), LRB_ERR_ALLOC;
@@ -267,6 +269,9 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
   int since_full = 1 << 30, phase = -1;
   bool fp32_done = false, fp64_final = false;
   double hist[3] = {1e300, 1e300, 1e300};   // delta of the last iterations
+  // LRB_SCF_TRACE=1: one line per iteration on stderr (phase, build kind,
+  // quartets, build time, DIIS depth, density change)
+  static const bool trace = getenv("LRB_SCF_TRACE") && atoi(getenv("LRB_SCF_TRACE")) > 0;
   while (delta > o.conv && it < o.max_iter) {
     cudaMemcpyAsync(Pold, P, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
     const auto tf = std::chrono::steady_clock::now();
@@ -300,6 +305,7 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
     k_axpby<<<gb, 256, 0, st>>>(H, G, F, 1.0, 1.0, nn);
     cudaStreamSynchronize(st);
     fock_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tf).count();
+    const double build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tf).count();
     const double *Fuse = F;
     if (ndiis) {
       // error e = F P S - S P F, stored in slot it % ndiis
@@ -334,6 +340,10 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
     if ((rc = density_from_fock(Fuse))) return rc;
     k_axpby<<<gb, 256, 0, st>>>(P, Pold, W1, 1.0, -1.0, nn);
     delta = std::sqrt(dot(W1, W1, nn, st, scr)) / 2.0;
+    if (trace)
+      fprintf(stderr, "scf it %3d phase %2d %s quartets %11lld fp32 %11lld build %8.1f ms diis %d delta %.3e\n",
+              it, o.mixed ? phase : 0, o.mixed && since_full > 0 ? "incr" : "full", fs.quartets,
+              fs.fp32_quartets, build_ms, ndiis ? std::min(nd, ndiis) : 0, delta);
     hist[2] = hist[1];
     hist[1] = hist[0];
     hist[0] = delta;
