@@ -527,18 +527,19 @@ def fock_flops(cls, prim_quartets, quartets):
 NCLASS_FOCK = 55        # Fock class ids: canonical class id, + 55 for the FP32 kernels
 
 
-def lane_class(c):
+def lane_class(c, prec):
     """Classes with the lane-per-primitive Fock kernel (csrc/eri_kernel.cuh
-    lp_passes): at most 27 cartesian elements, or momentum sum 4 with a bra
-    of at most (dp|."""
+    lp_passes): at most 27 cartesian elements, (ds|pp), (ds|ds), and (pp|pp)
+    in FP64."""
     nf = ncart(c[0]) * ncart(c[1]) * ncart(c[2]) * ncart(c[3])
-    return nf <= 27 or (sum(c) == 4 and c[0] + c[1] <= 3)
+    return nf <= 27 or tuple(c) in ((2, 0, 1, 1), (2, 0, 2, 0)) or \
+        (tuple(c) == (1, 1, 1, 1) and prec == 0)
 
 
 def fock_kernel_name(c, prec):
     r = "double" if prec == 0 else "float"
     slot = "k_eri<%d,%d,%d,%d,1,%s>" % (tuple(c) + (r,))
-    if lane_class(c):
+    if lane_class(c, prec):
         return "k_fock_lp<%d,%d,%d,%d,%s> (quartets with >= 32 primitive quartets) + %s" % (
             tuple(c) + (r, slot))
     return slot
@@ -644,11 +645,12 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True, ablations=False
                functional at its density against the oracle); with
                reference_run, or without that file, the plain run continued
                from its density to 1e-8 on this GPU;
-    learned_mixed (the chosen form): the learned guess (when its network
-               applies to this basis; the host prediction is timed in) and
-               incremental Fock builds with FP32 quartets, FP32 phases
-               screened at tau_fp32 = 1e-11, FP64 finish at 1e-13;
-    with ablations also mixed (core-H start) and learned_fp64.
+    mixed:     core-H start, incremental Fock builds with FP32 quartets
+               (FP32 phases screened at tau_fp32 = 1e-11), FP64 finish at
+               1e-13;
+    learned_mixed: the same from the learned guess (when its network
+               applies to this basis; the host prediction is timed in);
+    with ablations also learned_fp64.
     chosen = the fastest leg within 1e-6 Eh of the reference.  Times exclude
     the one-off pair table / Schwarz set-up (setup_s)."""
     import torch
@@ -701,7 +703,7 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True, ablations=False
             out["predict_ms"] = t_pred
         else:
             out["learned"] = "network does not apply to this basis"
-    if "learned_mixed" not in out and not ablations:
+    if "mixed" not in out:
         out["mixed"] = run(1e-5, mixed=1, tau_fp32=TAU_FP32)
         legs.append("mixed")
     e_ref = out["reference"]["energy"]

@@ -99,9 +99,10 @@ LRB_API int lrb_profile_read(double *ms, int n);
  * plus 55 for the FP32 kernels) the shell quartets and the primitive
  * quartets that passed screening, since the last read (which clears them). */
 LRB_API int lrb_fock_class_counts(long long *quartets, long long *prim_quartets, int n);
-/* Fock builds: shell quartets of the small classes ((ss|ss) ... (dp|ss), at
- * most 27 cartesian elements) with at least kmin primitive quartets run one
- * lane per primitive quartet instead of one slot per shell quartet.  kmin > 0
+/* Fock builds: shell quartets of the small classes (at most 27 cartesian
+ * elements, (ss|ss) ... (dp|ss); also (ds|pp), (ds|ds) and, FP64, (pp|pp))
+ * with at least kmin primitive quartets run one lane per primitive quartet
+ * instead of one slot per shell quartet.  kmin > 0
  * sets the bound for the process (default 32, or LRB_FOCK_LP_MIN; 1048576
  * disables those kernels); every call returns the bound in force. */
 LRB_API int lrb_fock_lane_min(int kmin);

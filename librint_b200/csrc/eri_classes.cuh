@@ -60,10 +60,12 @@ ClassEntry make_entry() {
   e.gen = 0;
   e.lp[0] = e.lp[1] = nullptr;
   e.lp_smem[0] = e.lp_smem[1] = 0;
-  if constexpr (lp_passes<LI, LJ, LK, LL>() > 0) {
+  if constexpr (lp_passes<LI, LJ, LK, LL, double>() > 0) {
     e.lp[0] = k_fock_lp<LI, LJ, LK, LL, double>;
-    e.lp[1] = k_fock_lp<LI, LJ, LK, LL, float>;
     e.lp_smem[0] = LpLayout<LI, LJ, LK, LL, double>::SMEM;
+  }
+  if constexpr (lp_passes<LI, LJ, LK, LL, float>() > 0) {
+    e.lp[1] = k_fock_lp<LI, LJ, LK, LL, float>;
     e.lp_smem[1] = LpLayout<LI, LJ, LK, LL, float>::SMEM;
   }
   return e;

@@ -726,17 +726,19 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
 // the slot kernels do.  Blocks of more than LP_CHUNK elements are made in
 // passes of at most LP_CHUNK accumulators each, every pass recomputing the
 // recurrences (registers bound the accumulators).  The classes: at most 27
-// cartesian elements ((ss|ss) .. (dp|ss), one pass), and the momentum-sum-4
-// classes with a bra of at most (dp|: (pp|pp) in 3 passes, (ds|pp), (dp|ps)
-// and (ds|ds) in 2.
+// cartesian elements ((ss|ss) .. (dp|ss), one pass), (ds|pp) and (ds|ds) in
+// 2 passes and, FP64 only, (pp|pp) in 3: the classes and precisions where
+// the C3 cluster's build measured faster than on the slot kernel ((pp|pp)
+// FP32 and (dp|ps) in 2 passes measured 22 % and 4-31 % slower).
 constexpr int LP_CHUNK = 27;
 constexpr int LP_MIN_PRIM = 32;
 
-template <int LI, int LJ, int LK, int LL>
+template <int LI, int LJ, int LK, int LL, typename R>
 constexpr int lp_passes() {
   constexpr int ne = ncart(LI) * ncart(LJ) * ncart(LK) * ncart(LL);
   if (ne <= LP_CHUNK) return 1;
-  if (LI + LJ + LK + LL == 4 && LI + LJ <= 3) return (ne + LP_CHUNK - 1) / LP_CHUNK;
+  if (LI == 2 && LJ == 0 && ((LK == 1 && LL == 1) || (LK == 2 && LL == 0))) return 2;
+  if (LI == 1 && LJ == 1 && LK == 1 && LL == 1 && sizeof(R) == 8) return 3;
   return 0;
 }
 
@@ -767,7 +769,7 @@ struct LpLayout {
   using C = EriClass<LI, LJ, LK, LL, true>;
   using S = FockStage<C::NI, C::NJ, C::NK, C::NL>;
   static constexpr int NE = C::NBRA * C::NKET;
-  static constexpr int NPASS = lp_passes<LI, LJ, LK, LL>();
+  static constexpr int NPASS = lp_passes<LI, LJ, LK, LL, R>();
   static constexpr int CH = (NE + NPASS - 1) / NPASS;   // accumulators per pass
   static constexpr int TAB = RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR];
   static constexpr int WAREA = RD_(NE * sizeof(R)) + RD_(S::SIZE * sizeof(R)) + 1;   // doubles

@@ -262,7 +262,8 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
   double *dPm = o.mixed ? dv.alloc<double>(nn) : nullptr;
   if (!dv.ok) return set_error("scf: device allocation failed"), LRB_ERR_ALLOC;
   // mixed schedule: phase 1 all FP32 while the density moves by more than
-  // fp32_until (left for good when it stops shrinking), phase 2 FP32 only
+  // fp32_until (left for good when it stops shrinking below 10 x
+  // fp32_until), phase 2 FP32 only
   // for quartets with bound < tau32, phase 0 all FP64 once ||dP||/2 is within
   // 10 x conv, so the last iterations and the fixed point are those of the
   // FP64 operator.  A phase change forces a full build and restarts DIIS.
@@ -279,7 +280,10 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
     if (!o.mixed) {
       if ((rc = fock_build(m, P, G, o.tau, st, &fs))) return rc;
     } else {
-      if (it >= 3 && delta > 0.5 * hist[2]) fp32_done = true;   // no progress in two steps
+      // no progress in two steps: the FP32 operator's error floor, which
+      // lies near fp32_until; far above it a stall is the iteration's own
+      // (DIIS between two basins) and FP64 builds would not end it sooner
+      if (it >= 3 && delta > 0.5 * hist[2] && delta < 10.0 * o.fp32_until) fp32_done = true;
       if (it > 0 && delta <= o.fp32_until) fp32_done = true;
       if (fp32_done && delta <= 10.0 * o.conv) fp64_final = true;
       const int want = !fp32_done ? 1 : (fp64_final ? 0 : 2);

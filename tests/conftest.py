@@ -171,7 +171,7 @@ def block_scale(m, shls, coord, values):
 
 def assert_close_block_scale(got, ref, m, shls, coord, scale_values=None, rel_block=1e-12,
                              what="", atol=ERI_ATOL, gpu_cart=None, max_arbitrated=3,
-                             rel_hard=None, exact_floor=1e-11):
+                             rel_hard=None, exact_floor=1e-11, arbitrated=None):
     """Per integral 1e-12 relative plus ``rel_block`` of the largest |value| of
     its quartet block (of ``scale_values``, default ref) plus ``atol``: the
     bar for blocks whose small elements come out of cancellation between
@@ -181,7 +181,9 @@ def assert_close_block_scale(got, ref, m, shls, coord, scale_values=None, rel_bl
     ``max_arbitrated`` quartets among them (largest difference over block
     scale; cartesian blocks from ``gpu_cart(shls)``) go to the 40-digit
     evaluation: the GPU may not be further from it than 4x the oracle's error,
-    or ``exact_floor`` of the exact block's largest element, plus 1e-15."""
+    or ``exact_floor`` of the exact block's largest element, plus 1e-15.
+    ``arbitrated`` (a set) carries the quartets already judged across calls
+    on the same quartet list (cartesian and spherical passes)."""
     import numpy as np
     got, ref = np.asarray(got), np.asarray(ref)
     scale = block_scale(m, shls, coord, ref if scale_values is None else scale_values)
@@ -210,6 +212,10 @@ def assert_close_block_scale(got, ref, m, shls, coord, scale_values=None, rel_bl
     import oracle
     from oracle import mp_exact
     for q in sorted(worst, key=lambda k: -worst[k])[:max_arbitrated]:
+        if arbitrated is not None:
+            if q in arbitrated:
+                continue
+            arbitrated.add(q)
         sh = np.ascontiguousarray(np.asarray(shls)[q:q + 1], dtype=np.int32)
         ex = np.array(mp_exact.eri_cart_exact(m.atm, m.bas, m.env, sh[0]), dtype=float).ravel()
         e_or = np.abs(oracle.int2e_batch(m, sh, 0) - ex).max()

