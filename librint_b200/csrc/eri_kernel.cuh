@@ -83,9 +83,15 @@ struct EriClass {
   static constexpr int CW = ROWKET ? BSZ : KSZ;   // column values per axis
   // after the bra shift; not needed when the ket has no shift (LD == 0)
   static constexpr int TSZ = LD > 0 ? BSZ * (NCD + 1) : 0;
+  // shared-memory strides of the per-(root, axis) G arrays and bra-shift
+  // scratch, odd so that the units' lanes, which write and read their own
+  // arrays in step, fall on distinct banks (an even stride put lanes 2k and
+  // 2k + 16 words apart on the same banks)
+  static constexpr int GST = GSZ | 1;
+  static constexpr int TST = TSZ > 0 ? (TSZ | 1) : 0;
   // shared-memory doubles of one slot (loop area or output epilogue)
   static constexpr int slot_doubles() {
-    const int loop = 3 * NR + 3 * NR * GSZ + 3 * NR * TSZ;
+    const int loop = 3 * NR + 3 * NR * GST + 3 * NR * TST;
     const int epi = 2 * NBRA * NKET;
     return loop > epi ? loop : epi;
   }
@@ -122,16 +128,18 @@ template <class C, int MODE = 0, typename R = double>
 struct EriLayout {
   static constexpr int NKO_MAX = C::NKET;   // cartesian >= spherical
   // per-slot sizes in doubles: roots, weights, 1/(1+u) (3 NR, FP64), then G
-  // (NR*3*GSZ) and per-unit bra-shift scratch (3*NR*TSZ) in the arithmetic
+  // (NR*3*GST) and per-unit bra-shift scratch (3*NR*TST) in the arithmetic
   // type R in the loop; block (NBRA*NKET, R) + ket-transformed block
   // (NBRA*NKO, output mode only) in the epilogue.  FP32 halves the R parts.
   static constexpr int RD(int n) { return (int)((n * sizeof(R) + 7) / 8); }
-  static constexpr int LOOP = 3 * C::NR + RD(C::NR * 3 * C::GSZ + C::NR * 3 * C::TSZ);
+  static constexpr int LOOP = 3 * C::NR + RD(C::NR * 3 * C::GST + C::NR * 3 * C::TST);
   // Fock mode stages the quartet's density blocks after the block
   static constexpr int EPI = RD(C::NBRA * C::NKET) +
                              (MODE == 0 ? C::NBRA * NKO_MAX
                                         : RD(FockStage<C::NI, C::NJ, C::NK, C::NL>::SIZE) + 1);
-  static constexpr int SLOT = LOOP > EPI ? LOOP : EPI;
+  // odd, so that 1-lane slots (32 per warp, each lane in its own slot) put
+  // the lanes' same-offset accesses on distinct banks
+  static constexpr int SLOT = (LOOP > EPI ? LOOP : EPI) | 1;
   static constexpr int WARP = C::SLOTS * SLOT;
   static constexpr int TAB = (RYS_TAB_OFFSET[C::NR + 1] - RYS_TAB_OFFSET[C::NR]);
   static constexpr int C2S = 3 * 5 * 6;    // l <= 2, m, cart
@@ -345,8 +353,8 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
   const int myslot = lane_live ? slot : C::SLOTS - 1;
   double *sb = wbuf + myslot * L::SLOT;        // this slot's area
   double *RW = sb;                             // [3*NR] FP64 roots, weights, 1/(1+u)
-  R *G = reinterpret_cast<R *>(sb + 3 * C::NR);            // [NR][3][GSZ]
-  R *Tsc = G + C::NR * 3 * C::GSZ;                         // [3*NR][TSZ]
+  R *G = reinterpret_cast<R *>(sb + 3 * C::NR);            // [NR][3][GST]
+  R *Tsc = G + C::NR * 3 * C::GST;                         // [3*NR][TST]
 
   // row offsets of this lane (row side indices, per axis)
   int roff[3] = {0, 0, 0};
@@ -604,7 +612,7 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
           const double cn = pa - 2.0 * tmp5 * akl * pqa;
           const double cm = qc + 2.0 * tmp5 * aij * pqa;
           const double v00 = ax == 2 ? RW[C::NR + r] * fac1 : 1.0;
-          vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GSZ, Tsc + u * C::TSZ, (R)v00, (R)cn, (R)cm,
+          vrr_hrr_unit<C, R>(G + (r * 3 + ax) * C::GST, Tsc + u * C::TST, (R)v00, (R)cn, (R)cm,
                              (R)b10, (R)b01, (R)tmp5, (R)ab, (R)cd);
         }
       }
@@ -612,8 +620,8 @@ k_eri(EriParams prm, FockParams fk, const double *__restrict__ rys_tab_n, int *c
       if (run) {
 #pragma unroll
         for (int r = 0; r < C::NR; ++r) {
-          const R *gx = G + (r * 3 + 0) * C::GSZ, *gy = G + (r * 3 + 1) * C::GSZ;
-          const R *gz = G + (r * 3 + 2) * C::GSZ;
+          const R *gx = G + (r * 3 + 0) * C::GST, *gy = G + (r * 3 + 1) * C::GST;
+          const R *gz = G + (r * 3 + 2) * C::GST;
           if (rho < C::NROWS) {
             R vx[C::CW], vy[C::CW], vz[C::CW];
 #pragma unroll

@@ -169,6 +169,18 @@ def block_scale(m, shls, coord, values):
     return np.repeat(mx, np.diff(off))
 
 
+def cart_block_scale(m, shls, coord, cart_values):
+    """Per element of the ``coord`` layout of the quartet list ``shls``, the
+    largest |value| of the same quartet's cartesian block (``cart_values``,
+    packed cartesian blocks of the same list): the magnitude the spherical
+    transform's rounding scales with."""
+    import numpy as np
+    mx = block_scale(m, shls, 0, cart_values)
+    off0 = np.concatenate([[0], np.cumsum(_block_sizes(m, shls, 0))])
+    per_q = mx[off0[:-1]] if len(off0) > 1 else mx
+    return np.repeat(per_q, _block_sizes(m, shls, coord))
+
+
 def assert_close_block_scale(got, ref, m, shls, coord, scale_values=None, rel_block=1e-12,
                              what="", atol=ERI_ATOL, gpu_cart=None, max_arbitrated=3,
                              rel_hard=None, exact_floor=1e-11, arbitrated=None):

@@ -116,3 +116,24 @@ def test_errors_are_reported_not_fatal():
         eri.int2e_batch(m3, shls[:1], 0)
     # the library still works afterwards
     assert_eri_close(eri.int2e_batch(m, shls), oracle.int2e_batch(m, shls, 1))
+
+
+@pytest.mark.skipif(__import__("torch").cuda.device_count() < 2, reason="needs two GPUs")
+def test_second_device_same_results():
+    """Kernel tables, cart->sph coefficients and shared-memory limits are set
+    up per device: spherical (dd|dd) blocks (> 48 KB of shared memory) and a
+    Fock build on device 1 equal those of device 0 in the same process."""
+    import torch
+    from librint_b200 import scf
+    m, shls = synthetic.eri_sweep((2, 2, 2, 2), 64, seed=5)
+    mw = synthetic.water_like()
+    P = np.eye(mw.nao(0))
+    out = []
+    for dev in (0, 1):
+        torch.cuda.set_device(dev)
+        ctx = scf.MolContext(mw)
+        out.append((eri.int2e_batch(m, shls, 1), ctx.fock_G(P, 0.0)))
+        ctx.close()
+    torch.cuda.set_device(0)
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-13, atol=1e-14)
