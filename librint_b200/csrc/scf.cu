@@ -266,7 +266,8 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
   // fp32_until), phase 2 FP32 only
   // for quartets with bound < tau32, phase 0 all FP64 once ||dP||/2 is within
   // 10 x conv, so the last iterations and the fixed point are those of the
-  // FP64 operator.  A phase change forces a full build and restarts DIIS.
+  // FP64 operator.  A phase change forces a full build; leaving phase 1
+  // restarts DIIS.
   int since_full = 1 << 30, phase = -1;
   bool fp32_done = false, fp64_final = false;
   double hist[3] = {1e300, 1e300, 1e300};   // delta of the last iterations
@@ -288,7 +289,10 @@ int scf_run(MolCtx &m, size_t nelec, const ScfOptions &o, ScfResult *res, double
       if (fp32_done && delta <= 10.0 * o.conv) fp64_final = true;
       const int want = !fp32_done ? 1 : (fp64_final ? 0 : 2);
       const bool full = want != phase || since_full >= o.rebuild_every;
-      if (want != phase && phase >= 0) nd = 0;   // DIIS restarts with the new operator
+      // DIIS restarts when the all-FP32 phase ends: its Fock matrices carry
+      // the FP32 error.  The split phase differs from FP64 only in quartets
+      // below tau32, so its history stays valid for the FP64 phase.
+      if (want != phase && phase == 1) nd = 0;
       // the FP32 phases screen at tau_fp32: their G carries the FP32 error
       // already, and the FP64 phase starts with a full build at tau
       const double tau_b = want == 0 ? o.tau : std::max(o.tau, o.tau_fp32);
