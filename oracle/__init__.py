@@ -35,6 +35,7 @@ def lib():
             build()
         L = ctypes.CDLL(path)
         L.orc_rys_roots.argtypes = (_i, _d, _pd, _pd)
+        L.orc_set_rys_mode.argtypes = (_i,)
         L.orc_int2e_cart.argtypes = (_pd, _pi, _pi, _i, _pi, _i, _pd)
         L.orc_int2e_cart.restype = _i
         L.orc_int2e_sph.argtypes = (_pd, _pi, _pi, _i, _pi, _i, _pd)
@@ -77,6 +78,22 @@ def rys_roots(n: int, x: float):
     w = np.zeros(n)
     lib().orc_rys_roots(n, float(x), _p(u, _pd), _p(w, _pd))
     return u, w
+
+
+class independent_roots:
+    """Context manager: inside it every Rys rule of the oracle is computed in
+    binary128 from the Rys measure itself (orc_set_rys_mode(1): Gauss-
+    Legendre discretisation, Stieltjes procedure, Sturm bisection) instead of
+    read from the node tables that the CUDA kernels share; about 1 ms per
+    rule, for small checks only."""
+
+    def __enter__(self):
+        lib().orc_set_rys_mode(1)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_rys_mode(0)
+        return False
 
 
 def nao(m, coord=0) -> int:

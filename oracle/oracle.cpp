@@ -2,7 +2,10 @@
 // only -- see oracle.h).  Citations are paths inside the reference project.
 #include "oracle.h"
 
+#include <quadmath.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -45,10 +48,117 @@ struct CartComp {
 };
 
 // ---------------------------------------------------------------- Rys roots
-// Node/weight tables from librint_b200/csrc/gen_rys_tables.py (own fits to
-// exact 60-digit rules); same u = t^2/(1-t^2) convention as CINTrys_roots
-// (src/rys_roots.rs:3036-3158).
+// Two sources of the n-point Rys rule, selected by orc_set_rys_mode:
+//   0 (default): the node/weight tables of librint_b200/csrc/rys_tables.h
+//     (generated by librint_b200/csrc/gen_rys_tables.py, own fits to exact
+//     60-digit rules) -- the tables the CUDA kernels read;
+//   1: the rule computed here in binary128 from the measure itself, sharing
+//     no table, generator or algorithm with the kernels (rys_rule_q below).
+// Both return nodes u = t^2/(1-t^2) and weights summing to F_0(x), the
+// convention of CINTrys_roots (src/rys_roots.rs:3036-3158).
+std::atomic<int> g_rys_mode{0};
+
+using f128 = __float128;
+
+// 128-point Gauss-Legendre rule on [0, 1] in binary128 (Newton on the
+// Legendre recurrence), built once.
+constexpr int GL_M = 128;
+struct GaussLegendre {
+  f128 t[GL_M], w[GL_M];
+  GaussLegendre() {
+    for (int i = 0; i < GL_M; ++i) {
+      f128 z = cosq(M_PIq * (i + 0.75Q) / (GL_M + 0.5Q)), dp = 0;
+      for (int it = 0; it < 100; ++it) {
+        f128 p0 = 1, p1 = z;
+        for (int k = 2; k <= GL_M; ++k) {
+          const f128 p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+          p0 = p1;
+          p1 = p2;
+        }
+        dp = GL_M * (z * p1 - p0) / (z * z - 1);
+        const f128 dz = p1 / dp;
+        z -= dz;
+        if (fabsq(dz) <= 1e-33Q * fabsq(z)) break;
+      }
+      t[i] = (1 - z) / 2;                                  // [-1, 1] -> [0, 1]
+      w[i] = 1 / ((1 - z * z) * dp * dp);                  // 2 / (...) / 2
+    }
+  }
+};
+
+// n-point Gauss rule of dmu(s) = e^{-x s} s^{-1/2} / 2 ds on [0, 1] (the Rys
+// measure in s = t^2; its moments are the Boys functions F_m(x)):
+//  * the measure in t, e^{-x t^2} dt on [0, T], T = min(1, 12 / sqrt(x))
+//    (beyond T the density is below e^{-144} of its peak), is discretised by
+//    the Gauss-Legendre rule scaled to [0, T];
+//  * the Stieltjes procedure gives the recurrence coefficients alpha_k,
+//    beta_k of the monic polynomials in s orthogonal under that measure;
+//  * the nodes are the eigenvalues of the Jacobi matrix, found by bisection
+//    on its Sturm sequence (LDL^T negative counts), and the weights are the
+//    Christoffel numbers 1 / sum_k pi_k(s_i)^2 / h_k.
+void rys_rule_q(int n, double xd, double *u, double *w) {
+  static const GaussLegendre gl;
+  const f128 x = xd;
+  const f128 T = x > 144 ? 12 / sqrtq(x) : f128(1);
+  f128 s[GL_M], W[GL_M], p0[GL_M], p1[GL_M];
+  for (int j = 0; j < GL_M; ++j) {
+    const f128 t = T * gl.t[j];
+    s[j] = t * t;
+    W[j] = T * gl.w[j] * expq(-x * s[j]);
+    p0[j] = 0;
+    p1[j] = 1;
+  }
+  f128 alpha[10], beta[10], h[10];
+  for (int k = 0; k < n; ++k) {
+    f128 num = 0, den = 0;
+    for (int j = 0; j < GL_M; ++j) {
+      const f128 q = W[j] * p1[j] * p1[j];
+      den += q;
+      num += q * s[j];
+    }
+    h[k] = den;
+    alpha[k] = num / den;
+    beta[k] = k == 0 ? den : den / h[k - 1];
+    if (k + 1 < n)
+      for (int j = 0; j < GL_M; ++j) {
+        const f128 p2 = (s[j] - alpha[k]) * p1[j] - (k == 0 ? f128(0) : beta[k]) * p0[j];
+        p0[j] = p1[j];
+        p1[j] = p2;
+      }
+  }
+  // eigenvalues below lam: negative pivots of J - lam I
+  auto below = [&](f128 lam) {
+    int c = 0;
+    f128 d = alpha[0] - lam;
+    if (d < 0) ++c;
+    for (int k = 1; k < n; ++k) {
+      if (d == 0) d = 1e-4900Q;
+      d = alpha[k] - lam - beta[k] / d;
+      if (d < 0) ++c;
+    }
+    return c;
+  };
+  for (int i = 0; i < n; ++i) {
+    f128 lo = 0, hi = T * T;
+    for (int it = 0; it < 400 && hi - lo > 1e-34Q * hi; ++it) {
+      const f128 mid = (lo + hi) / 2;
+      if (below(mid) > i) hi = mid; else lo = mid;
+    }
+    const f128 si = (lo + hi) / 2;
+    f128 a = 0, b = 1, sum = b * b / h[0];
+    for (int k = 0; k + 1 < n; ++k) {
+      const f128 c = (si - alpha[k]) * b - (k == 0 ? f128(0) : beta[k]) * a;
+      a = b;
+      b = c;
+      sum += b * b / h[k + 1];
+    }
+    u[i] = (double)(si / (1 - si));
+    w[i] = (double)(1 / sum);
+  }
+}
+
 void rys_roots(int n, double x, double *u, double *w) {
+  if (g_rys_mode.load(std::memory_order_relaxed)) return rys_rule_q(n, x, u, w);
   const double xbreak = 43.0 + 5.0 * n;
   if (x >= xbreak) {
     const int off = n * (n - 1) / 2;
@@ -610,7 +720,7 @@ void int1e_block(double *out, int typec, const Shell &a, const Shell &b,
 // 2-index cart -> sph for a 1e block (i fastest)
 void cart2sph_2(double *sph, const double *cart, const Shell &a, const Shell &b) {
   const int nca = ncart(a.l), ncb = ncart(b.l), nsa = nsph(a.l), nsb = nsph(b.l);
-  const int Na = nca * a.nctr, Nb = ncb * b.nctr, Sa = nsa * a.nctr, Sb = nsb * b.nctr;
+  const int Na = nca * a.nctr, Nb = ncb * b.nctr, Sa = nsa * a.nctr;
   const std::vector<double> &A = sph_table().c[a.l], &B = sph_table().c[b.l];
   std::vector<double> tmp((size_t)Sa * Nb, 0.0);
   for (int j = 0; j < Nb; ++j)
@@ -709,6 +819,7 @@ double nuclear_repulsion(const int *atm, int natm, const double *env) {
 extern "C" {
 
 void orc_rys_roots(int n, double x, double *u, double *w) { rys_roots(n, x, u, w); }
+void orc_set_rys_mode(int mode) { g_rys_mode.store(mode ? 1 : 0); }
 
 int orc_nao(int coord, const int *bas, int nbas) {
   int n = 0;

@@ -23,6 +23,10 @@ extern "C" {
 
 /* Rys nodes u = t^2/(1-t^2) and weights for nroots n (1..9) at x. */
 void orc_rys_roots(int n, double x, double *u, double *w);
+/* Source of every Rys rule the oracle uses from now on: 0 (default) the
+ * tables the CUDA kernels also read, 1 a binary128 Gauss rule computed from
+ * the measure (no shared table or generator; about 1 ms per rule). */
+void orc_set_rys_mode(int mode);
 
 /* One shell quartet, libcint layout out[i + ni*(j + nj*(k + nk*l))].
  * Returns 1 if any primitive quartet survived screening, else 0 (out zeroed).

@@ -257,3 +257,73 @@ def test_short_range_high_order_vs_exact(golden, omega):
         ex = np.asarray(mp_exact.eri_cart_exact(m.atm, m.bas, m.env, shls)).reshape(
             got.shape[::-1]).transpose(3, 2, 1, 0)
         assert_eri_close(got, ex, what=f"omega {omega} {shls}")
+
+
+def _boys(m, x):
+    """F_m(x) = int_0^1 t^2m e^{-x t^2} dt at the current mpmath precision."""
+    from mpmath import gammainc, mpf
+    x = mpf(x)
+    if x == 0:
+        return mpf(1) / (2 * m + 1)
+    h = m + mpf(1) / 2
+    return gammainc(h, 0, x) / (2 * x ** h)
+
+
+def test_independent_rys_rule_reproduces_boys_moments():
+    """The oracle's binary128 Rys rule (computed from the measure, no node
+    tables) integrates s^k exactly: sum_i w_i s_i^k = F_k(x) for k < 2n, with
+    F_k from mpmath's incomplete gamma function at 40 digits; all terms are
+    positive, so the only error is the rounding of nodes and weights."""
+    from mpmath import mp, mpf
+    mp.dps = 40
+    with oracle.independent_roots():
+        for n in range(1, 10):
+            for x in (0.0, 1e-8, 0.7, 5.0, 23.0, 60.0, 43.0 + 5 * n + 0.5, 400.0, 2e4):
+                u, w = oracle.rys_roots(n, x)
+                s = [mpf(float(v)) / (1 + mpf(float(v))) for v in u]
+                for k in range(2 * n):
+                    got = sum(mpf(float(wi)) * si ** k for wi, si in zip(w, s))
+                    ref = _boys(k, x)
+                    assert abs(got - ref) <= 2e-14 * ref, (n, x, k, float(got / ref - 1))
+
+
+def test_node_tables_vs_independent_rule():
+    """Every segment of the node/weight tables that the CUDA kernels and, by
+    default, the oracle read (edges, midpoints, random points) and the
+    large-x limit used from 43 + 5n, against the independent binary128 rule:
+    4e-15 relative for every node and weight."""
+    rng = np.random.default_rng(11)
+    for n in range(1, 10):
+        xb = 43.0 + 5 * n
+        edges = np.arange(0.0, xb, 4.0)
+        xs = np.concatenate([edges, edges + 1e-9, edges + 2.0, np.minimum(edges + 4.0, xb) - 1e-9,
+                             [xb, xb + 3.0, 1e3, 1e6], rng.uniform(0.0, xb + 20.0, 10)])
+        for x in xs:
+            u0, w0 = oracle.rys_roots(n, x)
+            with oracle.independent_roots():
+                u1, w1 = oracle.rys_roots(n, x)
+            np.testing.assert_allclose(u0, u1, rtol=4e-15, err_msg=f"nodes n={n} x={x}")
+            np.testing.assert_allclose(w0, w1, rtol=4e-15, err_msg=f"weights n={n} x={x}")
+
+
+def test_oracle_eris_independent_of_node_tables():
+    """The oracle's ERIs with the independent binary128 Rys rules equal its
+    ERIs from the node tables that the CUDA kernels also read, so the GPU's
+    parity against the oracle does not rest on those tables: 3 quartets of
+    every class up to (dd|dd), cartesian and spherical, per element within
+    1e-12 relative + 1e-13 of the block's largest element; 1 quartet of every
+    class with an f shell, cartesian, within 2e-11 of the block's largest
+    element (high-l recurrences amplify the last-digit differences of the
+    rules by cancellation, as in the f-class parity tests)."""
+    from librint_b200 import synthetic
+    for cls in synthetic.canonical_classes(3):
+        f = max(cls) == 3
+        m, sh = synthetic.eri_sweep(cls, 1 if f else 3, seed=21, kmax=2, cube_ang=3.0, elo=0.1,
+                                    ehi=100.0)
+        for coord in ((0,) if f else (0, 1)):
+            a = oracle.int2e_batch(m, sh, coord)
+            with oracle.independent_roots():
+                b = oracle.int2e_batch(m, sh, coord)
+            scale = np.abs(a).max()
+            bound = (2e-11 * scale) if f else (1e-12 * np.abs(a) + 1e-13 * scale)
+            assert (np.abs(a - b) <= bound).all(), (cls, coord, float(np.abs(a - b).max() / max(scale, 1e-300)))
