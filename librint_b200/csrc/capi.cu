@@ -3,10 +3,14 @@
 // there is no CPU fallback.
 #include <cuda_runtime.h>
 
+#include <sched.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "engine.h"
@@ -88,6 +92,44 @@ int check_common(const int *atm, int natm, const int *bas, int nbas, const doubl
   return LRB_OK;
 }
 
+// Host threads this process may run on (its CPU affinity), at least 1.
+int host_threads() {
+  cpu_set_t set;
+  if (sched_getaffinity(0, sizeof set, &set) == 0) return std::max(1, CPU_COUNT(&set));
+  return std::max(1u, std::thread::hardware_concurrency());
+}
+
+// fn(begin, end) over contiguous parts of [0, n), each of at least `grain`
+// items, on up to 32 host threads (the caller's thread takes the first
+// part); one part when n <= grain.  A thread that cannot be started runs its
+// part on the caller's thread.
+template <class F>
+void host_parallel(long long n, long long grain, F &&fn) {
+  if (n <= 0) return;
+  const long long nt = std::min<long long>({(long long)host_threads(), 32, (n + grain - 1) / grain});
+  if (nt <= 1) {
+    fn(0LL, n);
+    return;
+  }
+  const long long per = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  th.reserve((size_t)nt);
+  for (long long t = 1; t < nt; ++t) {
+    const long long b = t * per, e = std::min(n, b + per);
+    if (b >= e) break;
+    try {
+      th.emplace_back([&fn, b, e] { fn(b, e); });
+    } catch (...) {
+      fn(b, e);
+    }
+  }
+  fn(0LL, std::min(n, per));
+  for (std::thread &x : th) x.join();
+}
+
+// Items per host thread below which a loop stays on one thread.
+constexpr long long HOST_GRAIN = 1 << 16;
+
 // Dense symmetric tensor from canonical quartet blocks.
 __global__ void k_scatter8(const double *__restrict__ blocks, const long long *__restrict__ boff,
                            const int *__restrict__ quart, const int *__restrict__ aooff,
@@ -143,10 +185,14 @@ int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq
                           (cudaStream_t)stream, nullptr);
 }
 
-// Host buffers in and out.  The quartets run in chunks on two alternating
-// non-blocking streams: chunk c's output copy to the host overlaps chunk
-// c+1's preparation and kernels.  A chunk starts only after the previous
-// chunk's kernels (event), because both share the engine's workspace.
+// Host buffers in and out.  The quartets run in chunks through three
+// non-blocking streams: copies in (the chunk's quartet list, and in the
+// streamed layout its part of the molecule), kernels, copies out.  Chunk c
+// uses device slot c % 2 for its quartet list and output, so chunk c+1's
+// copy in and chunk c-1's copy out overlap chunk c's kernels; events hand
+// each slot on (copy in -> kernels -> copy out -> the copy in two chunks
+// later).  The kernels of all chunks share the engine's workspace and run in
+// order on the one kernel stream.
 // Shells, atoms and env entries (half-open ranges) that one chunk's quartets
 // can reach: every shell between the lowest and highest index it names,
 // their atoms, and the env entries of those shells and atoms.
@@ -157,14 +203,16 @@ struct ChunkRange {
 
 // Ranges of every chunk; false (upload everything up front) unless they are
 // valid and each chunk's ranges lie after the previous chunk's, so a chunk can
-// upload its own part of the molecule while earlier chunks compute.
+// upload its own part of the molecule while earlier chunks compute.  The
+// chunks' ranges are found in parallel, then checked in order.
 static bool chunk_ranges(const int *shls, const std::vector<long long> &qb, const int *atm,
                          int natm, const int *bas, int nbas, long long nenv, long long head,
                          std::vector<ChunkRange> &rg) {
   const int nchunk = (int)qb.size() - 1;
   if (nchunk < 2) return false;
-  rg.resize(nchunk);
-  for (int c = 0; c < nchunk; ++c) {
+  rg.assign(nchunk, ChunkRange{0, 0, 0, 0, 0, 0});
+  std::vector<char> valid(nchunk, 0);
+  auto one = [&](int c) {
     ChunkRange r{nbas, -1, natm, -1, nenv, -1};
     for (long long q = 4 * qb[c]; q < 4 * qb[c + 1]; ++q) {
       r.s0 = std::min(r.s0, shls[q]);
@@ -174,7 +222,7 @@ static bool chunk_ranges(const int *shls, const std::vector<long long> &qb, cons
       const int *b = bas + 8 * sh;
       if (b[0] < 0 || b[0] >= natm || b[2] < 1 || b[3] < 1 || b[5] < 0 || b[6] < 0 ||
           (long long)b[5] + b[2] > nenv || (long long)b[6] + (long long)b[2] * b[3] > nenv)
-        return false;
+        return;
       r.a0 = std::min(r.a0, b[0]);
       r.a1 = std::max(r.a1, b[0] + 1);
       r.e0 = std::min({r.e0, (long long)b[5], (long long)b[6]});
@@ -182,14 +230,22 @@ static bool chunk_ranges(const int *shls, const std::vector<long long> &qb, cons
     }
     for (int a = r.a0; a < r.a1; ++a) {
       const long long pc = atm[6 * a + 1];
-      if (pc < 0 || pc + 3 > nenv) return false;
+      if (pc < 0 || pc + 3 > nenv) return;
       r.e0 = std::min(r.e0, pc);
       r.e1 = std::max(r.e1, pc + 3);
     }
+    rg[c] = r;
+    valid[c] = 1;
+  };
+  host_parallel(nchunk, 1, [&](long long b, long long e) {
+    for (long long c = b; c < e; ++c) one((int)c);
+  });
+  for (int c = 0; c < nchunk; ++c) {
+    if (!valid[c]) return false;
+    const ChunkRange &r = rg[c];
     const ChunkRange *prev = c > 0 ? &rg[c - 1] : nullptr;
     if (r.e0 < head || (prev && (r.s0 < prev->s1 || r.a0 < prev->a1 || r.e0 < prev->e1)))
       return false;
-    rg[c] = r;
   }
   return true;
 }
@@ -199,16 +255,26 @@ static int batch_host(double *out, int coord, const int *shls, long long nq, con
                       int gc_screen) {
   int rc = LRB_OK;
   // chunk boundaries: at most CHUNK_Q quartets and about CHUNK_OUT doubles each
-  constexpr long long CHUNK_Q = 1 << 17, CHUNK_OUT = 1 << 25;
+  constexpr long long CHUNK_Q = 1 << 18, CHUNK_OUT = 1 << 25;
+  std::vector<long long> blen((size_t)nq);
+  host_parallel(nq, HOST_GRAIN, [&](long long b, long long e) {
+    for (long long q = b; q < e; ++q) {
+      long long d = 1;
+      for (int a = 0; a < 4; ++a) d *= shell_dim(coord, bas, shls[4 * q + a]);
+      blen[(size_t)q] = d;
+    }
+  });
   std::vector<long long> qb{0}, ob{0};
+  long long max_q = 0, max_len = 1;
   {
     long long cq = 0, co = 0, tot = 0;
     for (long long q = 0; q < nq; ++q) {
-      long long b = 1;
-      for (int a = 0; a < 4; ++a) b *= shell_dim(coord, bas, shls[4 * q + a]);
+      const long long b = blen[(size_t)q];
       if (cq > 0 && (cq == CHUNK_Q || co + b > CHUNK_OUT)) {
         qb.push_back(q);
         ob.push_back(tot);
+        max_q = std::max(max_q, cq);
+        max_len = std::max(max_len, co);
         cq = co = 0;
       }
       ++cq;
@@ -217,86 +283,98 @@ static int batch_host(double *out, int coord, const int *shls, long long nq, con
     }
     qb.push_back(nq);
     ob.push_back(tot);
+    max_q = std::max(max_q, cq);
+    max_len = std::max(max_len, co);
   }
-  Engine &eng = engine();
-  for (int i = 0; i < 2; ++i) {
-    if (!eng.pipe[i] && cudaStreamCreateWithFlags(&eng.pipe[i], cudaStreamNonBlocking) != cudaSuccess)
-      return set_error("stream creation failed"), LRB_ERR_CUDA;
-    if (!eng.done[i] && cudaEventCreateWithFlags(&eng.done[i], cudaEventDisableTiming) != cudaSuccess)
-      return set_error("event creation failed"), LRB_ERR_CUDA;
-  }
+  const int nchunk = (int)qb.size() - 1;
   // env[0..head) holds the settings every chunk reads (cutoff, omega)
   const long long head = std::min(nenv, 20LL);
   std::vector<ChunkRange> rg;
   const bool streamed = chunk_ranges(shls, qb, atm, natm, bas, nbas, nenv, head, rg);
+
+  Engine &eng = engine();
+  for (int i = 0; i < 3; ++i)
+    if (!eng.pipe[i] && cudaStreamCreateWithFlags(&eng.pipe[i], cudaStreamNonBlocking) != cudaSuccess)
+      return set_error("stream creation failed"), LRB_ERR_CUDA;
+  for (int i = 0; i < 2; ++i)
+    for (cudaEvent_t *ev : {&eng.ev_in[i], &eng.ev_cmp[i], &eng.ev_out[i]})
+      if (!*ev && cudaEventCreateWithFlags(ev, cudaEventDisableTiming) != cudaSuccess)
+        return set_error("event creation failed"), LRB_ERR_CUDA;
+  cudaStream_t s_in = eng.pipe[0], s_k = eng.pipe[1], s_out = eng.pipe[2];
+  // every device buffer of the call is allocated on the kernel stream before
+  // the synchronisation below, so all three streams may use it afterwards
   DevMol m;
-  double *cen = (double *)eng.pipe_centers.get(eng.pipe[0], sizeof(double) * 3 * (size_t)nbas + 256);
-  if (!cen) rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
+  double *cen = (double *)eng.pipe_centers.get(s_k, sizeof(double) * 3 * (size_t)nbas + 256);
+  bool got = cen != nullptr;
+  for (int X = 0; X < std::min(nchunk, 2); ++X)
+    got = got && eng.pipe_in[X].get(s_k, sizeof(int) * 4 * (size_t)max_q) &&
+          eng.pipe_out[X].get(s_k, sizeof(double) * (size_t)max_len);
+  if (!got) return set_error("device allocation failed"), LRB_ERR_ALLOC;
   int *d_err = reinterpret_cast<int *>(cen + 3 * (size_t)nbas);
-  if (!rc && !streamed) {
-    // the whole molecule, and shell centres once per call (chunk 0's kernels,
-    // and through its event every later chunk, are ordered after them)
-    rc = m.upload(eng.pipe[0], atm, natm, bas, nbas, env, nenv);
-    if (!rc) rc = eri_centers(m.atm, natm, m.bas, nbas, m.env, nenv, cen, d_err, eng.pipe[0]);
-  } else if (!rc) {
+  if (!streamed) {
+    // the whole molecule, and shell centres once per call (synchronises s_k)
+    rc = m.upload(s_k, atm, natm, bas, nbas, env, nenv);
+    if (!rc) rc = eri_centers(m.atm, natm, m.bas, nbas, m.env, nenv, cen, d_err, s_k);
+  } else {
     // device arrays of full size; each chunk fills its own ranges
-    rc = m.alloc(eng.pipe[0], natm, nbas, nenv);
-    if (!rc && (cudaMemcpyAsync(m.env, env, sizeof(double) * head, cudaMemcpyHostToDevice,
-                                eng.pipe[0]) != cudaSuccess ||
-                cudaStreamSynchronize(eng.pipe[0]) != cudaSuccess))
+    rc = m.alloc(s_k, natm, nbas, nenv);
+    if (!rc && (cudaMemcpyAsync(m.env, env, sizeof(double) * head, cudaMemcpyHostToDevice, s_k) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s_k) != cudaSuccess))
       rc = (set_error("copy failed"), LRB_ERR_CUDA);
   }
-  const int nchunk = (int)qb.size() - 1;
   for (int c = 0; c < nchunk && !rc; ++c) {
     const int X = c & 1;
-    cudaStream_t st = eng.pipe[X];
     const long long nqc = qb[c + 1] - qb[c], len = ob[c + 1] - ob[c];
-    int *d_sh = (int *)eng.pipe_in[X].get(st, sizeof(int) * 4 * (size_t)nqc);
-    double *d_o = (double *)eng.pipe_out[X].get(st, sizeof(double) * (size_t)std::max(len, 1LL));
-    if (!d_sh || !d_o) {
-      rc = (set_error("device allocation failed"), LRB_ERR_ALLOC);
-      break;
-    }
-    // this chunk's inputs go up before it waits for the previous chunk, so
-    // they overlap that chunk's kernels
-    bool ok = cudaMemcpyAsync(d_sh, shls + 4 * qb[c], sizeof(int) * 4 * (size_t)nqc,
-                              cudaMemcpyHostToDevice, st) == cudaSuccess;
+    int *d_sh = (int *)eng.pipe_in[X].ptr;
+    double *d_o = (double *)eng.pipe_out[X].ptr;
+    // copy in: slot X's quartet list is free once chunk c-2's kernels ran
+    bool ok = c < 2 || cudaStreamWaitEvent(s_in, eng.ev_cmp[X], 0) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(d_sh, shls + 4 * qb[c], sizeof(int) * 4 * (size_t)nqc,
+                               cudaMemcpyHostToDevice, s_in) == cudaSuccess;
     if (streamed) {
       const ChunkRange &r = rg[c];
       ok = ok && cudaMemcpyAsync(m.bas + 8 * (size_t)r.s0, bas + 8 * (size_t)r.s0,
                                  sizeof(int) * 8 * (size_t)(r.s1 - r.s0), cudaMemcpyHostToDevice,
-                                 st) == cudaSuccess;
+                                 s_in) == cudaSuccess;
       ok = ok && cudaMemcpyAsync(m.atm + 6 * (size_t)r.a0, atm + 6 * (size_t)r.a0,
                                  sizeof(int) * 6 * (size_t)(r.a1 - r.a0), cudaMemcpyHostToDevice,
-                                 st) == cudaSuccess;
+                                 s_in) == cudaSuccess;
       ok = ok && cudaMemcpyAsync(m.env + r.e0, env + r.e0, sizeof(double) * (size_t)(r.e1 - r.e0),
-                                 cudaMemcpyHostToDevice, st) == cudaSuccess;
+                                 cudaMemcpyHostToDevice, s_in) == cudaSuccess;
     }
+    ok = ok && cudaEventRecord(eng.ev_in[X], s_in) == cudaSuccess;
+    // kernels: after this chunk's copy in, and after chunk c-2's output left slot X
+    ok = ok && cudaStreamWaitEvent(s_k, eng.ev_in[X], 0) == cudaSuccess;
+    ok = ok && (c < 2 || cudaStreamWaitEvent(s_k, eng.ev_out[X], 0) == cudaSuccess);
     if (!ok) {
       rc = (set_error("copy failed"), LRB_ERR_CUDA);
       break;
     }
-    if (c > 0 && cudaStreamWaitEvent(st, eng.done[1 - X], 0) != cudaSuccess) {
-      rc = (set_error("stream wait failed"), LRB_ERR_CUDA);
-      break;
-    }
     if (streamed)
       eri_centers_async(m.atm, natm, m.bas + 8 * (size_t)rg[c].s0, rg[c].s1 - rg[c].s0, m.env,
-                        nenv, cen + 3 * (size_t)rg[c].s0, d_err, st);
-    rc = eri_batch_device(eng, d_o, coord, d_sh, nqc, m.atm, natm, m.bas, nbas, m.env, nenv, st,
+                        nenv, cen + 3 * (size_t)rg[c].s0, d_err, s_k);
+    rc = eri_batch_device(eng, d_o, coord, d_sh, nqc, m.atm, natm, m.bas, nbas, m.env, nenv, s_k,
                           nullptr, cen, gc_screen);
     if (rc) break;
-    if (cudaEventRecord(eng.done[X], st) != cudaSuccess ||
+    // copy out, after the chunk's kernels
+    if (cudaEventRecord(eng.ev_cmp[X], s_k) != cudaSuccess ||
+        cudaStreamWaitEvent(s_out, eng.ev_cmp[X], 0) != cudaSuccess ||
         cudaMemcpyAsync(out + ob[c], d_o, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost,
-                        st) != cudaSuccess)
+                        s_out) != cudaSuccess ||
+        cudaEventRecord(eng.ev_out[X], s_out) != cudaSuccess)
       rc = (set_error("copy failed"), LRB_ERR_CUDA);
   }
-  const cudaError_t e0 = cudaStreamSynchronize(eng.pipe[0]);
-  const cudaError_t e1 = cudaStreamSynchronize(eng.pipe[1]);
-  m.release(eng.pipe[0]);
-  const cudaError_t e2 = cudaStreamSynchronize(eng.pipe[0]);
-  if (!rc && (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess)) {
-    set_error(cudaGetErrorString(e0 != cudaSuccess ? e0 : (e1 != cudaSuccess ? e1 : e2)));
+  cudaError_t e = cudaSuccess;
+  for (cudaStream_t s : {s_in, s_k, s_out}) {
+    const cudaError_t ei = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = ei;
+  }
+  m.release(s_k);
+  const cudaError_t ef = cudaStreamSynchronize(s_k);
+  if (e == cudaSuccess) e = ef;
+  if (!rc && e != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
     rc = LRB_ERR_CUDA;
   }
   return rc;
@@ -309,11 +387,35 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
   int rc = check_common(atm, natm, bas, nbas, env, nenv);
   if (rc) return rc;
   if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
-  for (long long q = 0; q < 4 * nq; ++q)
-    if (shls[q] < 0 || shls[q] >= nbas) return set_error("shell index out of range"), LRB_ERR_INPUT;
+  // shell indices, then every shell's bas entry (the checks of gc_expand),
+  // on the host threads; gc_expand runs only when a shell has nctr > 1
+  std::atomic<bool> bad_index{false}, bad_shell{false}, any_gc{false};
+  host_parallel(4 * nq, HOST_GRAIN, [&](long long b, long long e) {
+    for (long long q = b; q < e; ++q)
+      if (shls[q] < 0 || shls[q] >= nbas) {
+        bad_index.store(true, std::memory_order_relaxed);
+        return;
+      }
+  });
+  if (bad_index.load()) return set_error("shell index out of range"), LRB_ERR_INPUT;
+  host_parallel(nbas, HOST_GRAIN, [&](long long b0, long long e0) {
+    bool gc = false;
+    for (long long s = b0; s < e0; ++s) {
+      const int *b = bas + 8 * s;
+      if (b[3] < 1 || b[2] < 1 || b[5] < 0 || b[6] < 0 || (long long)b[5] + b[2] > nenv ||
+          (long long)b[6] + (long long)b[2] * b[3] > nenv) {
+        bad_shell.store(true, std::memory_order_relaxed);
+        return;
+      }
+      gc = gc || b[3] > 1;
+    }
+    if (gc) any_gc.store(true, std::memory_order_relaxed);
+  });
+  if (bad_shell.load())
+    return set_error("bas entry out of range (nprim, nctr or env pointers)"), LRB_ERR_INPUT;
+  if (!any_gc.load()) return batch_host(out, coord, shls, nq, atm, natm, bas, nbas, env, nenv, 0);
   GcExpanded x;
   if ((rc = gc_expand(bas, nbas, env, nenv, x))) return rc;
-  if (!x.any) return batch_host(out, coord, shls, nq, atm, natm, bas, nbas, env, nenv, 0);
   // Generally contracted shells: every quartet becomes prod(nctr) quartets of
   // segmented sub-shells (contraction of i fastest), computed as one batch
   // and placed into the quartet's block at rows ctr * nf + component

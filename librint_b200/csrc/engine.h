@@ -64,11 +64,14 @@ struct Engine {
   // primitive quartets that passed screening
   long long fock_quartets[128] = {};
   unsigned long long *fock_prim = nullptr;   // 128 device counters
-  // host-buffer entry points: two non-blocking streams that alternate over
-  // chunks (copy-out of one chunk overlaps the next chunk's kernels) and
-  // per-stream device buffers that only grow
-  cudaStream_t pipe[2] = {nullptr, nullptr};
-  cudaEvent_t done[2] = {nullptr, nullptr};
+  // host-buffer entry points: three non-blocking streams (copies in,
+  // kernels, copies out) so that one chunk's copy in, the previous chunk's
+  // kernels and the one before's copy out run at the same time; two device
+  // slots for quartet lists and outputs (chunk c uses slot c % 2) that only
+  // grow, and the events that hand a slot from one stream to the next
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_cmp[2] = {nullptr, nullptr},
+              ev_out[2] = {nullptr, nullptr};
   Arena pipe_out[2], pipe_in[2], pipe_centers;
 };
 Engine &engine();          // for the current device

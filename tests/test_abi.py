@@ -90,3 +90,40 @@ def test_ctypes_struct_layout_matches_c_compiler(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for f, _t in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def _batch(L, m, sh, coord=1):
+    import numpy as np
+    out = np.empty(8)
+    atm, bas, env = m.atm, m.bas, m.env
+    return L.lrb_int2e_batch(out.ctypes.data_as(B.P_d), coord, sh.ctypes.data_as(B.P_i),
+                             sh.shape[0], atm.ctypes.data_as(B.P_i), atm.size // 6,
+                             bas.ctypes.data_as(B.P_i), bas.size // 8,
+                             env.ctypes.data_as(B.P_d), env.size)
+
+
+def test_batch_host_checks_before_any_device_work():
+    """lrb_int2e_batch checks every shell index and every bas entry on the
+    host threads before it touches a device; a bad index or entry anywhere
+    in a large batch (several threads' parts) is reported with the same code
+    and message as in a small one."""
+    import numpy as np
+    from librint_b200 import synthetic
+    L = B.lib()
+    m, sh = synthetic.eri_sweep((1, 0, 1, 0), 300_000, seed=3)
+    for pos in (0, 150_001, 299_999):
+        bad = sh.copy()
+        bad[pos, 2] = m.nbas
+        assert _batch(L, m, bad) == -1
+        assert b"shell index out of range" in L.lrb_last_error()
+        bad[pos, 2] = -1
+        assert _batch(L, m, bad) == -1
+    for s in (3, m.nbas // 2 + 1, m.nbas - 1):
+        bas = m.bas.copy().reshape(-1, 8)
+        bas[s, 5] = m.env.size          # exponents beyond env
+        mb = type(m)(m.atm, bas.ravel(), m.env)
+        assert _batch(L, mb, sh) == -1
+        assert b"bas entry out of range" in L.lrb_last_error()
+    bad = np.ascontiguousarray(sh[:10])
+    assert _batch(L, m, bad, coord=2) == -1
+    assert b"coord" in L.lrb_last_error()
