@@ -56,7 +56,11 @@ LRB_API const char *lrb_last_error(void);
  * -------------------------------------------------------------------*/
 LRB_API long long lrb_int2e_batch_len(int coord, const int *shls, long long nq, const int *bas, int nbas);
 
-/* Host pointers; copies in, computes on the current device, copies out. */
+/* Host pointers; copies in, computes on the current device, copies out.
+ * The indices and bas entries are checked on up to 32 host threads before
+ * any device work; the quartets then run in chunks whose copies in and out
+ * overlap other chunks' kernels when out (and the inputs) are page-locked.
+ * Returns after the whole output is on the host. */
 LRB_API int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const int *atm,
                     int natm, const int *bas, int nbas, const double *env, long long nenv);
 

@@ -7,7 +7,9 @@
  * Parity pins: the oracle is checked against golden vectors produced by the
  * reference's own shipped library (tests/golden/make_golden.py), against the
  * energy truths in checks/truth/{h2,h2o}/sto3g_E.txt, and its Rys tables
- * against 60-digit mpmath rules.
+ * against 60-digit mpmath rules and against its own binary128 rules
+ * (orc_set_rys_mode), which share no table, generator or algorithm with the
+ * CUDA kernels.
  *
  * Array conventions are librint's (src/p2c.rs, src/scf.rs): atm has 6 ints per
  * atom, bas 8 ints per shell, env holds coordinates, exponents and PySCF-
