@@ -457,15 +457,25 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, s, tcpu = cpu_rate(data, threads, steps=3, warmup=1)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"first {s} quartets of each of the {len(CLASSES)} classes of the same "
-                         f"workload, 1 untimed + 3 timed passes ({3 * len(CLASSES) * s} quartets, "
-                         f"{tcpu:.1f} s), oracle/ C++ restatement, OpenMP over quartets"}
+        try:
+            v, s, tcpu = cpu_rate(data, threads, steps=3, warmup=1)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"first {s} quartets of each of the {len(CLASSES)} classes of the "
+                             f"same workload, 1 untimed + 3 timed passes ({3 * len(CLASSES) * s} "
+                             f"quartets, {tcpu:.1f} s), oracle/ C++ restatement, OpenMP over "
+                             f"quartets"}
+        except Exception as exc:   # noqa: BLE001
+            cpu = {"error": "%s: %s" % (type(exc).__name__, exc)}
 
-    rhf = run_rhf(args.guess, threads, fp64_peak, cpu=not args.no_cpu,
-                  ablations=args.rhf_ablations, reference_run=args.rhf_reference_run) \
-        if (args.rhf and world == 1) else None
+    rhf = None
+    if args.rhf and world == 1:
+        # single-process leg (no collectives): a failure is reported in its
+        # key and does not cost the sweep's line
+        try:
+            rhf = run_rhf(args.guess, threads, fp64_peak, cpu=not args.no_cpu,
+                          ablations=args.rhf_ablations, reference_run=args.rhf_reference_run)
+        except Exception as exc:   # noqa: BLE001
+            rhf = {"error": "%s: %s" % (type(exc).__name__, exc)}
 
     if rank == 0:
         line = {

@@ -327,3 +327,37 @@ def test_oracle_eris_independent_of_node_tables():
             scale = np.abs(a).max()
             bound = (2e-11 * scale) if f else (1e-12 * np.abs(a) + 1e-13 * scale)
             assert (np.abs(a - b) <= bound).all(), (cls, coord, float(np.abs(a - b).max() / max(scale, 1e-300)))
+
+
+@pytest.mark.parametrize("omega", [0.3, -0.3])
+def test_oracle_range_separated_independent_of_node_tables(omega):
+    """Long-range (omega > 0: nodes at theta x) and short-range (omega < 0:
+    full minus long range) oracle ERIs with the independent binary128 Rys
+    rules equal those from the node tables, 3 quartets of six classes,
+    cartesian, within 1e-12 relative + 1e-13 of the block's largest element
+    (short range: 1e-12 of it, the difference of two nearly equal sums)."""
+    from librint_b200 import synthetic
+    for cls in [(0, 0, 0, 0), (1, 0, 1, 0), (1, 1, 1, 1), (2, 1, 1, 0), (2, 2, 1, 1), (2, 2, 2, 2)]:
+        m, sh = synthetic.eri_sweep(cls, 3, seed=23, kmax=2, cube_ang=3.0, elo=0.1, ehi=100.0)
+        env = m.env.copy()
+        env[8] = omega
+        m = Molecule(m.atm, m.bas, env)
+        a = oracle.int2e_batch(m, sh, 0)
+        with oracle.independent_roots():
+            b = oracle.int2e_batch(m, sh, 0)
+        scale = np.abs(a).max()
+        bound = 1e-12 * np.abs(a) + (1e-13 if omega > 0 else 1e-12) * scale
+        assert (np.abs(a - b) <= bound).all(), (cls, float(np.abs(a - b).max() / scale))
+
+
+def test_oracle_nuclear_attraction_independent_of_node_tables(golden):
+    """The oracle's nuclear-attraction matrix (Rys rules with (la+lb)/2+1
+    nodes per nucleus) with the independent binary128 rules equals the one
+    from the node tables, h2o/def2svp (d shells), 1e-14 of its largest
+    element."""
+    m = Molecule(golden["mol/h2o/def2svp/atm"], golden["mol/h2o/def2svp/bas"],
+                 golden["mol/h2o/def2svp/env"])
+    a = oracle.int1e(m, 2)
+    with oracle.independent_roots():
+        b = oracle.int1e(m, 2)
+    assert np.abs(a - b).max() <= 1e-14 * np.abs(a).max()
