@@ -221,8 +221,6 @@ double sqr_dist(const double *a, const double *b) {
 // src/g2e.rs:113-181, which keeps the HRR short on the high-l centre).
 // G[a][b][c][d]: a = power on the bra base A, b on its partner B, c on the
 // ket base C, d on its partner D.
-constexpr int NAB = 2 * LMAX + 1;
-constexpr int GSIZE = NAB * (LMAX + 1) * NAB * (LMAX + 1);
 
 struct Quartet {
   Shell si, sj, sk, sl;
@@ -345,8 +343,15 @@ int eri_cart(double *out, const Quartet &q) {
   // pair data for (ij)
   double log_rr_ij = 1.7 - 1.5 * std::log(si.a[si.nprim - 1] + sj.a[sj.nprim - 1]);
   if (q.li + q.lj > 0) log_rr_ij += (q.li + q.lj) * std::log(std::sqrt(q.rr_ij) + 1.0);
-  std::vector<double> cceij(si.nprim * sj.nprim), eij(si.nprim * sj.nprim),
-      rij(3 * si.nprim * sj.nprim);
+  // per-thread scratch, grown once: no allocation per quartet
+  static thread_local std::vector<double> cceij, eij, rij, gbuf, prim;
+  static thread_local std::vector<int> goff;
+  const size_t npij = (size_t)si.nprim * sj.nprim;
+  if (cceij.size() < npij) {
+    cceij.resize(npij);
+    eij.resize(npij);
+    rij.resize(3 * npij);
+  }
   bool empty = true;
   for (int jp = 0; jp < sj.nprim; ++jp)
     for (int ip = 0; ip < si.nprim; ++ip) {
@@ -371,8 +376,35 @@ int eri_cart(double *out, const Quartet &q) {
   const CartComp ci(q.li), cj(q.lj), ck(q.lk), cl(q.ll);
   const int nf = nfi * nfj * nfk * nfl;
   const int nc = si.nctr * sj.nctr * sk.nctr * sl.nctr;
-  std::vector<double> gbuf(3 * GSIZE), prim(nf);
-  double *g[3] = {gbuf.data(), gbuf.data() + GSIZE, gbuf.data() + 2 * GSIZE};
+  // per root three tables (x, y, z) of gs doubles each, all roots of a
+  // primitive quartet side by side
+  const int gs = (q.nab + 1) * q.sA;
+  if (gbuf.size() < 3 * (size_t)gs * 2 * NROOT_MAX) gbuf.resize(3 * (size_t)gs * 2 * NROOT_MAX);
+  if (prim.size() < (size_t)nf) {
+    prim.resize(nf);
+    goff.resize(3 * (size_t)nf);
+  }
+  // offsets into the per-axis tables of every cartesian element (i fastest):
+  // G[a][b][c][d] with a, b the powers on the bra base and partner, c, d on
+  // the ket's (src/g2e.rs:195-315, CINTg2e_index_xyz)
+  {
+    int idx = 0;
+    for (int lf = 0; lf < nfl; ++lf)
+      for (int kf = 0; kf < nfk; ++kf)
+        for (int jf = 0; jf < nfj; ++jf)
+          for (int iff = 0; iff < nfi; ++iff, ++idx) {
+            const int pi_[3] = {ci.x[iff], ci.y[iff], ci.z[iff]};
+            const int pj_[3] = {cj.x[jf], cj.y[jf], cj.z[jf]};
+            const int pk_[3] = {ck.x[kf], ck.y[kf], ck.z[kf]};
+            const int pl_[3] = {cl.x[lf], cl.y[lf], cl.z[lf]};
+            for (int ax = 0; ax < 3; ++ax) {
+              const int a = q.ibase ? pi_[ax] : pj_[ax], b = q.ibase ? pj_[ax] : pi_[ax];
+              const int c = q.kbase ? pk_[ax] : pl_[ax], d = q.kbase ? pl_[ax] : pk_[ax];
+              goff[3 * idx + ax] = a * q.sA + b * q.sB + c * q.sC + d;
+            }
+          }
+  }
+  const int *go = goff.data();
   double u[2 * NROOT_MAX], w[2 * NROOT_MAX];
   int any = 0;
 
@@ -432,28 +464,33 @@ int eri_cart(double *out, const Quartet &q) {
               nr *= 2;
             }
           }
-          std::fill(prim.begin(), prim.end(), 0.0);
+          // every root's tables, then per element the sum over the roots in
+          // root order (CINTgout2e, src/cint2e.rs:2456-2895)
+          double *gb = gbuf.data();
           for (int r = 0; r < nr; ++r) {
-            g_one_root(g, q, aij, akl, a0, fac1r, u[r], w[r], pij, rkl, rijrkl);
-            int idx = 0;
-            for (int lf = 0; lf < nfl; ++lf)
-              for (int kf = 0; kf < nfk; ++kf)
-                for (int jf = 0; jf < nfj; ++jf)
-                  for (int iff = 0; iff < nfi; ++iff, ++idx) {
-                    const int pi_[3] = {ci.x[iff], ci.y[iff], ci.z[iff]};
-                    const int pj_[3] = {cj.x[jf], cj.y[jf], cj.z[jf]};
-                    const int pk_[3] = {ck.x[kf], ck.y[kf], ck.z[kf]};
-                    const int pl_[3] = {cl.x[lf], cl.y[lf], cl.z[lf]};
-                    double v = 1.0;
-                    for (int ax = 0; ax < 3; ++ax) {
-                      const int a = q.ibase ? pi_[ax] : pj_[ax], b = q.ibase ? pj_[ax] : pi_[ax];
-                      const int c = q.kbase ? pk_[ax] : pl_[ax], d = q.kbase ? pl_[ax] : pk_[ax];
-                      v *= g[ax][a * q.sA + b * q.sB + c * q.sC + d];
-                    }
-                    prim[idx] += v;
-                  }
+            double *gr[3] = {gb + (3 * r) * (size_t)gs, gb + (3 * r + 1) * (size_t)gs,
+                             gb + (3 * r + 2) * (size_t)gs};
+            g_one_root(gr, q, aij, akl, a0, fac1r, u[r], w[r], pij, rkl, rijrkl);
+          }
+          // segmented shells (one contraction each): the block is the
+          // element order itself, so each element is contracted as it is summed
+          const bool seg = nc == 1;
+          const double cc1 = seg ? si.c[ip] * sj.c[jp] * sk.c[kp] * sl.c[lp] : 0.0;
+          double *pr = prim.data();
+          for (int idx = 0; idx < nf; ++idx) {
+            const int ox = go[3 * idx], oy = gs + go[3 * idx + 1], oz = 2 * gs + go[3 * idx + 2];
+            double sum = 0.0;
+            for (int r = 0; r < nr; ++r) {
+              const double *gr = gb + (3 * r) * (size_t)gs;
+              double v = gr[ox];
+              v *= gr[oy];
+              v *= gr[oz];
+              sum += v;
+            }
+            if (seg) out[idx] += cc1 * sum; else pr[idx] = sum;
           }
           any = 1;
+          if (seg) continue;
           // contract over every (ci, cj, ck, cl) combination
           for (int c = 0; c < nc; ++c) {
             const int cci = c % si.nctr, ccj = (c / si.nctr) % sj.nctr;
