@@ -1,6 +1,7 @@
 """Frozen-density gradients with respect to basis exponents and contraction
 coefficients -- the reference's python/librint/dscf.py functions (grad, dSf,
-dHcoref, dRf, danalyticalf, denergyf) over this library's C ABI.  The result
+dHcoref, dRf, danalyticalf, denergyf; each takes a Molecule or a PySCF-style
+object, like the scf module) over this library's C ABI.  The result
 vector indexes env[s1:s2] as the reference's utils.split does; the adjoint
 ERI kernel replaces the Enzyme reverse passes."""
 from __future__ import annotations
@@ -36,9 +37,10 @@ def _require_grad_domain(m: Molecule):
                          "separation")
 
 
-def _call(fname, m: Molecule, P):
+def _call(fname, mol, P):
+    from .scf import _p2c, _take, as_molecule
+    m = as_molecule(mol)
     _require_grad_domain(m)
-    from .scf import _p2c, _take
     args, _keep = _p2c(m)
     P = np.ascontiguousarray(P, dtype=np.float64)
     s1, s2 = split(m.bas)
@@ -46,11 +48,12 @@ def _call(fname, m: Molecule, P):
     return _take(ptr, s2 - s1)
 
 
-def dSu(m: Molecule) -> np.ndarray:
+def dSu(mol) -> np.ndarray:
     """Overlap Jacobian (s2 - s1, n, n): [l, nu, mu] = d S[mu nu] / d env[s1 + l]
     (src/p2c.rs:131; the reference's python/librint/dscf.py dSu layout)."""
+    from .scf import _p2c, _take, as_molecule
+    m = as_molecule(mol)
     _require_grad_domain(m)
-    from .scf import _p2c, _take
     args, _keep = _p2c(m)
     s1, s2 = split(m.bas)
     n = m.nao(0)

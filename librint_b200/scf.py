@@ -8,8 +8,8 @@ import ctypes
 import numpy as np
 
 from . import _bindings as B
+from . import eri as _eri
 from .basis import Molecule
-from .eri import int2e  # noqa: F401  (reference scf.int2e)
 
 
 def _arr(m: Molecule):
@@ -151,20 +151,76 @@ def _take(ptr, n):
     return a
 
 
-def int1e(m: Molecule, typec: int, coord: int = 0):
+# Codes of the reference's string arguments (python/librint/scf.py:7-36).
+INT1E_TYPES = {"ovlp": 0, "kin": 1, "nuc": 2}
+COORDS = {"cart": 0, "sph": 1}
+
+
+def as_molecule(mol) -> Molecule:
+    """``mol`` itself when it is a Molecule; otherwise a Molecule from a
+    PySCF-style object's ``_atm``, ``_bas``, ``_env`` and ``nelec`` (alpha,
+    beta), the fields the reference reads (python/librint/utils.py:21-28)."""
+    if isinstance(mol, Molecule):
+        return mol
+    try:
+        atm, bas, env, ne = mol._atm, mol._bas, mol._env, mol.nelec
+    except AttributeError as exc:
+        raise TypeError("expected a Molecule or an object with _atm, _bas, _env and nelec") from exc
+    nelec = int(ne[0] + ne[1]) if np.ndim(ne) else int(ne)
+    return Molecule(np.ascontiguousarray(atm, dtype=np.int32).ravel(),
+                    np.ascontiguousarray(bas, dtype=np.int32).ravel(),
+                    np.ascontiguousarray(env, dtype=np.float64).ravel(), nelec)
+
+
+def _code(value, table, message):
+    """Integer code of a reference string argument (an int passes through);
+    None after printing the reference's message for an unknown string."""
+    if isinstance(value, str):
+        if value not in table:
+            print(message)
+            return None
+        return table[value]
+    return int(value)
+
+
+def int1e(mol, typei="ovlp", coord="cart"):
+    """S, T or V (typei 'ovlp' / 'kin' / 'nuc', or 0 / 1 / 2), cartesian or
+    spherical (coord 'cart' / 'sph', or 0 / 1): int1e_c, src/p2c.rs:86.
+    Unknown strings print the reference's message and return None."""
+    typec = _code(typei, INT1E_TYPES, "integral type does not exist: ovlp, kin, nuc")
+    if typec is None:
+        return None
+    c = _code(coord, COORDS, "coordinate type does not exist: cart, sph")
+    if c is None:
+        return None
+    m = as_molecule(mol)
     args, _keep = _p2c(m)
-    n = m.nao(coord)
-    return _take(B.lib().int1e_c(*args, coord, typec), n * n).reshape(n, n)
+    n = m.nao(c)
+    return _take(B.lib().int1e_c(*args, c, typec), n * n).reshape(n, n)
 
 
-def density(m: Molecule, nelec=None, imax: int = 100, conv: float = 1e-6):
+def int2e(mol, coord="cart"):
+    """The dense (n, n, n, n) ERI tensor (int2e_c, src/p2c.rs:109; the
+    reference's integral2e layout, src/scf.rs:215)."""
+    c = _code(coord, COORDS, "coordinate type does not exist: cart, sph")
+    if c is None:
+        return None
+    return _eri.int2e(as_molecule(mol), c)
+
+
+def density(mol, imax: int = 200, conv: float = 1e-6, nelec=None):
+    """Converged density (density_c, src/p2c.rs:153); RuntimeError
+    (LibrintError) when the SCF fails.  nelec defaults to the molecule's."""
+    m = as_molecule(mol)
     args, _keep = _p2c(m)
     n = m.nao(0)
     nelec = m.nelec if nelec is None else nelec
     return _take(B.lib().density_c(*args, nelec, imax, conv), n * n).reshape(n, n)
 
 
-def energy(m: Molecule, P):
+def energy(mol, P):
+    """Total energy at the density P (energy_c, src/p2c.rs:186)."""
+    m = as_molecule(mol)
     args, _keep = _p2c(m)
     P = np.ascontiguousarray(P, dtype=np.float64)
     e = B.lib().energy_c(*args, P.ctypes.data_as(B.P_d), P.size)
@@ -173,7 +229,10 @@ def energy(m: Molecule, P):
     return e
 
 
-def scf(m: Molecule, nelec=None, imax: int = 100, conv: float = 1e-6):
+def scf(mol, imax: int = 200, conv: float = 1e-6, nelec=None):
+    """Converged RHF energy (scf_c, src/p2c.rs:210); RuntimeError
+    (LibrintError) when the SCF fails.  nelec defaults to the molecule's."""
+    m = as_molecule(mol)
     args, _keep = _p2c(m)
     nelec = m.nelec if nelec is None else nelec
     e = B.lib().scf_c(*args, nelec, imax, conv)
