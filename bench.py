@@ -148,6 +148,50 @@ def screened_prim_quartets(atm, bas, env, shls, expcutoff=60.0, chunk=32768):
     return total
 
 
+# Upper edges of the K^4 bins (P = Ki Kj Kk Kl primitive quartets per shell
+# quartet, K = 1..6) of the screening profile.
+K4_BINS = (1, 16, 81, 256, 625, 1296)
+
+
+def screening_profile(atm, bas, env, shls, expcutoff=60.0, chunk=32768):
+    """Per K^4 bin: shell quartets, primitive quartets, and primitive
+    quartets that pass the reference's screening (the test of
+    screened_prim_quartets), as rows of a (len(K4_BINS), 3) array."""
+    b = bas.reshape(-1, 8)
+    out = np.zeros((len(K4_BINS), 3))
+    for a in range(0, shls.shape[0], chunk):
+        sh = shls[a:a + chunk]
+        cb = _pair_cce(bas, env, atm, sh[:, 0], sh[:, 1])
+        ck = _pair_cce(bas, env, atm, sh[:, 2], sh[:, 3])
+        ck = np.where(ck <= expcutoff, ck, np.inf)
+        ok = (cb[:, :, None] + ck[:, None, :] <= expcutoff).reshape(sh.shape[0], -1)
+        passed = np.count_nonzero(ok, axis=1)
+        P = b[sh, 2].astype(np.int64).prod(axis=1)
+        k = np.searchsorted(K4_BINS, P)
+        np.add.at(out[:, 0], k, 1)
+        np.add.at(out[:, 1], k, P)
+        np.add.at(out[:, 2], k, passed)
+    return out
+
+
+def screening_summary(data, sample=65536):
+    """Fraction of primitive quartets that pass the reference's screening,
+    per class and per K^4 bin over all classes, on the first `sample`
+    quartets of every class of the sweep."""
+    tot = np.zeros((len(K4_BINS), 3))
+    per_class = {}
+    for cls, atm, bas, env, shls in data:
+        prof = screening_profile(atm, bas, env, shls[:sample])
+        tot += prof
+        per_class["%d%d%d%d" % tuple(cls)] = round(float(prof[:, 2].sum() / prof[:, 1].sum()), 4)
+    bins = [{"P_max": int(e), "quartets": int(r[0]), "prim_quartets": int(r[1]),
+             "passed": int(r[2]), "fraction": round(float(r[2] / r[1]), 4) if r[1] else None}
+            for e, r in zip(K4_BINS, tot)]
+    return {"sample": f"first {sample} quartets of each class",
+            "fraction_passed": round(float(tot[:, 2].sum() / tot[:, 1].sum()), 4),
+            "classes": per_class, "k4_bins": bins}
+
+
 def class_flops(cls, prim_quartets, nq):
     """class_flops_bytes' FLOP convention with a given primitive-quartet count."""
     li, lj, lk, ll = cls
@@ -467,6 +511,13 @@ def main():
         except Exception as exc:   # noqa: BLE001
             cpu = {"error": "%s: %s" % (type(exc).__name__, exc)}
 
+    screening = None
+    if rank == 0:
+        try:
+            screening = screening_summary(data)
+        except Exception as exc:   # noqa: BLE001
+            screening = {"error": "%s: %s" % (type(exc).__name__, exc)}
+
     rhf = None
     if args.rhf and world == 1:
         # single-process leg (no collectives): a failure is reported in its
@@ -499,6 +550,7 @@ def main():
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                            "65,536 quartets of this class, scaled per quartet"},
             "class_kernel_ms": {"%d%d%d%d" % c: round(v, 4) for c, v in cls_ms.items()},
+            "screening": screening,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),

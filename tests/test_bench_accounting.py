@@ -94,3 +94,21 @@ def test_traffic_figure_close_to_algorithmic_bytes():
     per_q = nbytes / shls.shape[0]
     assert 8 * 625 < per_q < 8 * 700
     assert abs(bench.NCU_TRAFFIC_PER_QUARTET[cls] / per_q - 1.0) < 0.10
+
+
+def test_screening_profile_matches_the_screened_count():
+    """The K^4-binned screening profile sums to screened_prim_quartets and to
+    the unscreened primitive quartets, and puts each quartet in its bin."""
+    for cls in [(0, 0, 0, 0), (2, 1, 1, 0), (2, 2, 2, 2)]:
+        atm, bas, env, shls = _data(cls, 3000, seed=9)
+        prof = bench.screening_profile(atm, bas, env, shls, chunk=1000)
+        assert prof[:, 0].sum() == 3000
+        k = bas.reshape(-1, 8)[:, 2][shls].astype(np.int64).prod(axis=1)
+        assert prof[:, 1].sum() == k.sum()
+        assert prof[:, 2].sum() == bench.screened_prim_quartets(atm, bas, env, shls)
+        assert prof[0, 0] == np.count_nonzero(k == 1)
+    data = [(c,) + _data(c, 500, seed=3) for c in [(1, 0, 0, 0), (2, 2, 1, 1)]]
+    summ = bench.screening_summary(data, sample=400)
+    assert set(summ["classes"]) == {"1000", "2211"}
+    assert sum(b["quartets"] for b in summ["k4_bins"]) == 800
+    assert 0.0 < summ["fraction_passed"] <= 1.0
