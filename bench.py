@@ -346,6 +346,128 @@ def cpu_rate(data, threads, steps, warmup, sample=None):
     return steps * len(data) * s / tt, s, tt
 
 
+# ------------------------------------------------------------ end to end
+def merged_layout(data):
+    """Sizes and offsets of the sweep's classes placed back to back in one
+    molecule: per class its first atom, shell and env entry and its first
+    output element; totals last."""
+    na = nb = ne = no = 0
+    offs = []
+    for cls, atm, bas, env, shls in data:
+        b = bas.reshape(-1, 8)
+        l = b[:, 1][shls]
+        nout = int(((2 * l + 1).prod(axis=1)).sum())
+        offs.append((na, nb, ne, no))
+        na += atm.size // 6
+        nb += b.shape[0]
+        ne += env.size
+        no += nout
+    # the atm/bas/env pointers are int32; the kernels index bas and atm rows
+    # with 32-bit products
+    if ne >= 2 ** 31 or 8 * nb >= 2 ** 31 or 6 * na >= 2 ** 31:
+        raise ValueError("sweep too large for one molecule (int32 pointers)")
+    return offs, (na, nb, ne, no)
+
+
+def fill_merged(data, offs, atm_all, bas_all, env_all, shls_all):
+    """Writes the classes into the merged arrays (numpy views), shifting
+    atom, shell and env pointers by each class's offsets."""
+    A = atm_all.reshape(-1, 6)
+    Bv = bas_all.reshape(-1, 8)
+    S = shls_all.reshape(-1, 4)
+    q = 0
+    for (cls, atm, bas, env, shls), (oa, ob, oe, _) in zip(data, offs):
+        a = atm.reshape(-1, 6)
+        b = bas.reshape(-1, 8)
+        A[oa:oa + a.shape[0]] = a
+        A[oa:oa + a.shape[0], 1] += oe
+        A[oa:oa + a.shape[0], 3] += oe
+        Bv[ob:ob + b.shape[0]] = b
+        Bv[ob:ob + b.shape[0], 0] += oa
+        Bv[ob:ob + b.shape[0], 5] += oe
+        Bv[ob:ob + b.shape[0], 6] += oe
+        env_all[oe:oe + env.size] = env
+        S[q:q + shls.shape[0]] = shls
+        S[q:q + shls.shape[0]] += ob
+        q += shls.shape[0]
+
+
+def e2e_one_call(L, data, dev_data):
+    """Step function of the end-to-end leg as one lrb_int2e_batch call over
+    all classes (page-locked inputs and output); (step, h2d bytes, d2h
+    bytes).  step.out is the output tensor."""
+    import ctypes
+    import torch
+    from librint_b200 import _bindings as B
+    offs, (na, nb, ne, no) = merged_layout(data)
+    nq = sum(d[4].shape[0] for d in data)
+    atm = torch.empty(6 * na, dtype=torch.int32, pin_memory=True)
+    bas = torch.empty(8 * nb, dtype=torch.int32, pin_memory=True)
+    env = torch.empty(ne, dtype=torch.float64, pin_memory=True)
+    shl = torch.empty(4 * nq, dtype=torch.int32, pin_memory=True)
+    out = torch.empty(no, dtype=torch.float64, pin_memory=True)
+    fill_merged(data, offs, atm.numpy(), bas.numpy(), env.numpy(), shl.numpy())
+    P_i, P_d = B.P_i, B.P_d
+
+    def step():
+        rc = L.lrb_int2e_batch(ctypes.cast(out.data_ptr(), P_d), 1,
+                               ctypes.cast(shl.data_ptr(), P_i), nq,
+                               ctypes.cast(atm.data_ptr(), P_i), na,
+                               ctypes.cast(bas.data_ptr(), P_i), nb,
+                               ctypes.cast(env.data_ptr(), P_d), ne)
+        B.check(rc, "lrb_int2e_batch")
+    step.out = out
+    step.keep = (atm, bas, env, shl)
+    h2d = 4 * (6 * na + 8 * nb + 4 * nq) + 8 * ne
+    return step, h2d, 8 * no
+
+
+def e2e_check_one_call(data, dev_data, out, n=4096):
+    """The one-call output equals the device-resident leg's class outputs
+    (the same kernels on the same quartets), bit for bit, on the first,
+    middle and last n elements of every class."""
+    import torch
+    o = 0
+    for t in dev_data:
+        ref = t["out"]
+        m = ref.numel()
+        for a in (0, max(0, m // 2 - n // 2), max(0, m - n)):
+            b = min(m, a + n)
+            if not torch.equal(out[o + a:o + b], ref[a:b].cpu()):
+                raise AssertionError("one-call output differs from the device-resident leg in "
+                                     "class %s" % (t["cls"],))
+        o += m
+    if o != out.numel():
+        raise AssertionError("one-call output length %d, classes %d" % (out.numel(), o))
+
+
+def e2e_per_class(L, data, dev_data):
+    """Step function of the end-to-end leg as one lrb_int2e_batch call per
+    class (page-locked inputs and outputs); (step, h2d bytes, d2h bytes)."""
+    import ctypes
+    import torch
+    from librint_b200 import _bindings as B
+    host = []
+    h2d = d2h = 0
+    for (cls, atm, bas, env, shls), t in zip(data, dev_data):
+        pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+        out = torch.empty(t["out"].numel(), dtype=torch.float64, pin_memory=True)
+        host.append((pin(atm), pin(bas), pin(env), pin(shls), out))
+        h2d += atm.nbytes + bas.nbytes + env.nbytes + shls.nbytes
+        d2h += out.numel() * 8
+    P_i, P_d = B.P_i, B.P_d
+
+    def step():
+        for (a, b, e, s, o) in host:
+            rc = L.lrb_int2e_batch(ctypes.cast(o.data_ptr(), P_d), 1,
+                                   ctypes.cast(s.data_ptr(), P_i), s.numel() // 4,
+                                   ctypes.cast(a.data_ptr(), P_i), a.numel() // 6,
+                                   ctypes.cast(b.data_ptr(), P_i), b.numel() // 8,
+                                   ctypes.cast(e.data_ptr(), P_d), e.numel())
+            B.check(rc, "lrb_int2e_batch")
+    return step, h2d, d2h
+
+
 # ------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -459,31 +581,29 @@ def main():
     # end to end through the host API (pinned host buffers, copies timed)
     e2e = None
     if args.e2e_steps > 0:
-        from librint_b200.basis import Molecule
-        host = []
-        h2d = d2h = 0
-        for (cls, atm, bas, env, shls), t in zip(data, dev_data):
-            pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
-            out = torch.empty(t["out"].numel(), dtype=torch.float64).pin_memory()
-            host.append((pin(atm), pin(bas), pin(env), pin(shls), out))
-            h2d += atm.nbytes + bas.nbytes + env.nbytes + shls.nbytes
-            d2h += out.numel() * 8
-        P_i, P_d = B.P_i, B.P_d
-        import ctypes
-
-        def e2e_step():
-            for (a, b, e, s, o) in host:
-                rc = L.lrb_int2e_batch(ctypes.cast(o.data_ptr(), P_d), 1,
-                                       ctypes.cast(s.data_ptr(), P_i), s.numel() // 4,
-                                       ctypes.cast(a.data_ptr(), P_i), a.numel() // 6,
-                                       ctypes.cast(b.data_ptr(), P_i), b.numel() // 8,
-                                       ctypes.cast(e.data_ptr(), P_d), e.numel())
-                B.check(rc, "lrb_int2e_batch")
-        e2e_step()
-        torch.cuda.synchronize()
+        import torch.distributed as tdist
+        form, err = "one call", None
+        try:
+            step_fn, h2d, d2h = e2e_one_call(L, data, dev_data)
+            step_fn()                                   # warm-up, then checked
+            torch.cuda.synchronize()
+            e2e_check_one_call(data, dev_data, step_fn.out)
+        except Exception as exc:   # noqa: BLE001
+            err = "%s: %s" % (type(exc).__name__, exc)
+        if world > 1:
+            flag = torch.tensor([0 if err else 1], device=dev)
+            tdist.all_reduce(flag, op=tdist.ReduceOp.MIN)
+            if int(flag.item()) == 0 and err is None:
+                err = "another rank's one-call form failed"
+        if err is not None:
+            step_fn = h2d = d2h = None
+            form = "one call per class"
+            step_fn, h2d, d2h = e2e_per_class(L, data, dev_data)
+            step_fn()
+            torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            e2e_step()
+            step_fn()
         torch.cuda.synchronize()
         te = shard.max_over_ranks(time.perf_counter() - t0, dev)
         bw = link_bandwidth(dev)
@@ -494,10 +614,15 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "step_s": step_s, "link": bw, "bound_s": bound,
                "frac_of_overlapped_bound": max(bound.values()) / step_s,
-               "note": "lrb_int2e_batch with pinned host buffers; all %d classes per step; "
-                       "bound_s = bytes / measured pinned copy bandwidth per direction, and the "
+               "form": form,
+               "note": "lrb_int2e_batch with pinned host buffers; all %d classes per step (%s: "
+                       "one call over the classes' quartets back to back, its output checked "
+                       "against the device-resident leg's, or one call per class); bound_s = "
+                       "bytes / measured pinned copy bandwidth per direction, and the "
                        "device-resident step time; a fully overlapped pipeline takes the largest"
-                       % len(CLASSES)}
+                       % (len(CLASSES), form)}
+        if err is not None:
+            e2e["one_call_error"] = err
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

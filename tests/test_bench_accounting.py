@@ -112,3 +112,48 @@ def test_screening_profile_matches_the_screened_count():
     assert set(summ["classes"]) == {"1000", "2211"}
     assert sum(b["quartets"] for b in summ["k4_bins"]) == 800
     assert 0.0 < summ["fraction_passed"] <= 1.0
+
+
+def test_merged_sweep_layout():
+    """The end-to-end leg's one-call layout: every quartet of the merged
+    molecule names shells with the same angular momentum, primitives,
+    exponents, coefficients and centres as in its own class; the merged
+    arrays pass the library's host checks (on a machine without a GPU the
+    call then stops at the first CUDA call, not at an input error), and the
+    packed output length is the classes' lengths summed."""
+    from librint_b200 import _bindings as B
+    from librint_b200 import eri
+    from librint_b200.basis import Molecule
+    data = [(c,) + _data(c, 700, seed=4) for c in [(0, 0, 0, 0), (2, 1, 1, 0), (2, 2, 2, 2)]]
+    offs, (na, nb, ne, no) = bench.merged_layout(data)
+    nq = sum(d[4].shape[0] for d in data)
+    atm = np.empty(6 * na, np.int32)
+    bas = np.empty(8 * nb, np.int32)
+    env = np.empty(ne)
+    shl = np.empty(4 * nq, np.int32)
+    bench.fill_merged(data, offs, atm, bas, env, shl)
+    A, Bm, S = atm.reshape(-1, 6), bas.reshape(-1, 8), shl.reshape(-1, 4)
+    q0 = 0
+    for (cls, a, b, e, sh), (oa, ob, oe, oo) in zip(data, offs):
+        a, b = a.reshape(-1, 6), b.reshape(-1, 8)
+        for q in (0, 350, 699):
+            for k in range(4):
+                s_old, s_new = sh[q, k], S[q0 + q, k]
+                bo, bn = b[s_old], Bm[s_new]
+                assert bn[1] == bo[1] and bn[2] == bo[2]
+                K = bo[2]
+                np.testing.assert_array_equal(env[bn[5]:bn[5] + K], e[bo[5]:bo[5] + K])
+                np.testing.assert_array_equal(env[bn[6]:bn[6] + K], e[bo[6]:bo[6] + K])
+                pc_o, pc_n = a[bo[0], 1], A[bn[0], 1]
+                np.testing.assert_array_equal(env[pc_n:pc_n + 3], e[pc_o:pc_o + 3])
+        q0 += sh.shape[0]
+    m = Molecule(atm, bas, env)
+    assert eri.batch_len(m, S, 1) == no == sum(eri.batch_len(Molecule(d[1], d[2], d[3]), d[4], 1)
+                                              for d in data)
+    import torch
+    if not torch.cuda.is_available():
+        out = np.empty(no)
+        rc = B.lib().lrb_int2e_batch(out.ctypes.data_as(B.P_d), 1, shl.ctypes.data_as(B.P_i), nq,
+                                     atm.ctypes.data_as(B.P_i), na, bas.ctypes.data_as(B.P_i), nb,
+                                     env.ctypes.data_as(B.P_d), ne)
+        assert rc == -4, B.lib().lrb_last_error()
