@@ -3,6 +3,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "engine.h"
 
@@ -32,10 +33,11 @@ char *Arena::get(cudaStream_t st, size_t need) {
 
 Engine &engine() {
   static std::mutex mu;
-  static Engine *per_dev[64] = {nullptr};
+  static std::vector<Engine *> per_dev;   // indexed by device; engines live until exit
   int dev = 0;
-  cudaGetDevice(&dev);
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
   std::lock_guard<std::mutex> g(mu);
+  if ((size_t)dev >= per_dev.size()) per_dev.resize((size_t)dev + 1, nullptr);
   if (!per_dev[dev]) {
     // keep freed stream-ordered memory in the device's default pool instead
     // of returning it to the driver at every synchronisation, so repeated
