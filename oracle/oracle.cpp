@@ -273,11 +273,14 @@ Quartet make_quartet(const int *shls, const int *atm, const int *bas, const doub
 }
 
 // One root: B00/B10/B01/C00/C0p (src/g2e.rs:5655-5673), 2D VRR on (A, C)
-// (src/g2e.rs:316-506), HRR A->B and C->D (src/g2e.rs:507-909).
-void g_one_root(double *g[3], const Quartet &q, double aij, double akl,
+// (src/g2e.rs:316-506), HRR A->B and C->D (src/g2e.rs:507-909).  Element e
+// of axis ax is at g[ax][e * rs]: the tables of all roots of a primitive
+// quartet interleave (root innermost, as libcint's g arrays).
+void g_one_root(double *g[3], int rs, const Quartet &q, double aij, double akl,
                 double a0, double fac1, double u, double w,
                 const double *rij, const double *rkl, const double *rijrkl) {
-  const int nab = q.nab, ncd = q.ncd, sA = q.sA, sB = q.sB, sC = q.sC;
+  const int sA = q.sA * rs, sB = q.sB * rs, sC = q.sC * rs, sD = rs;
+  const int nab = q.nab, ncd = q.ncd;
   const double a1 = aij * akl;
   const double u2 = a0 * u;
   const double tmp4 = 0.5 / (u2 * (aij + akl) + a1);
@@ -319,8 +322,8 @@ void g_one_root(double *g[3], const Quartet &q, double aij, double akl,
       for (int b = 0; b <= q.lB; ++b)
         for (int d = 1; d <= q.lD; ++d)
           for (int c = 0; c <= ncd - d; ++c)
-            G[a * sA + b * sB + c * sC + d] = G[a * sA + b * sB + (c + 1) * sC + d - 1] +
-                                              cd * G[a * sA + b * sB + c * sC + d - 1];
+            G[a * sA + b * sB + c * sC + d * sD] = G[a * sA + b * sB + (c + 1) * sC + (d - 1) * sD] +
+                                                   cd * G[a * sA + b * sB + c * sC + (d - 1) * sD];
   }
 }
 
@@ -464,13 +467,13 @@ int eri_cart(double *out, const Quartet &q) {
               nr *= 2;
             }
           }
-          // every root's tables, then per element the sum over the roots in
-          // root order (CINTgout2e, src/cint2e.rs:2456-2895)
+          // every root's tables (root innermost), then per element the sum
+          // over the roots in root order (CINTgout2e, src/cint2e.rs:2456-2895)
           double *gb = gbuf.data();
+          const size_t ga = (size_t)gs * nr;     // one axis, all roots
           for (int r = 0; r < nr; ++r) {
-            double *gr[3] = {gb + (3 * r) * (size_t)gs, gb + (3 * r + 1) * (size_t)gs,
-                             gb + (3 * r + 2) * (size_t)gs};
-            g_one_root(gr, q, aij, akl, a0, fac1r, u[r], w[r], pij, rkl, rijrkl);
+            double *gr[3] = {gb + r, gb + ga + r, gb + 2 * ga + r};
+            g_one_root(gr, nr, q, aij, akl, a0, fac1r, u[r], w[r], pij, rkl, rijrkl);
           }
           // segmented shells (one contraction each): the block is the
           // element order itself, so each element is contracted as it is summed
@@ -478,13 +481,14 @@ int eri_cart(double *out, const Quartet &q) {
           const double cc1 = seg ? si.c[ip] * sj.c[jp] * sk.c[kp] * sl.c[lp] : 0.0;
           double *pr = prim.data();
           for (int idx = 0; idx < nf; ++idx) {
-            const int ox = go[3 * idx], oy = gs + go[3 * idx + 1], oz = 2 * gs + go[3 * idx + 2];
+            const double *px = gb + (size_t)go[3 * idx] * nr;
+            const double *py = gb + ga + (size_t)go[3 * idx + 1] * nr;
+            const double *pz = gb + 2 * ga + (size_t)go[3 * idx + 2] * nr;
             double sum = 0.0;
             for (int r = 0; r < nr; ++r) {
-              const double *gr = gb + (3 * r) * (size_t)gs;
-              double v = gr[ox];
-              v *= gr[oy];
-              v *= gr[oz];
+              double v = px[r];
+              v *= py[r];
+              v *= pz[r];
               sum += v;
             }
             if (seg) out[idx] += cc1 * sum; else pr[idx] = sum;
