@@ -508,13 +508,35 @@ def lowdin(S):
     return (U * np.sqrt(w)) @ U.T, (U / np.sqrt(w)) @ U.T
 
 
-def density_from_lowdin(Pt, S, nocc):
-    """Closed-shell AO density from an approximate Loewdin density: the N/2
-    largest eigenvectors C of sym(Pt) give S^(-1/2) (2 C C^T) S^(-1/2), which
-    is idempotent in the S metric (P S P = 2 P) with tr(P S) = 2 nocc."""
+def fractional_occupations(w, nocc, iters=200):
+    """Occupations f_i = clip(w_i + mu, 0, 2) of eigenvalues w with the shift
+    mu (bisection) that makes sum f = 2 nocc: the order of the eigenvalues
+    is kept and every occupation lies in [0, 2]."""
+    lo, hi = -float(w.max()) - 2.0, 2.0 - float(w.min())
+    for _ in range(iters):
+        mu = 0.5 * (lo + hi)
+        if np.clip(w + mu, 0.0, 2.0).sum() > 2.0 * nocc:
+            hi = mu
+        else:
+            lo = mu
+    return np.clip(w + 0.5 * (lo + hi), 0.0, 2.0)
+
+
+def density_from_lowdin(Pt, S, nocc, fractional=False):
+    """Closed-shell AO density from an approximate Loewdin density.  By
+    default the N/2 largest eigenvectors C of sym(Pt) give
+    S^(-1/2) (2 C C^T) S^(-1/2), idempotent in the S metric (P S P = 2 P)
+    with tr(P S) = 2 nocc.  With ``fractional`` the eigenvectors keep
+    occupations in [0, 2] from their eigenvalues (fractional_occupations),
+    so orbitals the prediction leaves near the occupation cut enter the
+    first Fock build partly filled instead of being dropped; tr(P S) is
+    still 2 nocc."""
     w, V = np.linalg.eigh(0.5 * (Pt + Pt.T))
-    C = V[:, len(w) - nocc:]
     _, Sih = lowdin(S)
+    if fractional:
+        f = fractional_occupations(w, nocc)
+        return Sih @ ((V * f) @ V.T) @ Sih
+    C = V[:, len(w) - nocc:]
     return Sih @ (2.0 * C @ C.T) @ Sih
 
 
@@ -617,11 +639,14 @@ class LearnedGuess:
         y = out.double().cpu().numpy()
         return self.ymu[T] + self.ysd[T] * y
 
-    def predict(self, m: Molecule, S: np.ndarray, nelec=None):
-        """P0 in the AO basis from the overlap matrix S of ``m``."""
+    def predict(self, m: Molecule, S: np.ndarray, nelec=None, fractional=False):
+        """P0 in the AO basis from the overlap matrix S of ``m`` (projected on
+        the N/2 most occupied predicted orbitals, or with fractional
+        occupations: density_from_lowdin)."""
         ps = self.model.pairs(m)
         Pt = self.model.to_density(m, self.predict_local(ps.X, ps.types), ps)
-        return density_from_lowdin(Pt, S, (m.nelec if nelec is None else nelec) // 2)
+        return density_from_lowdin(Pt, S, (m.nelec if nelec is None else nelec) // 2,
+                                   fractional=fractional)
 
     # persistence -----------------------------------------------------
     def save(self, path):

@@ -149,6 +149,31 @@ def test_lowdin_density_round_trip():
     np.testing.assert_allclose(P0 @ S @ P0, 2 * P0, atol=1e-10)
 
 
+def test_fractional_lowdin_density():
+    """The fractional start keeps the electron count, has Loewdin occupations
+    in [0, 2] in the order of the predicted eigenvalues, equals the
+    projected density for an exact (0 / 2) prediction, and keeps partly
+    filled the orbitals a fuzzy prediction leaves near the cut."""
+    m = synthetic.water_like()
+    P = oracle.density(m, conv=1e-11)[0]
+    S = oracle.int1e(m, 0)
+    Sh, _ = G.lowdin(S)
+    Pt = Sh @ P @ Sh
+    np.testing.assert_allclose(G.density_from_lowdin(Pt, S, m.nelec // 2, fractional=True), P,
+                               atol=1e-9)
+    # a prediction unsure about the 5th and 6th orbitals (7 AOs, 5 occupied)
+    _, V = np.linalg.eigh(Pt)
+    Pn = (V * np.array([-0.1, 0.2, 0.9, 1.1, 1.9, 2.0, 2.1])) @ V.T
+    P0 = G.density_from_lowdin(Pn, S, m.nelec // 2, fractional=True)
+    assert abs(np.sum(P0 * S) - m.nelec) < 1e-9
+    occ = np.linalg.eigvalsh(Sh @ P0 @ Sh)
+    assert occ.min() > -1e-10 and occ.max() < 2 + 1e-10
+    assert ((occ > 1e-6) & (occ < 2 - 1e-6)).any()        # some partly filled
+    w = np.linalg.eigvalsh(0.5 * (Pn + Pn.T))
+    f = G.fractional_occupations(w, m.nelec // 2)
+    assert abs(f.sum() - m.nelec) < 1e-9 and (np.diff(f) >= -1e-12).all()
+
+
 def _pairs_loop(pm, m):
     """Per-pair restatement of PairModel.pairs (frames by _frame), the
     reference for the vectorised version."""
