@@ -3,16 +3,13 @@
 // there is no CPU fallback.
 #include <cuda_runtime.h>
 
-#include <sched.h>
-
 #include <algorithm>
-#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
-#include <thread>
 #include <vector>
 
+#include "batch_plan.h"
 #include "engine.h"
 #include "eri_device.cuh"
 #include "fock.h"
@@ -92,43 +89,21 @@ int check_common(const int *atm, int natm, const int *bas, int nbas, const doubl
   return LRB_OK;
 }
 
-// Host threads this process may run on (its CPU affinity), at least 1.
-int host_threads() {
-  cpu_set_t set;
-  if (sched_getaffinity(0, sizeof set, &set) == 0) return std::max(1, CPU_COUNT(&set));
-  return std::max(1u, std::thread::hardware_concurrency());
-}
-
-// fn(begin, end) over contiguous parts of [0, n), each of at least `grain`
-// items, on up to 32 host threads (the caller's thread takes the first
-// part); one part when n <= grain.  A thread that cannot be started runs its
-// part on the caller's thread.
-template <class F>
-void host_parallel(long long n, long long grain, F &&fn) {
-  if (n <= 0) return;
-  const long long nt = std::min<long long>({(long long)host_threads(), 32, (n + grain - 1) / grain});
-  if (nt <= 1) {
-    fn(0LL, n);
-    return;
+// Two device buffers of na and nb doubles on st; on failure neither is
+// kept and the allocation error is cleared.
+int alloc_pair(cudaStream_t st, size_t na, double **a, size_t nb, double **b) {
+  *a = *b = nullptr;
+  if (cudaMallocAsync((void **)a, std::max(na, (size_t)1) * 8, st) != cudaSuccess) {
+    *a = nullptr;
+  } else if (cudaMallocAsync((void **)b, std::max(nb, (size_t)1) * 8, st) != cudaSuccess) {
+    *b = nullptr;
   }
-  const long long per = (n + nt - 1) / nt;
-  std::vector<std::thread> th;
-  th.reserve((size_t)nt);
-  for (long long t = 1; t < nt; ++t) {
-    const long long b = t * per, e = std::min(n, b + per);
-    if (b >= e) break;
-    try {
-      th.emplace_back([&fn, b, e] { fn(b, e); });
-    } catch (...) {
-      fn(b, e);
-    }
-  }
-  fn(0LL, std::min(n, per));
-  for (std::thread &x : th) x.join();
+  if (*a && *b) return LRB_OK;
+  cudaGetLastError();
+  if (*a) cudaFreeAsync(*a, st);
+  *a = *b = nullptr;
+  return set_error("device allocation failed"), LRB_ERR_ALLOC;
 }
-
-// Items per host thread below which a loop stays on one thread.
-constexpr long long HOST_GRAIN = 1 << 16;
 
 // Dense symmetric tensor from canonical quartet blocks.
 __global__ void k_scatter8(const double *__restrict__ blocks, const long long *__restrict__ boff,
@@ -185,6 +160,11 @@ int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq
                           (cudaStream_t)stream, nullptr);
 }
 
+// Chunk limits: at most CHUNK_Q quartets and, past a chunk's first quartet,
+// CHUNK_OUT output doubles (256 MB); env[0..ENV_HEAD) holds the settings
+// every chunk reads (cutoff, omega).
+constexpr long long CHUNK_Q = 1 << 18, CHUNK_OUT = 1 << 25, ENV_HEAD = 20;
+
 // Host buffers in and out.  The quartets run in chunks through three
 // non-blocking streams: copies in (the chunk's quartet list, and in the
 // streamed layout its part of the molecule), kernels, copies out.  Chunk c
@@ -192,105 +172,18 @@ int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq
 // copy in and chunk c-1's copy out overlap chunk c's kernels; events hand
 // each slot on (copy in -> kernels -> copy out -> the copy in two chunks
 // later).  The kernels of all chunks share the engine's workspace and run in
-// order on the one kernel stream.
-// Shells, atoms and env entries (half-open ranges) that one chunk's quartets
-// can reach: every shell between the lowest and highest index it names,
-// their atoms, and the env entries of those shells and atoms.
-struct ChunkRange {
-  int s0, s1, a0, a1;
-  long long e0, e1;
-};
-
-// Ranges of every chunk; false (upload everything up front) unless they are
-// valid and each chunk's ranges lie after the previous chunk's, so a chunk can
-// upload its own part of the molecule while earlier chunks compute.  The
-// chunks' ranges are found in parallel, then checked in order.
-static bool chunk_ranges(const int *shls, const std::vector<long long> &qb, const int *atm,
-                         int natm, const int *bas, int nbas, long long nenv, long long head,
-                         std::vector<ChunkRange> &rg) {
-  const int nchunk = (int)qb.size() - 1;
-  if (nchunk < 2) return false;
-  rg.assign(nchunk, ChunkRange{0, 0, 0, 0, 0, 0});
-  std::vector<char> valid(nchunk, 0);
-  auto one = [&](int c) {
-    ChunkRange r{nbas, -1, natm, -1, nenv, -1};
-    for (long long q = 4 * qb[c]; q < 4 * qb[c + 1]; ++q) {
-      r.s0 = std::min(r.s0, shls[q]);
-      r.s1 = std::max(r.s1, shls[q] + 1);
-    }
-    for (int sh = r.s0; sh < r.s1; ++sh) {
-      const int *b = bas + 8 * sh;
-      if (b[0] < 0 || b[0] >= natm || b[2] < 1 || b[3] < 1 || b[5] < 0 || b[6] < 0 ||
-          (long long)b[5] + b[2] > nenv || (long long)b[6] + (long long)b[2] * b[3] > nenv)
-        return;
-      r.a0 = std::min(r.a0, b[0]);
-      r.a1 = std::max(r.a1, b[0] + 1);
-      r.e0 = std::min({r.e0, (long long)b[5], (long long)b[6]});
-      r.e1 = std::max({r.e1, (long long)b[5] + b[2], (long long)b[6] + (long long)b[2] * b[3]});
-    }
-    for (int a = r.a0; a < r.a1; ++a) {
-      const long long pc = atm[6 * a + 1];
-      if (pc < 0 || pc + 3 > nenv) return;
-      r.e0 = std::min(r.e0, pc);
-      r.e1 = std::max(r.e1, pc + 3);
-    }
-    rg[c] = r;
-    valid[c] = 1;
-  };
-  host_parallel(nchunk, 1, [&](long long b, long long e) {
-    for (long long c = b; c < e; ++c) one((int)c);
-  });
-  for (int c = 0; c < nchunk; ++c) {
-    if (!valid[c]) return false;
-    const ChunkRange &r = rg[c];
-    const ChunkRange *prev = c > 0 ? &rg[c - 1] : nullptr;
-    if (r.e0 < head || (prev && (r.s0 < prev->s1 || r.a0 < prev->a1 || r.e0 < prev->e1)))
-      return false;
-  }
-  return true;
-}
-
-static int batch_host(double *out, int coord, const int *shls, long long nq, const int *atm,
-                      int natm, const int *bas, int nbas, const double *env, long long nenv,
-                      int gc_screen) {
+// order on the one kernel stream.  The batch has been checked and planned by
+// plan::plan_batch.
+static int batch_host(double *out, int coord, const int *shls, const int *atm, int natm,
+                      const int *bas, int nbas, const double *env, long long nenv, int gc_screen,
+                      const plan::BatchPlan &p) {
   int rc = LRB_OK;
-  // chunk boundaries: at most CHUNK_Q quartets and about CHUNK_OUT doubles each
-  constexpr long long CHUNK_Q = 1 << 18, CHUNK_OUT = 1 << 25;
-  std::vector<long long> blen((size_t)nq);
-  host_parallel(nq, HOST_GRAIN, [&](long long b, long long e) {
-    for (long long q = b; q < e; ++q) {
-      long long d = 1;
-      for (int a = 0; a < 4; ++a) d *= shell_dim(coord, bas, shls[4 * q + a]);
-      blen[(size_t)q] = d;
-    }
-  });
-  std::vector<long long> qb{0}, ob{0};
-  long long max_q = 0, max_len = 1;
-  {
-    long long cq = 0, co = 0, tot = 0;
-    for (long long q = 0; q < nq; ++q) {
-      const long long b = blen[(size_t)q];
-      if (cq > 0 && (cq == CHUNK_Q || co + b > CHUNK_OUT)) {
-        qb.push_back(q);
-        ob.push_back(tot);
-        max_q = std::max(max_q, cq);
-        max_len = std::max(max_len, co);
-        cq = co = 0;
-      }
-      ++cq;
-      co += b;
-      tot += b;
-    }
-    qb.push_back(nq);
-    ob.push_back(tot);
-    max_q = std::max(max_q, cq);
-    max_len = std::max(max_len, co);
-  }
-  const int nchunk = (int)qb.size() - 1;
-  // env[0..head) holds the settings every chunk reads (cutoff, omega)
-  const long long head = std::min(nenv, 20LL);
-  std::vector<ChunkRange> rg;
-  const bool streamed = chunk_ranges(shls, qb, atm, natm, bas, nbas, nenv, head, rg);
+  const std::vector<long long> &qb = p.qb, &ob = p.ob;
+  const long long max_q = p.max_q, max_len = p.max_len;
+  const int nchunk = p.nchunk();
+  const long long head = std::min(nenv, ENV_HEAD);
+  const std::vector<plan::ChunkRange> &rg = p.rg;
+  const bool streamed = p.streamed;
 
   Engine &eng = engine();
   for (int i = 0; i < 3; ++i)
@@ -333,7 +226,7 @@ static int batch_host(double *out, int coord, const int *shls, long long nq, con
     ok = ok && cudaMemcpyAsync(d_sh, shls + 4 * qb[c], sizeof(int) * 4 * (size_t)nqc,
                                cudaMemcpyHostToDevice, s_in) == cudaSuccess;
     if (streamed) {
-      const ChunkRange &r = rg[c];
+      const plan::ChunkRange &r = rg[c];
       ok = ok && cudaMemcpyAsync(m.bas + 8 * (size_t)r.s0, bas + 8 * (size_t)r.s0,
                                  sizeof(int) * 8 * (size_t)(r.s1 - r.s0), cudaMemcpyHostToDevice,
                                  s_in) == cudaSuccess;
@@ -387,33 +280,14 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
   int rc = check_common(atm, natm, bas, nbas, env, nenv);
   if (rc) return rc;
   if (coord != 0 && coord != 1) return set_error("coord must be 0 or 1"), LRB_ERR_INPUT;
-  // shell indices, then every shell's bas entry (the checks of gc_expand),
-  // on the host threads; gc_expand runs only when a shell has nctr > 1
-  std::atomic<bool> bad_index{false}, bad_shell{false}, any_gc{false};
-  host_parallel(4 * nq, HOST_GRAIN, [&](long long b, long long e) {
-    for (long long q = b; q < e; ++q)
-      if (shls[q] < 0 || shls[q] >= nbas) {
-        bad_index.store(true, std::memory_order_relaxed);
-        return;
-      }
-  });
-  if (bad_index.load()) return set_error("shell index out of range"), LRB_ERR_INPUT;
-  host_parallel(nbas, HOST_GRAIN, [&](long long b0, long long e0) {
-    bool gc = false;
-    for (long long s = b0; s < e0; ++s) {
-      const int *b = bas + 8 * s;
-      if (b[3] < 1 || b[2] < 1 || b[5] < 0 || b[6] < 0 || (long long)b[5] + b[2] > nenv ||
-          (long long)b[6] + (long long)b[2] * b[3] > nenv) {
-        bad_shell.store(true, std::memory_order_relaxed);
-        return;
-      }
-      gc = gc || b[3] > 1;
-    }
-    if (gc) any_gc.store(true, std::memory_order_relaxed);
-  });
-  if (bad_shell.load())
-    return set_error("bas entry out of range (nprim, nctr or env pointers)"), LRB_ERR_INPUT;
-  if (!any_gc.load()) return batch_host(out, coord, shls, nq, atm, natm, bas, nbas, env, nenv, 0);
+  // every check before any device work, chunks and molecule ranges, on the
+  // host threads; gc_expand runs only when a shell has nctr > 1
+  plan::BatchPlan p;
+  const char *msg = "";
+  if ((rc = plan::plan_batch(coord, shls, nq, atm, natm, bas, nbas, nenv, std::min(nenv, ENV_HEAD),
+                             CHUNK_Q, CHUNK_OUT, p, &msg)))
+    return set_error(msg), rc;
+  if (!p.gc) return batch_host(out, coord, shls, atm, natm, bas, nbas, env, nenv, 0, p);
   GcExpanded x;
   if ((rc = gc_expand(bas, nbas, env, nenv, x))) return rc;
   // Generally contracted shells: every quartet becomes prod(nctr) quartets of
@@ -435,9 +309,14 @@ int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const
   }
   const long long nsub = (long long)sub.size() / 4;
   const int nbx = (int)(x.bas.size() / 8);
+  const long long nenx = (long long)x.env.size();
+  plan::BatchPlan px;
+  if ((rc = plan::plan_batch(coord, sub.data(), nsub, atm, natm, x.bas.data(), nbx, nenx,
+                             std::min(nenx, ENV_HEAD), CHUNK_Q, CHUNK_OUT, px, &msg)))
+    return set_error(msg), rc;
   std::vector<double> tmp((size_t)eri_batch_out_len(coord, sub.data(), nsub, x.bas.data()));
-  rc = batch_host(tmp.data(), coord, sub.data(), nsub, atm, natm, x.bas.data(), nbx, x.env.data(),
-                  (long long)x.env.size(), 1);
+  rc = batch_host(tmp.data(), coord, sub.data(), atm, natm, x.bas.data(), nbx, x.env.data(), nenx,
+                  1, px);
   if (rc) return rc;
   size_t src = 0, dst = 0;
   for (long long q = 0; q < nq; ++q) {
@@ -695,9 +574,7 @@ LRB_API int lrb_fock_G(LrbMol *m, const double *P, double *G, double tau, long l
   const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
   cudaStream_t st = nullptr;
   double *dP = nullptr, *dG = nullptr;
-  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
-      cudaMallocAsync((void **)&dG, nn * 8, st) != cudaSuccess)
-    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  if (alloc_pair(st, nn, &dP, nn, &dG)) return LRB_ERR_ALLOC;
   cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
   FockStats fs;
   int rc = fock_build(m->ctx, dP, dG, tau, st, &fs);
@@ -716,9 +593,7 @@ LRB_API int lrb_fock_G_prec(LrbMol *m, const double *P, double *G, double tau, i
   const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
   cudaStream_t st = nullptr;
   double *dP = nullptr, *dG = nullptr;
-  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
-      cudaMallocAsync((void **)&dG, nn * 8, st) != cudaSuccess)
-    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  if (alloc_pair(st, nn, &dP, nn, &dG)) return LRB_ERR_ALLOC;
   cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
   FockStats fs;
   int rc = fock_build(m->ctx, dP, dG, tau, st, &fs, prec, tau32, false);
@@ -747,9 +622,7 @@ LRB_API int lrb_fock_G_part(LrbMol *m, const double *P, double *G, double tau, i
   const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
   cudaStream_t st = nullptr;
   double *dP = nullptr, *dG = nullptr;
-  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
-      cudaMallocAsync((void **)&dG, nn * 8, st) != cudaSuccess)
-    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  if (alloc_pair(st, nn, &dP, nn, &dG)) return LRB_ERR_ALLOC;
   cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
   int rc = lrb_fock_G_part_device(m, dP, dG, tau, rank, nranks, quartets, st);
   if (!rc) cudaMemcpyAsync(G, dG, nn * 8, cudaMemcpyDeviceToHost, st);
@@ -904,9 +777,7 @@ LRB_API int lrb_grad(LrbMol *m, const double *P, double cH, double cR, double cS
   const size_t glen = (size_t)(c.nenv - s1), nn = (size_t)c.nao * c.nao;
   cudaStream_t st = nullptr;
   double *dP = nullptr, *dg = nullptr;
-  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
-      cudaMallocAsync((void **)&dg, glen * 8, st) != cudaSuccess)
-    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  if (alloc_pair(st, nn, &dP, glen, &dg)) return LRB_ERR_ALLOC;
   cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(dg, 0, glen * 8, st);
   int rc = grad_run(c, dP, cH, cR, cS, tau, dg, s1, st);
@@ -923,9 +794,7 @@ LRB_API int lrb_grad_nuc(LrbMol *m, const double *P, double tau, double *out) {
   const size_t nn = (size_t)c.nao * c.nao, ng = 3 * (size_t)c.natm;
   cudaStream_t st = nullptr;
   double *dP = nullptr, *dg = nullptr;
-  if (cudaMallocAsync((void **)&dP, nn * 8, st) != cudaSuccess ||
-      cudaMallocAsync((void **)&dg, ng * 8, st) != cudaSuccess)
-    return set_error("allocation failed"), LRB_ERR_ALLOC;
+  if (alloc_pair(st, nn, &dP, ng, &dg)) return LRB_ERR_ALLOC;
   cudaMemcpyAsync(dP, P, nn * 8, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(dg, 0, ng * 8, st);
   int rc = grad_nuc_run(c, dP, tau, dg, st);
