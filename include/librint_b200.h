@@ -11,6 +11,11 @@
  * (LRB_OK or a negative LRB_ERR_*); lrb_last_error() describes the last
  * failure on the calling thread.  The reference-shaped entry points keep the
  * reference's in-band conventions (NULL / NaN) and never exit the process.
+ *
+ * Threads: the library keeps one set of streams and device workspaces per
+ * device, shared by every call on that device; calls on one device from
+ * several host threads must not overlap (each call works on the device that
+ * is current on its thread).
  */
 #ifndef LIBRINT_B200_H
 #define LIBRINT_B200_H
