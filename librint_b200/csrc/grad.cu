@@ -720,10 +720,15 @@ int grad_nuc_run(MolCtx &m, const double *d_P, double tau, double *d_gatom, cuda
 
 namespace lrb {
 
+// cuBLAS handle of the current device, created on first use and kept until
+// exit.
 cublasHandle_t grad_blas() {
-  static cublasHandle_t h[64] = {nullptr};
+  static std::mutex mu;
+  static std::vector<cublasHandle_t> h;   // indexed by device
   int dev = 0;
-  cudaGetDevice(&dev);
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+  std::lock_guard<std::mutex> g(mu);
+  if ((size_t)dev >= h.size()) h.resize((size_t)dev + 1, nullptr);
   if (!h[dev]) cublasCreate(&h[dev]);
   return h[dev];
 }

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "fock.h"
@@ -33,10 +34,15 @@ struct Handles {
   cusolverDnHandle_t sol = nullptr;
 };
 
+// cuBLAS / cuSOLVER handles of the current device, created on first use and
+// kept until exit.
 Handles &handles() {
-  static Handles *h[64] = {nullptr};
+  static std::mutex mu;
+  static std::vector<Handles *> h;   // indexed by device
   int dev = 0;
-  cudaGetDevice(&dev);
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+  std::lock_guard<std::mutex> g(mu);
+  if ((size_t)dev >= h.size()) h.resize((size_t)dev + 1, nullptr);
   if (!h[dev]) {
     h[dev] = new Handles();
     cublasCreate(&h[dev]->blas);
