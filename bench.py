@@ -487,7 +487,8 @@ def main():
                     help="compute the RHF reference energy on the GPU (plain run continued to "
                          "1e-8) instead of reading the recorded one")
     ap.add_argument("--rhf-ablations", action="store_true",
-                    help="also run the mixed (core-H start) and learned FP64 RHF legs")
+                    help="also run the learned FP64 and learned fractional-occupation mixed RHF "
+                         "legs (the mixed core-H leg runs first then)")
     ap.add_argument("--classes", default="",
                     help="comma list of classes to run, e.g. 2222,2221 (default: all 21)")
     args = ap.parse_args()
@@ -837,7 +838,9 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True, ablations=False
                1e-13;
     learned_mixed: the same from the learned guess (when its network
                applies to this basis; the host prediction is timed in);
-    with ablations also learned_fp64.
+    with ablations also learned_fp64 and learned_fractional_mixed (the
+               learned start with fractional occupations at its occupation
+               cut, guess.density_from_lowdin).
     chosen = the fastest leg within 1e-6 Eh of the reference.  Times exclude
     the one-off pair table / Schwarz set-up (setup_s)."""
     import torch
@@ -885,6 +888,13 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True, ablations=False
             if ablations:
                 out["learned_fp64"] = run(1e-5, P0=P0, extra_ms=t_pred)
                 legs.append("learned_fp64")
+                # fractional occupations at the predicted occupation cut
+                tp = time.perf_counter()
+                P0f = g.predict(mol, S=S_ov, fractional=True)
+                t_f = (time.perf_counter() - tp) * 1e3
+                out["learned_fractional_mixed"] = run(1e-5, P0=P0f, extra_ms=t_f, mixed=1,
+                                                      tau_fp32=TAU_FP32)
+                legs.append("learned_fractional_mixed")
             out["learned_mixed"] = run(1e-5, P0=P0, extra_ms=t_pred, mixed=1, tau_fp32=TAU_FP32)
             legs.append("learned_mixed")
             out["predict_ms"] = t_pred
