@@ -66,3 +66,34 @@ def test_string_codes_and_reference_messages(capsys):
     assert "coordinate type does not exist: cart, sph" in capsys.readouterr().out
     assert scf.int2e(m, "spinor") is None
     assert "coordinate type does not exist: cart, sph" in capsys.readouterr().out
+
+
+def test_utils_mirror(capsys):
+    """librint_b200.utils follows python/librint/utils.py: AO counts, the
+    differentiable env range, per-contraction normalisation of [l, [e, c..]]
+    shells (exponents descending, contraction-major coefficients), in-place
+    renormalisation of a molecule's shells (a no-op on normalised ones, a
+    repair after scaling), prep of a PySCF-style molecule and pmat's format."""
+    from librint_b200 import utils
+    m = synthetic.water_like()
+    assert utils.angl(m.bas.reshape(-1, 8), 0) == m.nao(0) == 7
+    assert utils.nparams(m.atm, m.bas) == (3, 5, 7)
+    assert utils.split(m.bas) == dscf.split(m.bas)
+    env = utils.norm([[1, [0.5, 0.3, 1.0], [4.0, 0.7, 0.0], [1.5, 0.2, 2.0]]])
+    e, c = env[:3], env[3:].reshape(2, 3)
+    np.testing.assert_array_equal(e, [4.0, 1.5, 0.5])
+    from librint_b200.basis import gaussian_int
+    ee = np.array([[gaussian_int(4, a + b) for b in e] for a in e])
+    np.testing.assert_allclose([ci @ ee @ ci for ci in c], [1.0, 1.0], rtol=1e-14)
+    env2 = m.env.copy()
+    utils.basis_atm(m.bas.reshape(-1, 8), env2)
+    np.testing.assert_allclose(env2, m.env, rtol=1e-13, atol=0)
+    b0 = m.bas.reshape(-1, 8)[0]
+    env2[b0[6]:b0[6] + b0[2]] *= 2.0
+    utils.basis_atm(m.bas.reshape(-1, 8), env2)
+    np.testing.assert_allclose(env2, m.env, rtol=1e-13, atol=0)
+    atm, bas, env3, nelec = utils.prep(_pyscf_like(m))
+    assert atm.shape == (3, 6) and bas.shape == (5, 8) and nelec == 10
+    np.testing.assert_array_equal(env3, m.env)
+    utils.pmat(np.array([[1.0, -2.0]]))
+    assert capsys.readouterr().out == " 1.000000 -2.000000 \n"
