@@ -717,7 +717,7 @@ double *density_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *en
   if (!m) return nullptr;
   const size_t nn = (size_t)m->ctx.nao * m->ctx.nao;
   double *P = (double *)std::malloc(sizeof(double) * nn);
-  LrbScfOptions o{imax, conv, 0, 0, 0.0, 0, 0.0, 0.0, 6};
+  LrbScfOptions o{imax, conv, 0, 0, 0.0, 0, 0.0, 0.0, 6, 0.0, 0.0};
   if (!P || lrb_scf(m, (long long)nelec, &o, nullptr, P, nullptr)) {
     std::free(P);
     P = nullptr;
@@ -740,7 +740,7 @@ double scf_c(int *atm_p, size_t atm_l, int *bas_p, size_t bas_l, double *env_p, 
              size_t nelec, int imax, double conv) {
   LrbMol *m = mol_from_p2c(atm_p, atm_l, bas_p, bas_l, env_p, env_l);
   if (!m) return NAN;
-  LrbScfOptions o{imax, conv, 0, 0, 0.0, 0, 0.0, 0.0, 6};
+  LrbScfOptions o{imax, conv, 0, 0, 0.0, 0, 0.0, 0.0, 6, 0.0, 0.0};
   LrbScfResult r;
   const int rc = lrb_scf(m, (long long)nelec, &o, &r, nullptr, nullptr);
   lrb_mol_destroy(m);
