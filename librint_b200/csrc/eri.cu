@@ -329,8 +329,10 @@ void fill_c2s(double *c) {
             const int sg = t + (twov - twovm) / 2;
             const double coef = (sg % 2 ? -1.0 : 1.0) * std::pow(0.25, t) * bin(l, t) *
                                 bin(l - t, am + t) * bin(t, u) * bin(am, twov);
-            const int px = 2 * t + am - 2 * u - twov, py = 2 * u + twov, pz = l - 2 * t - am;
-            const int k = (py + pz) * (py + pz + 1) / 2 + pz;   // cart index of (px,py,pz)
+            // powers (2t + am - 2u - twov, py, pz); the cartesian index needs
+            // only py and pz
+            const int py = 2 * u + twov, pz = l - 2 * t - am;
+            const int k = (py + pz) * (py + pz + 1) / 2 + pz;
             c[(l * C2S_M + (m + l)) * C2S_C + k] += norm * scale * coef;
           }
     }

@@ -146,12 +146,6 @@ __global__ void k_dens_max(const double *__restrict__ P, int n, const int *__res
   Dsh[t] = m;
 }
 
-__device__ inline int pair_cls_of(int li, int lj) { return li * (li + 1) / 2 + lj; }
-
-// Quartet test: Schwarz factors times the largest density element that the
-// quartet's J and K contributions touch.  prec: 0 all FP64, 1 all FP32, 2 FP32
-// when the bound is below tau32; FP32 quartets get class ids offset by NCLASS.
-
 // Largest shell-block density maximum (one block).
 __global__ void k_max_reduce(const double *__restrict__ v, int n, double *out) {
   __shared__ double sm[1024];
