@@ -327,54 +327,158 @@ void g_one_root(double *g[3], int rs, const Quartet &q, double aij, double akl,
   }
 }
 
+// Primitive-pair data of an ordered shell pair (A, B), index n = b * nA + a,
+// with the reference's screening key (CINTset_pairdata,
+// src/optimizer.rs:732-808):
+//  * bra form (the pair in the i, j slots): cce, exp(-mu R^2) and the
+//    product centre as ri + (aj / (ai + aj)) (rj - ri); entries failing the
+//    cutoff get centre 1e18 and factor 0; returns true when none passes;
+//  * ket form (the k, l slots): cce, exp(-mu R^2) and the product centre as
+//    (ak rk + al rl) / (ak + al); entries failing the cutoff are skipped by
+//    the primitive loop (factor and centre 0).
+// Both forms restate the two ways src/cint2e.rs's loops compute them.
+double pair_log_rr(const Shell &a, const Shell &b, double rr) {
+  double lr = 1.7 - 1.5 * std::log(a.a[a.nprim - 1] + b.a[b.nprim - 1]);
+  if (a.l + b.l > 0) lr += (a.l + b.l) * std::log(std::sqrt(rr) + 1.0);
+  return lr;
+}
+
+bool pair_bra(const Shell &si, const Shell &sj, double rr, double expcutoff, double *cce,
+              double *e, double *r) {
+  double lci[32], lcj[32];
+  log_maxc(si, lci);
+  log_maxc(sj, lcj);
+  const double log_rr = pair_log_rr(si, sj, rr);
+  bool empty = true;
+  for (int jp = 0; jp < sj.nprim; ++jp)
+    for (int ip = 0; ip < si.nprim; ++ip) {
+      const int n = jp * si.nprim + ip;
+      const double inv = 1.0 / (si.a[ip] + sj.a[jp]);
+      const double x = rr * si.a[ip] * sj.a[jp] * inv;
+      cce[n] = x - log_rr - lci[ip] - lcj[jp];
+      if (cce[n] < expcutoff) {
+        empty = false;
+        const double wj = sj.a[jp] * inv;
+        for (int d = 0; d < 3; ++d) r[3 * n + d] = si.r[d] + wj * (sj.r[d] - si.r[d]);
+        e[n] = std::exp(-x);
+      } else {
+        for (int d = 0; d < 3; ++d) r[3 * n + d] = 1e18;
+        e[n] = 0.0;
+      }
+    }
+  return empty;
+}
+
+void pair_ket(const Shell &sk, const Shell &sl, double rr, double expcutoff, double *cce,
+              double *e, double *r) {
+  double lck[32], lcl[32];
+  log_maxc(sk, lck);
+  log_maxc(sl, lcl);
+  const double log_rr = pair_log_rr(sk, sl, rr);
+  for (int lp = 0; lp < sl.nprim; ++lp)
+    for (int kp = 0; kp < sk.nprim; ++kp) {
+      const int m = lp * sk.nprim + kp;
+      const double ak = sk.a[kp], al = sl.a[lp];
+      const double akl = ak + al;
+      const double x = rr * ak * al / akl;
+      cce[m] = x - log_rr - lck[kp] - lcl[lp];
+      if (cce[m] > expcutoff) {
+        for (int d = 0; d < 3; ++d) r[3 * m + d] = 0.0;
+        e[m] = 0.0;
+        continue;
+      }
+      for (int d = 0; d < 3; ++d) r[3 * m + d] = (ak * sk.r[d] + al * sl.r[d]) / akl;
+      e[m] = std::exp(-x);
+    }
+}
+
+// Pair data of every ordered shell pair of a molecule, built once for the
+// molecule-wide paths (Fock builds, energy, dense tensor), as the reference's
+// integral2e / integral2e_fock build libcint's optimizer once
+// (src/scf.rs:236-250, 333-343).  Per pair (I * nbas + J), np = KI KJ
+// entries each of: bra cce, bra factor, bra centre (3), ket cce, ket factor,
+// ket centre (3).
+struct PairCache {
+  int nbas = 0;
+  std::vector<long long> off;
+  std::vector<char> empty;
+  std::vector<double> buf;
+  const double *at(int i, int j) const { return buf.data() + off[(size_t)i * nbas + j]; }
+};
+
+double squared_distance(const double *a, const double *b) {
+  const double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
+  return d0 * d0 + d1 * d1 + d2 * d2;
+}
+
+void build_pair_cache(PairCache &pc, const int *atm, const int *bas, int nbas, const double *env,
+                      int nt) {
+  pc.nbas = nbas;
+  pc.off.assign((size_t)nbas * nbas + 1, 0);
+  for (int i = 0; i < nbas; ++i)
+    for (int j = 0; j < nbas; ++j)
+      pc.off[(size_t)i * nbas + j + 1] =
+          pc.off[(size_t)i * nbas + j] + 10LL * bas[BAS_SLOTS * i + 2] * bas[BAS_SLOTS * j + 2];
+  pc.buf.assign((size_t)pc.off.back(), 0.0);
+  pc.empty.assign((size_t)nbas * nbas, 0);
+  const double expcutoff = env[0] == 0.0 ? 60.0 : std::max(40.0, env[0]) + 1.0;
+#pragma omp parallel for schedule(dynamic, 8) num_threads(nt)
+  for (int i = 0; i < nbas; ++i) {
+    const Shell si = shell_of(i, atm, bas, env);
+    for (int j = 0; j < nbas; ++j) {
+      const Shell sj = shell_of(j, atm, bas, env);
+      const size_t np = (size_t)si.nprim * sj.nprim;
+      double *p = pc.buf.data() + pc.off[(size_t)i * nbas + j];
+      const double rr = squared_distance(si.r, sj.r);
+      pc.empty[(size_t)i * nbas + j] = pair_bra(si, sj, rr, expcutoff, p, p + np, p + 2 * np);
+      pair_ket(si, sj, rr, expcutoff, p + 5 * np, p + 6 * np, p + 7 * np);
+    }
+  }
+}
+
 // Cartesian block for one quartet, any contraction pattern.  Loop nest and
 // screening follow CINT2e_loop_nopt (src/cint2e.rs:36-465) with
 // CINTset_pairdata (src/optimizer.rs:732-808); the recurrence and the gout
 // root sum follow src/eri.rs:421-516 / src/cint2e.rs:2456, with the
 // recurrence orientation of src/g2e.rs:113-181.
 // out must hold ncart(i)*nctr_i * ... doubles; it is overwritten.
-int eri_cart(double *out, const Quartet &q) {
+int eri_cart(double *out, const Quartet &q, const PairCache *pc = nullptr,
+             const int *shls = nullptr) {
   const Shell &si = q.si, &sj = q.sj, &sk = q.sk, &sl = q.sl;
   const int nfi = ncart(q.li), nfj = ncart(q.lj), nfk = ncart(q.lk), nfl = ncart(q.ll);
   const int ni = nfi * si.nctr, nj = nfj * sj.nctr, nk = nfk * sk.nctr, nl = nfl * sl.nctr;
   const size_t ntot = (size_t)ni * nj * nk * nl;
   std::memset(out, 0, ntot * sizeof(double));
 
-  double lci[16], lcj[16], lck[16], lcl[16];
-  log_maxc(si, lci); log_maxc(sj, lcj); log_maxc(sk, lck); log_maxc(sl, lcl);
-
-  // pair data for (ij)
-  double log_rr_ij = 1.7 - 1.5 * std::log(si.a[si.nprim - 1] + sj.a[sj.nprim - 1]);
-  if (q.li + q.lj > 0) log_rr_ij += (q.li + q.lj) * std::log(std::sqrt(q.rr_ij) + 1.0);
-  // per-thread scratch, grown once: no allocation per quartet
-  static thread_local std::vector<double> cceij, eij, rij, gbuf, prim;
+  // pair data for (ij) and (kl): from the molecule's cache, or computed here
+  // into per-thread scratch (grown once: no allocation per quartet)
+  static thread_local std::vector<double> pbuf, gbuf, prim;
   static thread_local std::vector<int> goff;
-  const size_t npij = (size_t)si.nprim * sj.nprim;
-  if (cceij.size() < npij) {
-    cceij.resize(npij);
-    eij.resize(npij);
-    rij.resize(3 * npij);
+  const size_t npij = (size_t)si.nprim * sj.nprim, npkl = (size_t)sk.nprim * sl.nprim;
+  const double *cceij, *eij, *rij, *kcce, *kexp, *krkl;
+  bool empty;
+  if (pc) {
+    const double *b = pc->at(shls[0], shls[1]), *k = pc->at(shls[2], shls[3]);
+    empty = pc->empty[(size_t)shls[0] * pc->nbas + shls[1]] != 0;
+    cceij = b;
+    eij = b + npij;
+    rij = b + 2 * npij;
+    kcce = k + 5 * npkl;
+    kexp = k + 6 * npkl;
+    krkl = k + 7 * npkl;
+  } else {
+    if (pbuf.size() < 5 * (npij + npkl)) pbuf.resize(5 * (npij + npkl));
+    double *b = pbuf.data(), *k = b + 5 * npij;
+    empty = pair_bra(si, sj, q.rr_ij, q.expcutoff, b, b + npij, b + 2 * npij);
+    cceij = b;
+    eij = b + npij;
+    rij = b + 2 * npij;
+    if (!empty) pair_ket(sk, sl, q.rr_kl, q.expcutoff, k, k + npkl, k + 2 * npkl);
+    kcce = k;
+    kexp = k + npkl;
+    krkl = k + 2 * npkl;
   }
-  bool empty = true;
-  for (int jp = 0; jp < sj.nprim; ++jp)
-    for (int ip = 0; ip < si.nprim; ++ip) {
-      const int n = jp * si.nprim + ip;
-      const double inv = 1.0 / (si.a[ip] + sj.a[jp]);
-      const double e = q.rr_ij * si.a[ip] * sj.a[jp] * inv;
-      cceij[n] = e - log_rr_ij - lci[ip] - lcj[jp];
-      if (cceij[n] < q.expcutoff) {
-        empty = false;
-        const double wj = sj.a[jp] * inv;
-        for (int d = 0; d < 3; ++d) rij[3 * n + d] = si.r[d] + wj * (sj.r[d] - si.r[d]);
-        eij[n] = std::exp(-e);
-      } else {
-        for (int d = 0; d < 3; ++d) rij[3 * n + d] = 1e18;
-        eij[n] = 0.0;
-      }
-    }
   if (empty) return 0;
-  double log_rr_kl = 1.7 - 1.5 * std::log(sk.a[sk.nprim - 1] + sl.a[sl.nprim - 1]);
-  if (q.lk + q.ll > 0) log_rr_kl += (q.lk + q.ll) * std::log(std::sqrt(q.rr_kl) + 1.0);
 
   const CartComp ci(q.li), cj(q.lj), ck(q.lk), cl(q.ll);
   const int nf = nfi * nfj * nfk * nfl;
@@ -416,13 +520,12 @@ int eri_cart(double *out, const Quartet &q) {
     for (int kp = 0; kp < sk.nprim; ++kp) {
       const double ak = sk.a[kp];
       const double akl = ak + al;
-      const double ekl_val = q.rr_kl * ak * al / akl;
-      const double ccekl = ekl_val - log_rr_kl - lck[kp] - lcl[lp];
+      const int m = lp * sk.nprim + kp;
+      const double ccekl = kcce[m];
       if (ccekl > q.expcutoff) continue;
-      double rkl[3];
-      for (int d = 0; d < 3; ++d) rkl[d] = (ak * sk.r[d] + al * sl.r[d]) / akl;
+      const double *rkl = krkl + 3 * m;
       const double eijcutoff = q.expcutoff - ccekl;
-      const double ekl = std::exp(-ekl_val);
+      const double ekl = kexp[m];
       for (int jp = 0; jp < sj.nprim; ++jp)
         for (int ip = 0; ip < si.nprim; ++ip) {
           const int n = jp * si.nprim + ip;
@@ -606,13 +709,13 @@ void cart2sph_4(double *sph, const double *cart, const Quartet &q) {
 }
 
 int quartet_block(double *out, int coord, const int *shls, const int *atm,
-                  const int *bas, const double *env) {
+                  const int *bas, const double *env, const PairCache *pc = nullptr) {
   const Quartet q = make_quartet(shls, atm, bas, env);
-  if (coord == 0) return eri_cart(out, q);
+  if (coord == 0) return eri_cart(out, q, pc, shls);
   const size_t nct = (size_t)ncart(q.li) * q.si.nctr * ncart(q.lj) * q.sj.nctr *
                      ncart(q.lk) * q.sk.nctr * ncart(q.ll) * q.sl.nctr;
   std::vector<double> cart(nct);
-  const int r = eri_cart(cart.data(), q);
+  const int r = eri_cart(cart.data(), q, pc, shls);
   cart2sph_4(out, cart.data(), q);
   return r;
 }
@@ -896,6 +999,8 @@ void orc_int2e_tensor(double *out, int coord, const int *atm, int, const int *ba
   const std::vector<int> off = shell_offsets(coord, bas, nbas);
   const size_t n = off[nbas];
   const int nt = threads_or_default(nthreads);
+  PairCache pc;
+  build_pair_cache(pc, atm, bas, nbas, env, nt);
 #pragma omp parallel num_threads(nt)
   {
     std::vector<double> buf;
@@ -908,7 +1013,7 @@ void orc_int2e_tensor(double *out, int coord, const int *atm, int, const int *ba
             const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
             const int dk = off[k + 1] - off[k], dl = off[l + 1] - off[l];
             buf.resize((size_t)di * dj * dk * dl);
-            quartet_block(buf.data(), coord, shls, atm, bas, env);
+            quartet_block(buf.data(), coord, shls, atm, bas, env, &pc);
             size_t c = 0;
             for (int L = 0; L < dl; ++L)
               for (int K = 0; K < dk; ++K)
@@ -947,6 +1052,8 @@ void orc_fock_G(double *G, const double *P, int coord, const int *atm, int, cons
   const size_t n = off[nbas];
   std::memset(G, 0, n * n * sizeof(double));
   const int nt = threads_or_default(nthreads);
+  PairCache pc;
+  build_pair_cache(pc, atm, bas, nbas, env, nt);
 #pragma omp parallel num_threads(nt)
   {
     std::vector<double> Gl(n * n, 0.0), buf;
@@ -959,7 +1066,7 @@ void orc_fock_G(double *G, const double *P, int coord, const int *atm, int, cons
             const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
             const int dk = off[k + 1] - off[k], dl = off[l + 1] - off[l];
             buf.resize((size_t)di * dj * dk * dl);
-            quartet_block(buf.data(), coord, shls, atm, bas, env);
+            quartet_block(buf.data(), coord, shls, atm, bas, env, &pc);
             size_t c = 0;
             // slot (mu nu | sig lam): G[mu,nu] += P[lam,sig] v; G[mu,lam] -= P[nu,sig] v / 2
             // (src/scf.rs:379-391)
@@ -1003,6 +1110,8 @@ void orc_fock_G_quartets(double *G, const double *P, const int *shls, long nq, c
   const size_t n = off[nbas];
   std::memset(G, 0, n * n * sizeof(double));
   const int nt = threads_or_default(nthreads);
+  PairCache pc;
+  build_pair_cache(pc, atm, bas, nbas, env, nt);
 #pragma omp parallel num_threads(nt)
   {
     std::vector<double> Gl(n * n, 0.0), buf;
@@ -1012,7 +1121,7 @@ void orc_fock_G_quartets(double *G, const double *P, const int *shls, long nq, c
       size_t d = 1;
       for (int a = 0; a < 4; ++a) d *= off[s4[a] + 1] - off[s4[a]];
       buf.resize(d);
-      quartet_block(buf.data(), 0, s4, atm, bas, env);
+      quartet_block(buf.data(), 0, s4, atm, bas, env, &pc);
       digest_quartet(Gl.data(), P, n, off, s4, buf.data());
     }
 #pragma omp critical
@@ -1031,6 +1140,8 @@ void orc_fock_G_blocks(double *out, const double *P, const int *pairs, int npair
                                 (off[pairs[2 * p + 1] + 1] - off[pairs[2 * p + 1]]);
   std::memset(out, 0, boff[npairs] * sizeof(double));
   const int nt = threads_or_default(nthreads);
+  PairCache pc;
+  build_pair_cache(pc, atm, bas, nbas, env, nt);
   // Block (X, Y): every quartet of the reference's nbas^4 loop whose digestion
   // touches G[mu in X, nu in Y]: (X Y | K L) through the first update and
   // (X J | K Y) through the second.
@@ -1050,7 +1161,7 @@ void orc_fock_G_blocks(double *out, const double *P, const int *pairs, int npair
             const int d0 = off[s4[0] + 1] - off[s4[0]], d1 = off[s4[1] + 1] - off[s4[1]];
             const int d2 = off[s4[2] + 1] - off[s4[2]], d3 = off[s4[3] + 1] - off[s4[3]];
             buf.resize((size_t)d0 * d1 * d2 * d3);
-            quartet_block(buf.data(), 0, s4, atm, bas, env);
+            quartet_block(buf.data(), 0, s4, atm, bas, env, &pc);
             size_t c = 0;
             for (int L = 0; L < d3; ++L)
               for (int K = 0; K < d2; ++K)
@@ -1085,6 +1196,8 @@ double orc_energy2_sym(const double *P, const int *atm, int, const int *bas, int
     for (int j = 0; j <= i; ++j, ++p) { pi[p] = i; pj[p] = j; }
   double total = 0.0;
   const int nt = threads_or_default(nthreads);
+  PairCache pc;
+  build_pair_cache(pc, atm, bas, nbas, env, nt);
 #pragma omp parallel num_threads(nt) reduction(+ : total)
   {
     std::vector<double> buf;
@@ -1098,7 +1211,7 @@ double orc_energy2_sym(const double *P, const int *atm, int, const int *bas, int
         const int di = off[i + 1] - off[i], dj = off[j + 1] - off[j];
         const int dk = off[k + 1] - off[k], dl = off[l + 1] - off[l];
         buf.resize((size_t)di * dj * dk * dl);
-        if (!quartet_block(buf.data(), 0, s4, atm, bas, env)) continue;
+        if (!quartet_block(buf.data(), 0, s4, atm, bas, env, &pc)) continue;
         const double w = (i != j ? 2.0 : 1.0) * (k != l ? 2.0 : 1.0) * (bra != ket ? 2.0 : 1.0);
         double s = 0.0;
         size_t c = 0;
