@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -146,9 +147,22 @@ extern "C" {
 
 long long lrb_int2e_batch_len(int coord, const int *shls, long long nq, const int *bas, int nbas) {
   if (!shls || !bas || nq < 0) return -1;
-  for (long long q = 0; q < 4 * nq; ++q)
-    if (shls[q] < 0 || shls[q] >= nbas) return -1;
-  return eri_batch_out_len(coord, shls, nq, bas);
+  // per host-thread part: -1 on a shell index out of range, else its length
+  std::vector<long long> part(64, 0);   // host_parallel runs at most 32 parts
+  std::atomic<int> slot{0};
+  std::atomic<bool> bad{false};
+  plan::host_parallel(nq, plan::HOST_GRAIN, [&](long long b, long long e) {
+    for (long long q = 4 * b; q < 4 * e; ++q)
+      if (shls[q] < 0 || shls[q] >= nbas) {
+        bad.store(true, std::memory_order_relaxed);
+        return;
+      }
+    part[(size_t)slot.fetch_add(1)] = eri_batch_out_len(coord, shls + 4 * b, e - b, bas);
+  });
+  if (bad.load()) return -1;
+  long long n = 0;
+  for (long long v : part) n += v;
+  return n;
 }
 
 int lrb_int2e_batch_device(double *out, int coord, const int *shls, long long nq,

@@ -127,3 +127,24 @@ def test_batch_host_checks_before_any_device_work():
     bad = np.ascontiguousarray(sh[:10])
     assert _batch(L, m, bad, coord=2) == -1
     assert b"coord" in L.lrb_last_error()
+
+
+def test_batch_len_large_and_bad_indices():
+    """lrb_int2e_batch_len (block lengths summed on the host threads) equals
+    the sum of the blocks' products of shell dimensions, cartesian and
+    spherical, and is -1 for an index out of range anywhere in the list."""
+    import numpy as np
+    from librint_b200 import synthetic
+    L = B.lib()
+    m, sh = synthetic.eri_sweep((2, 1, 1, 0), 300_000, seed=4)
+    b = m.bas.reshape(-1, 8)
+    l = b[sh, 1]
+    for coord, dim in ((0, (l + 1) * (l + 2) // 2), (1, 2 * l + 1)):
+        want = int(dim.astype(np.int64).prod(axis=1).sum())
+        got = L.lrb_int2e_batch_len(coord, sh.ctypes.data_as(B.P_i), sh.shape[0],
+                                    m.bas.ctypes.data_as(B.P_i), b.shape[0])
+        assert got == want
+    bad = sh.copy()
+    bad[299_999, 3] = b.shape[0]
+    assert L.lrb_int2e_batch_len(1, bad.ctypes.data_as(B.P_i), bad.shape[0],
+                                 m.bas.ctypes.data_as(B.P_i), b.shape[0]) == -1
