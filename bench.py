@@ -11,6 +11,11 @@ no explicit L2 flush is needed between steps.
 Arms:
   default          the CUDA library (librint_b200), one process per GPU;
                    with torchrun each rank runs its own shard (weak scaling).
+                   On one GPU the line also carries the RHF leg on the
+                   60-atom C/H cluster (``rhf``: plain FP64 vs mixed precision
+                   and the learned start) and the learned guess on held-out
+                   C6H6-like rings (``guess``: SCF iterations and wall time
+                   against the core-Hamiltonian start).
   --impl reference the reference algorithm on the host cores (the CPU
                    restatement in oracle/, since the Rust reference cannot be
                    built here), rank 0 only, on a bounded sample.
@@ -489,6 +494,9 @@ def main():
     ap.add_argument("--rhf-ablations", action="store_true",
                     help="also run the learned FP64 and learned fractional-occupation mixed RHF "
                          "legs (the mixed core-H leg runs first then)")
+    ap.add_argument("--guess-rings", type=int, default=50,
+                    help="held-out C6H6-like ring geometries on which the learned guess is "
+                         "compared with the core-Hamiltonian start (0 skips)")
     ap.add_argument("--classes", default="",
                     help="comma list of classes to run, e.g. 2222,2221 (default: all 21)")
     args = ap.parse_args()
@@ -654,6 +662,13 @@ def main():
         except Exception as exc:   # noqa: BLE001
             rhf = {"error": "%s: %s" % (type(exc).__name__, exc)}
 
+    guess = None
+    if args.guess_rings > 0 and world == 1:
+        try:
+            guess = run_guess_rings(args.guess, args.guess_rings)
+        except Exception as exc:   # noqa: BLE001
+            guess = {"error": "%s: %s" % (type(exc).__name__, exc)}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -682,6 +697,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "rhf": rhf,
+            "guess": guess,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -919,6 +935,29 @@ def run_rhf(guess_file=None, threads=1, fp64_peak=0.0, cpu=True, ablations=False
     ctx.close()
     if cpu:
         out["cpu_baseline"] = rhf_cpu_baseline(mol, P_ref, threads, out["plain"]["iterations"])
+    return out
+
+
+def run_guess_rings(guess_file, n, first=2000, conv=1e-8):
+    """The learned-guess configuration: C6H6-like rings (synthetic.benzene_like,
+    seeds 10000 + i) held out of the network's training set (rings 0..1999),
+    each converged from the core-Hamiltonian start and from the learned start
+    (train_guess.evaluate_one: DIIS(8), tau 1e-12, primitive screening
+    TAU_PRIM, ||dP||/2 <= conv, the settings of the recorded evaluation); SCF
+    iterations and wall time per start (the prediction timed into the
+    learned one) and the largest energy difference between the two."""
+    from librint_b200 import train_guess
+    from librint_b200.guess import LearnedGuess
+    g = LearnedGuess.load(guess_file)
+    t0 = time.perf_counter()
+    rows = [r for r in (train_guess.evaluate_one(g, train_guess.geometry(i, "rings"), conv,
+                                                 {"tau_prim": TAU_PRIM})
+                        for i in range(first, first + n)) if r is not None]
+    out = train_guess.summarise(rows)
+    out.update(config="C6H6-like rings %d..%d (held out of training), 120 cartesian AOs"
+                      % (first, first + n - 1),
+               conv=conv, tau_prim=TAU_PRIM, wall_s=time.perf_counter() - t0,
+               iterations_saved=out["it_core"] - out["it_learned"])
     return out
 
 
