@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "batch_plan.h"
@@ -148,7 +149,7 @@ extern "C" {
 long long lrb_int2e_batch_len(int coord, const int *shls, long long nq, const int *bas, int nbas) {
   if (!shls || !bas || nq < 0) return -1;
   // per host-thread part: -1 on a shell index out of range, else its length
-  std::vector<long long> part(64, 0);   // host_parallel runs at most 32 parts
+  long long part[64] = {0};   // host_parallel runs at most 32 parts
   std::atomic<int> slot{0};
   std::atomic<bool> bad{false};
   plan::host_parallel(nq, plan::HOST_GRAIN, [&](long long b, long long e) {
@@ -287,8 +288,26 @@ static int batch_host(double *out, int coord, const int *shls, const int *atm, i
   return rc;
 }
 
+static int int2e_batch_host(double *out, int coord, const int *shls, long long nq,
+                            const int *atm, int natm, const int *bas, int nbas, const double *env,
+                            long long nenv);
+
 int lrb_int2e_batch(double *out, int coord, const int *shls, long long nq, const int *atm,
                     int natm, const int *bas, int nbas, const double *env, long long nenv) {
+  // host memory for the plan and the generally contracted split may run out;
+  // no exception leaves the C ABI
+  try {
+    return int2e_batch_host(out, coord, shls, nq, atm, natm, bas, nbas, env, nenv);
+  } catch (const std::bad_alloc &) {
+    return set_error("host allocation failed"), LRB_ERR_ALLOC;
+  } catch (...) {
+    return set_error("host error"), LRB_ERR_INPUT;
+  }
+}
+
+static int int2e_batch_host(double *out, int coord, const int *shls, long long nq,
+                            const int *atm, int natm, const int *bas, int nbas, const double *env,
+                            long long nenv) {
   if (nq == 0) return LRB_OK;
   if (!out || !shls || nq < 0) return set_error("bad output or quartet list"), LRB_ERR_INPUT;
   int rc = check_common(atm, natm, bas, nbas, env, nenv);
