@@ -682,7 +682,7 @@ def main():
                          "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
                          "frac": achieved_tf / fp64_peak if fp64_peak > 0 else None,
                          "peak_source": "measured FP64 FMA probe (lrb_fp64_peak_probe) on this "
-                                        "GPU; MEASURED_PEAKS.json has no FP64 figure",
+                                        "GPU (the measured copy and GEMM peaks have no FP64 figure)",
                          "kernel_ms": top_ms, "kernel_share": top_ms / total_kernel_ms,
                          "flop_convention": "fixed per-quartet count, see class_flops_bytes",
                          "traffic": (NCU_TRAFFIC_PER_QUARTET[tuple(top)] * d_top[4].shape[0]
