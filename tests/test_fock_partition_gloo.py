@@ -1,11 +1,13 @@
-"""The multi-GPU Fock build's partition and all-reduce on CPU: two gloo ranks
-take the screened quartet candidates t = rank (mod 2) of the enumeration the
-device uses (shard.fock_candidates), digest their shares with the oracle as
-the per-rank engine, and all-reduce the partial G; the sum must equal the
-oracle's full G, and the shares must be disjoint and complete."""
+"""The multi-GPU Fock build's partition and all-reduce on CPU: N = 2 and 3
+gloo ranks take the screened quartet candidates t = rank (mod N) of the
+enumeration the device uses (shard.fock_candidates), digest their shares
+with the oracle as the per-rank engine, and all-reduce the partial G; the
+sum must equal the oracle's full G, and the shares must be disjoint,
+complete and balanced."""
 import os
 
 import numpy as np
+import pytest
 import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
@@ -99,11 +101,12 @@ def _rank(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_partition_fock_build():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_partition_fock_build(world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 29700 + os.getpid() % 1000
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    port = 29700 + (os.getpid() * 7 + world) % 1000
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = [q.get(timeout=300) for _ in procs]
@@ -112,13 +115,16 @@ def test_two_gloo_ranks_partition_fock_build():
         assert p.exitcode == 0
     m = _molecule()
     G_full = oracle.fock_G(m, _density(m))
+    npair = m.nbas * (m.nbas + 1) // 2
     for rank, G, gathered in out:
         np.testing.assert_allclose(G, G_full, rtol=1e-12, atol=1e-12 * np.abs(G_full).max())
-        a, b = set(gathered[0]), set(gathered[1])
-        assert not (a & b)                                  # disjoint
-        npair = m.nbas * (m.nbas + 1) // 2
-        assert len(a | b) == npair * (npair + 1) // 2        # every canonical quartet (tau = 0)
-        assert abs(len(a) - len(b)) <= 1                     # balanced
+        shares = [set(g) for g in gathered]
+        for a in range(world):
+            for b in range(a + 1, world):
+                assert not (shares[a] & shares[b])         # disjoint
+        assert len(set().union(*shares)) == npair * (npair + 1) // 2   # every quartet (tau = 0)
+        sizes = [len(x) for x in shares]
+        assert max(sizes) - min(sizes) <= 1                # balanced
 
 
 def test_candidate_enumeration_prefix_rule():
