@@ -8,10 +8,12 @@ runs on, how fast that restatement is per core compared with the shipped
 library on the same shell quartets: for every class of the ERI sweep it draws
 8-shell molecules from the sweep's distribution (K = 1..6, exponents
 log-uniform in [0.05, 5000], centres in a 10 A cube), times the reference's
-``int2e_c`` (all nbas^4 quartets of the molecule, spherical, one core), and
-times the oracle on the same nbas^4 quartet list on one thread.  The library
-is only called through its exported C entry point (src/p2c.rs:109), as
-python/librint/_bindings.py does.
+``int2e_c`` (all nbas^4 quartets of the molecule, spherical, one core; the
+reference builds libcint's optimizer once per call, src/scf.rs:236-250), and
+times the oracle's dense tensor of the same molecule (orc_int2e_tensor: the
+same nbas^4 quartets, pair data built once per call) on one thread.  The
+library is only called through its exported C entry point
+(src/p2c.rs:109), as python/librint/_bindings.py does.
 
 Run (needs the reference checkout, only in the development container):
     python oracle/time_vs_reference.py <path of the reference checkout> [molecules per class]
@@ -19,7 +21,6 @@ Run (needs the reference checkout, only in the development container):
 from __future__ import annotations
 
 import ctypes
-import itertools
 import os
 import sys
 import time
@@ -71,11 +72,10 @@ def main():
             if not ptr:
                 sys.exit(f"reference int2e_c failed for class {cls}")
             libc.free(ptr)
-            sh = np.array(list(itertools.product(range(nb), repeat=4)), dtype=np.int32)
             t0 = time.perf_counter()
-            oracle.int2e_batch(m, sh, 1, nthreads=1)
+            oracle.int2e_tensor(m, 1, nthreads=1)
             to += time.perf_counter() - t0
-            nq += sh.shape[0]
+            nq += nb ** 4
         rows.append((cls, nq, nq / tr, nq / to))
         tr_all += tr
         to_all += to
