@@ -347,6 +347,9 @@ static int int2e_batch_host(double *out, int coord, const int *shls, long long n
   if ((rc = plan::plan_batch(coord, sub.data(), nsub, atm, natm, x.bas.data(), nbx, nenx,
                              std::min(nenx, ENV_HEAD), CHUNK_Q, CHUNK_OUT, px, &msg)))
     return set_error(msg), rc;
+  // the sub-shells' screening coefficients (bas slot 7) sit at the end of the
+  // expanded env, outside every chunk's env range: upload the whole molecule
+  px.streamed = false;
   std::vector<double> tmp((size_t)eri_batch_out_len(coord, sub.data(), nsub, x.bas.data()));
   rc = batch_host(tmp.data(), coord, sub.data(), atm, natm, x.bas.data(), nbx, x.env.data(), nenx,
                   1, px);
